@@ -1,0 +1,249 @@
+// common.cuh -- device-side helpers shared by the engine's kernels.
+//
+// Geometry follows the reference bit for bit where the density maps must be
+// reproducible: products that feed a sum use explicit round-to-nearest
+// intrinsics so nvcc cannot contract them into FMAs.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ep {
+
+constexpr double kEps = 1.0e-15;          // EPS, PlaceCommon/global.h:39
+constexpr double kNegMaxExp = -300.0;     // NEGATIVE_MAX_EXP, global.h:46
+
+enum ObjFlag : uint8_t {
+    kMacro = 1,     // Module::isMacro
+    kFiller = 2,    // Module::isFiller
+    kInView = 4,    // member of the current stage view
+    kBig = 8,       // spans more bins than a thread handles: block-per-object path
+};
+
+// Device-resident scalars of one engine (EPlacer_2D + EplaceNesterovOpt state
+// and the accumulators of the fused reductions).  Written only by the
+// finalising block of each reduction; every kernel reads `done`.
+struct DevScalars {
+    // arrival counters of the grid-wide reductions (reset by their last block)
+    unsigned int cnt_prep, cnt_wl, cnt_comb, cnt_upd, cnt_hp;
+    double hpwl_query;                // result of the standalone HPWL pass
+    // results
+    double tau;
+    double hpwl;
+    double wirelength;
+    double lambda;
+    double last_hpwl;
+    double inv_gamma_x, inv_gamma_y;
+    double step;
+    double a;          // Nesterov a_k
+    double coef;       // (a_k - 1) / a_{k+1}
+    double lip_step;   // 1/L of the last step (BB fallback)
+    int iter;          // steps taken in this stage
+    int done;          // stop condition reached: later kernels of the loop are no-ops
+    int stop_pending;  // set by the combine finaliser, committed by the update
+    int lambda_pending;// lambda update owed for the last step (uses the next HPWL)
+    int lambda0_mode;  // the evaluation of initialization(): lambda = 0, then lambda_0
+    int status;        // ep_status bits raised on the device
+    int stage;
+    int max_iter;
+    float target_overflow;
+    int step_rule;
+    int mgp_iterations;
+    int step_cap;      // > 0: also stop after this many steps (bounded runs)
+};
+
+// ----- geometry (reference float semantics) -------------------------------
+struct Grid {
+    int nx, ny;
+    float llx, lly, urx, ury;  // core region
+    float sx, sy;              // bin step
+    float td;                  // target density
+};
+
+// getOverlap/getOverlapArea (PlaceCommon/global.h:477-518), FP64.
+__device__ __forceinline__ double overlap_len(double a0, double a1, double b0, double b1) {
+    double s = fmax(a0, b0);
+    double e = fmin(a1, b1);
+    return s >= e ? 0.0 : __dsub_rn(s, e);
+}
+
+__device__ __forceinline__ double overlap_area(double l1, double b1, double r1, double t1,
+                                               double l2, double b2, double r2, double t2) {
+    double h = overlap_len(l1, r1, l2, r2);
+    if (h == 0.0) return 0.0;
+    double v = overlap_len(b1, t1, b2, t2);
+    if (v == 0.0) return 0.0;
+    return __dmul_rn(h, v);
+}
+
+// float_less (global.h:350-353)
+__device__ __forceinline__ bool f_less(float a, float b) {
+    return (double)__fsub_rn(a, b) < -kEps;
+}
+
+struct Rect {
+    float llx, lly, urx, ury, sx, sy;
+};
+
+// Object rectangle with local smoothing, EPlace/eplace.cpp:1052-1072.
+__device__ __forceinline__ Rect object_rect(const Grid &g, float cx, float cy, float w, float h) {
+    Rect r;
+    float cllx = __fsub_rn(cx, __fmul_rn(0.5f, w));
+    float clly = __fsub_rn(cy, __fmul_rn(0.5f, h));
+    r.llx = cllx;
+    r.urx = __fadd_rn(cllx, w);
+    r.lly = clly;
+    r.ury = __fadd_rn(clly, h);
+    r.sx = 1.0f;
+    r.sy = 1.0f;
+    if (f_less(w, g.sx)) {
+        r.sx = __fdiv_rn(w, g.sx);
+        double half = __dmul_rn(0.5, (double)g.sx);
+        r.llx = (float)__dsub_rn((double)cx, half);
+        r.urx = (float)__dadd_rn((double)cx, half);
+    }
+    if (f_less(h, g.sy)) {
+        r.sy = __fdiv_rn(h, g.sy);
+        double half = __dmul_rn(0.5, (double)g.sy);
+        r.lly = (float)__dsub_rn((double)cy, half);
+        r.ury = (float)__dadd_rn((double)cy, half);
+    }
+    return r;
+}
+
+// INT_DOWN bin range, end clamped (EPlace/eplace.cpp:1079-1104); the start is
+// clamped at 0 (the reference asserts it; the core clamp keeps it there).
+__device__ __forceinline__ void bin_range(const Grid &g, const Rect &r, int &i0, int &i1, int &j0,
+                                          int &j1) {
+    i0 = (int)__fdiv_rn(__fsub_rn(r.llx, g.llx), g.sx);
+    i1 = (int)__fdiv_rn(__fsub_rn(r.urx, g.llx), g.sx);
+    j0 = (int)__fdiv_rn(__fsub_rn(r.lly, g.lly), g.sy);
+    j1 = (int)__fdiv_rn(__fsub_rn(r.ury, g.lly), g.sy);
+    i0 = max(i0, 0);
+    j0 = max(j0, 0);
+    i1 = min(i1, g.nx - 1);
+    j1 = min(j1, g.ny - 1);
+}
+
+// Bin corners as binInitialization stores them (EPlace/eplace.cpp:300-307).
+__device__ __forceinline__ void bin_box(const Grid &g, int i, int j, float &l, float &b, float &r,
+                                        float &t) {
+    l = __fadd_rn(__fmul_rn((float)i, g.sx), g.llx);
+    b = __fadd_rn(__fmul_rn((float)j, g.sy), g.lly);
+    r = __fadd_rn(l, g.sx);
+    t = __fadd_rn(b, g.sy);
+}
+
+__device__ __forceinline__ double rect_bin_overlap(const Grid &g, const Rect &r, int i, int j) {
+    float l, b, rr, t;
+    bin_box(g, i, j, l, b, rr, t);
+    return overlap_area(l, b, rr, t, r.llx, r.lly, r.urx, r.ury);
+}
+
+// fastExp, PlaceCommon/global.h:457-471 (float, ten squarings).
+__device__ __forceinline__ float fast_exp(float a) {
+    a = __fadd_rn(1.0f, __fdiv_rn(a, 1024.0f));
+#pragma unroll
+    for (int i = 0; i < 10; i++) a = __fmul_rn(a, a);
+    return a;
+}
+
+__device__ __forceinline__ float wl_exp(float a, int exact) { return exact ? expf(a) : fast_exp(a); }
+
+// ----- reductions ------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum of NV doubles; result valid in thread 0.  `sh` needs
+// NV * 32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sh) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[k * 32 + wid] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = lane < nw ? sh[k * 32 + lane] : 0.0;
+            v[k] = warp_sum(s);
+        }
+    }
+    __syncthreads();
+}
+
+// "Last block done": returns true in thread 0 of the block that finishes
+// last among `total` blocks (counted on *cnt, which it resets).
+__device__ __forceinline__ bool last_block(unsigned int *cnt, unsigned int total) {
+    __threadfence();
+    unsigned int prev = atomicAdd(cnt, 1u);
+    if (prev == total - 1) {
+        __threadfence();
+        *cnt = 0;
+        return true;
+    }
+    return false;
+}
+
+// Deterministic grid-wide sum of NV doubles.  Every block writes its block
+// total to partials[k * total + block_id]; the block that arrives last sums
+// the partials in a fixed order (thread-strided, then a fixed tree), so the
+// result does not depend on block scheduling.  Must be called by all threads
+// of every participating block.  Returns true in all threads of the last
+// block; its thread 0 then holds the totals in v.
+template <int NV>
+__device__ __forceinline__ bool grid_sum(double (&v)[NV], double *sh, double *partials,
+                                         unsigned int *cnt, unsigned int total,
+                                         unsigned int block_id) {
+    __shared__ int is_last;
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) partials[(size_t)k * total + block_id] = v[k];
+        __threadfence();
+        unsigned int prev = atomicAdd(cnt, 1u);
+        is_last = (prev == total - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double s[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        s[k] = 0.0;
+        for (unsigned int i = threadIdx.x; i < total; i += blockDim.x)
+            s[k] += __ldcg(&partials[(size_t)k * total + i]);
+    }
+    block_sum<NV>(s, sh);
+    if (threadIdx.x == 0) {
+        *cnt = 0;
+#pragma unroll
+        for (int k = 0; k < NV; k++) v[k] = s[k];
+    }
+    return true;
+}
+
+}  // namespace ep

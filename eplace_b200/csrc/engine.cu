@@ -1,0 +1,1070 @@
+// engine.cu -- host side of the engine and the C-ABI of include/eplace_gpu.h.
+//
+// Construction mirrors what the reference does before the hot loop:
+//   PlaceDB::setCoreRegion            PlaceDB/placedb.cpp:52-77
+//   PlaceDB::addNode (macro test)     PlaceDB/placedb.cpp:96-114
+//   EPlacer_2D::fillerInitialization  EPlace/eplace.cpp:61-208
+//   EPlacer_2D::binInitialization     EPlace/eplace.cpp:221-412
+// with the same float arithmetic, so filler counts, bin geometry and the
+// static terminal / base density maps equal the reference's.  The netlist is
+// then laid out on the device as SoA arrays plus two CSRs (net -> pins,
+// object -> pins) and the loop of kernels.cu / dct.cu runs there.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+using namespace ep;
+
+struct ep_engine {
+    ep_params prm{};
+    std::string err;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+
+    int n_nodes = 0, n_fillers = 0, n_obj = 0, n_terms = 0, n_nets = 0, n_pins = 0;
+    int n_macros = 0, n_cgp = 0;
+    Grid grid{};
+    KernelCtx kc{};
+    float filler_w = 0, filler_h = 0;
+    double std_area = 0, macro_area = 0, total_row_area = 0;
+
+    std::vector<uint8_t> h_flags;  // kMacro / kFiller / kBig (no view bit)
+    std::vector<float2> h_size;
+    std::vector<int32_t> h_view[3];
+
+    // device buffers
+    float2 *pos = nullptr, *x = nullptr, *g = nullptr, *y_prev = nullptr, *g_prev = nullptr;
+    float2 *size = nullptr, *pin_off = nullptr, *pin_grad = nullptr, *gd_big = nullptr;
+    float2 *dump_gd = nullptr, *dump_gwl = nullptr, *field = nullptr, *static_map = nullptr;
+    float2 *staging = nullptr;
+    uint8_t *flags = nullptr;
+    float *npins = nullptr, *area = nullptr, *rho = nullptr, *node_f = nullptr, *filler_f = nullptr;
+    float *phi = nullptr;
+    int32_t *net_start = nullptr, *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pins = nullptr;
+    int32_t *small_nets = nullptr, *big_nets = nullptr, *big_objs = nullptr, *big_slot = nullptr;
+    int32_t *view_idx[3] = {nullptr, nullptr, nullptr};
+    unsigned long long *node_q = nullptr, *filler_q = nullptr;
+    DevScalars *S = nullptr;
+    DevScalars *hS = nullptr;  // pinned mirror
+    std::vector<void *> allocs;
+
+    DeviceNetlist dn{};
+    DctPlan dct;
+
+    int stage = EP_STAGE_MGP;
+    bool initialized = false;
+    bool in_run = false;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mt19937_64 rng;
+};
+
+namespace {
+
+constexpr double kHostEps = 1.0e-15;
+
+bool f_less_h(float a, float b) { return (double)(a - b) < -1.0 * kHostEps; }
+bool f_greater_h(float a, float b) { return (double)(a - b) > 1.0 * kHostEps; }
+bool f_equal_h(float a, float b) { return std::fabs((double)(a - b)) < kHostEps; }
+
+double overlap_len_h(double a0, double a1, double b0, double b1) {
+    double s = std::max(a0, b0), e = std::min(a1, b1);
+    return s >= e ? 0.0 : (s - e);
+}
+
+double overlap_area_h(double l1, double b1, double r1, double t1, double l2, double b2, double r2,
+                      double t2) {
+    double h = overlap_len_h(l1, r1, l2, r2);
+    if (h == 0) return 0;
+    double v = overlap_len_h(b1, t1, b2, t2);
+    if (v == 0) return 0;
+    return h * v;
+}
+
+// PlaceDB::setModuleCenter_2D clamp (PlaceDB/placedb.cpp:257-281).
+void clamp_center_h(const Grid &g, float &x, float &y, float w, float h) {
+    if (x - 0.5 * w < g.llx) x = (float)(g.llx + 0.5 * w + kHostEps);
+    if (x + 0.5 * w > g.urx) x = (float)(g.urx - 0.5 * w - kHostEps);
+    if (y - 0.5 * h < g.lly) y = (float)(g.lly + 0.5 * h + kHostEps);
+    if (y + 0.5 * h > g.ury) y = (float)(g.ury - 0.5 * h - kHostEps);
+}
+
+// PlaceDB::setModuleLocation_2D clamp of the lower-left corner
+// (PlaceDB/placedb.cpp:207-228), then Module::setLocation_2D's centre.
+void location_to_center_h(const Grid &g, float llx, float lly, float w, float h, float &cx, float &cy) {
+    float x = llx, y = lly;
+    if (x < g.llx) x = g.llx;
+    if (x + w > g.urx) x = (float)(g.urx - w - kHostEps);
+    if (y < g.lly) y = g.lly;
+    if (y + h > g.ury) y = (float)(g.ury - h - kHostEps);
+    cx = x + (float)0.5 * w;
+    cy = y + (float)0.5 * h;
+}
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t _e = (call);                                                   \
+        if (_e != cudaSuccess) {                                                   \
+            e->err = std::string(#call) + ": " + cudaGetErrorString(_e);           \
+            return EP_ERR_CUDA;                                                    \
+        }                                                                          \
+    } while (0)
+
+template <typename T>
+ep_status dalloc(ep_engine *e, T *&p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t rc = cudaMalloc((void **)&p, n * sizeof(T));
+    if (rc != cudaSuccess) {
+        e->err = std::string("cudaMalloc: ") + cudaGetErrorString(rc);
+        p = nullptr;
+        return EP_ERR_NOMEM;
+    }
+    e->allocs.push_back((void *)p);
+    return EP_OK;
+}
+
+template <typename T>
+ep_status dupload(ep_engine *e, T *&p, const std::vector<T> &v) {
+    ep_status s = dalloc(e, p, v.size());
+    if (s) return s;
+    if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return EP_OK;
+}
+
+// Reference bin-count rule, EPlace/eplace.cpp:230-261.
+int bin_dimension(float std_area, float macro_area, int num_nodes, float core_w, float core_h,
+                  float td) {
+    float node_area = std_area + macro_area;
+    float core_area = core_w * core_h;
+    float avg = (float)(1.0 * node_area / num_nodes);
+    float ideal = avg / td;
+    int ideal_count = (int)(1.0 * (core_area / ideal) + 0.5f);
+    for (int i = 1; i < 10; i++) {
+        long a = (long)(2 << i) * (2 << i), b = (long)(2 << (i + 1)) * (2 << (i + 1));
+        if (a <= ideal_count && b > ideal_count) return 2 << i;
+    }
+    return 1024;
+}
+
+ep_status check_netlist(ep_engine *e, const ep_netlist *nl) {
+    if (!nl || nl->num_nodes <= 0 || nl->num_terminals < 0 || nl->num_nets < 0 || nl->num_rows <= 0) {
+        e->err = "netlist: counts must be positive (nodes, rows) / non-negative";
+        return EP_ERR_ARG;
+    }
+    if (!nl->node_w || !nl->node_h || !nl->node_cx || !nl->node_cy || !nl->row_llx ||
+        !nl->row_lly || !nl->row_urx || !nl->row_h) {
+        e->err = "netlist: missing node or row arrays";
+        return EP_ERR_ARG;
+    }
+    if (nl->num_terminals > 0 && (!nl->term_llx || !nl->term_lly || !nl->term_w || !nl->term_h)) {
+        e->err = "netlist: missing terminal arrays";
+        return EP_ERR_ARG;
+    }
+    if (nl->num_nets > 0 && (!nl->net_start || !nl->pin_owner || !nl->pin_dx || !nl->pin_dy)) {
+        e->err = "netlist: missing net / pin arrays";
+        return EP_ERR_ARG;
+    }
+    if (nl->num_nets > 0) {
+        if (nl->net_start[0] != 0) {
+            e->err = "netlist: net_start[0] must be 0";
+            return EP_ERR_ARG;
+        }
+        for (int n = 0; n < nl->num_nets; n++)
+            if (nl->net_start[n + 1] < nl->net_start[n]) {
+                e->err = "netlist: net_start must be non-decreasing";
+                return EP_ERR_ARG;
+            }
+        int np = nl->net_start[nl->num_nets];
+        for (int p = 0; p < np; p++)
+            if (nl->pin_owner[p] < 0 || nl->pin_owner[p] >= nl->num_nodes + nl->num_terminals) {
+                e->err = "netlist: pin_owner out of range";
+                return EP_ERR_ARG;
+            }
+    }
+    for (int i = 0; i < nl->num_nodes; i++)
+        if (!(nl->node_w[i] > 0) || !(nl->node_h[i] > 0) || !std::isfinite(nl->node_cx[i]) ||
+            !std::isfinite(nl->node_cy[i])) {
+            e->err = "netlist: node sizes must be positive and centres finite";
+            return EP_ERR_ARG;
+        }
+    for (int n = 0; n < nl->num_nets; n++)
+        if (nl->net_start[n + 1] == nl->net_start[n]) {
+            e->err = "netlist: empty net (the reference asserts bound pins exist)";
+            return EP_ERR_ARG;
+        }
+    return EP_OK;
+}
+
+void set_view_flags(ep_engine *e, int stage, std::vector<uint8_t> &fl) {
+    fl = e->h_flags;
+    for (int o : e->h_view[stage]) fl[o] |= kInView;
+}
+
+ep_status upload_view(ep_engine *e, int stage) {
+    std::vector<uint8_t> fl;
+    set_view_flags(e, stage, fl);
+    CK(cudaMemcpyAsync(e->flags, fl.data(), fl.size(), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status fetch_scalars(ep_engine *e) {
+    CK(cudaMemcpyAsync(e->hS, e->S, sizeof(DevScalars), cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+template <typename F>
+ep_status update_scalars(ep_engine *e, F f) {
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    f(*e->hS);
+    CK(cudaMemcpyAsync(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status device_status(ep_engine *e) {
+    int st = e->hS->status;
+    if (st & (1 << EP_ERR_NAN)) {
+        e->err = "non-finite value in a device reduction (overflow, HPWL, lambda or step)";
+        return EP_ERR_NAN;
+    }
+    if (st & (1 << EP_ERR_TIMEOUT)) {
+        e->err = "a bounded device wait gave up";
+        return EP_ERR_TIMEOUT;
+    }
+    return EP_OK;
+}
+
+// totalGradientUpdate: enqueue one gradient evaluation at the current positions.
+void enqueue_eval(ep_engine *e, int stepping) {
+    cudaStream_t st = e->st;
+    bool keep = e->prm.keep_maps != 0;
+    if (keep) {
+        cudaMemsetAsync(e->node_q, 0, sizeof(unsigned long long) * e->grid.nx * e->grid.ny, st);
+        cudaMemsetAsync(e->filler_q, 0, sizeof(unsigned long long) * e->grid.nx * e->grid.ny, st);
+    }
+    launch_scatter(e->kc, e->dn, e->node_q, e->filler_q, e->S, st);
+    void *bf = e->dct.mode == EP_DCT_BF16X3 ? dct_tc_rho_planes(e->dct) : nullptr;
+    launch_prep(e->kc, e->node_q, e->filler_q, e->static_map, bf ? nullptr : e->rho, bf,
+                keep ? e->node_f : nullptr, keep ? e->filler_f : nullptr, keep ? 0 : 1, e->S, st);
+    dct_run(e->dct, e->rho, e->field, keep ? e->phi : nullptr, e->S, st);
+    launch_wirelength(e->kc, e->dn, e->pin_grad, e->S, st);
+    launch_gather_big(e->kc, e->dn, e->field, e->gd_big, e->S, st);
+    launch_combine(e->kc, e->dn, e->field, e->gd_big, e->pin_grad, e->g, e->g_prev, e->y_prev,
+                   keep ? e->dump_gd : nullptr, keep ? e->dump_gwl : nullptr, stepping, e->S, st);
+}
+
+void enqueue_step(ep_engine *e) {
+    enqueue_eval(e, 1);
+    launch_update(e->kc, e->dn, e->pos, e->x, e->g, e->y_prev, e->g_prev, e->S, e->st);
+}
+
+ep_status build_graph(ep_engine *e, int iters) {
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < iters; i++) enqueue_step(e);
+    CK(cudaStreamEndCapture(e->st, &g));
+    cudaError_t rc = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (rc != cudaSuccess) {
+        e->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc);
+        e->graph = nullptr;
+        return EP_ERR_CUDA;
+    }
+    e->graph_iters = iters;
+    return EP_OK;
+}
+
+__global__ void k_gather_view(const int32_t *__restrict__ idx, int n, const float2 *__restrict__ src,
+                              float2 *__restrict__ dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+
+__global__ void k_scatter_view(Grid g, const int32_t *__restrict__ idx, int n,
+                               const float2 *__restrict__ src, const float2 *__restrict__ size,
+                               float2 *__restrict__ pos) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = idx[i];
+    float2 c = src[i], s = size[o];
+    double hw = 0.5 * (double)s.x, hh = 0.5 * (double)s.y;
+    float xx = c.x, yy = c.y;
+    if ((double)xx - hw < (double)g.llx) xx = (float)((double)g.llx + hw + 1.0e-15);
+    if ((double)xx + hw > (double)g.urx) xx = (float)((double)g.urx - hw - 1.0e-15);
+    if ((double)yy - hh < (double)g.lly) yy = (float)((double)g.lly + hh + 1.0e-15);
+    if ((double)yy + hh > (double)g.ury) yy = (float)((double)g.ury - hh - 1.0e-15);
+    pos[o] = make_float2(xx, yy);
+}
+
+ep_status check_view(ep_engine *e, int view, int count) {
+    if (view < 0 || view > 2) {
+        e->err = "view must be an ep_stage";
+        return EP_ERR_ARG;
+    }
+    if (count != (int)e->h_view[view].size()) {
+        e->err = "count does not match the size of the stage view";
+        return EP_ERR_ARG;
+    }
+    return EP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ep_abi_version(void) { return EP_ABI_VERSION; }
+
+void ep_default_params(ep_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->target_density = 1.0f;
+    p->target_overflow = 0.10f;
+    p->max_iterations = 1000;
+    p->wl_model = EP_WL_WA;
+    p->exp_mode = EP_EXP_FAST;
+    p->step_rule = EP_STEP_LIPSCHITZ;
+    p->dct_mode = EP_DCT_FP32;
+    p->filler_seed = 1;
+}
+
+const char *ep_last_error(const ep_engine *e) { return e ? e->err.c_str() : "null engine"; }
+
+ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **out) {
+    if (!out || !params) return EP_ERR_ARG;
+    *out = nullptr;
+    ep_engine *e = new ep_engine();
+    *out = e;
+    e->prm = *params;
+    const ep_params &P = e->prm;
+    ep_status s = check_netlist(e, nl);
+    if (s) return s;
+    if (!(P.target_density > 0) || P.target_density > 1.0f + 1e-6f) {
+        e->err = "target_density must be in (0, 1]";
+        return EP_ERR_ARG;
+    }
+    if (P.dct_mode != EP_DCT_FP32 && P.dct_mode != EP_DCT_BF16X3) {
+        e->err = "unknown dct_mode";
+        return EP_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        e->err = "no CUDA device: the engine has no CPU fallback";
+        return EP_ERR_CUDA;
+    }
+    e->device = P.device;
+    CK(cudaSetDevice(P.device));
+    CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+    e->own_stream = true;
+    CK(cudaEventCreate(&e->ev0));
+    CK(cudaEventCreate(&e->ev1));
+    e->rng.seed(P.filler_seed);
+
+    const int nn = nl->num_nodes, nt = nl->num_terminals, nnet = nl->num_nets, nr = nl->num_rows;
+    const int np = nnet > 0 ? nl->net_start[nnet] : 0;
+    e->n_nodes = nn;
+    e->n_terms = nt;
+    e->n_nets = nnet;
+    e->n_pins = np;
+
+    // ---- core region and row area (PlaceDB::setCoreRegion) ----
+    float bottom = nl->row_lly[0];
+    float top = (float)((double)nl->row_lly[nr - 1] + (double)nl->row_h[nr - 1]);
+    float left = nl->row_llx[0], right = nl->row_urx[0];
+    float total_row_area = 0;
+    for (int r = 0; r < nr; r++) {
+        left = std::min(left, nl->row_llx[r]);
+        right = std::max(right, nl->row_urx[r]);
+        float cur = (float)((double)(nl->row_urx[r] - nl->row_llx[r]) * (double)nl->row_h[r]);
+        total_row_area += cur;
+    }
+    if (!(right > left) || !(top > bottom)) {
+        e->err = "rows give an empty core region";
+        return EP_ERR_ARG;
+    }
+    e->total_row_area = total_row_area;
+    float row_h = nl->common_row_height > 0 ? nl->common_row_height : nl->row_h[nr - 1];
+    Grid &g = e->grid;
+    g.llx = left;
+    g.lly = bottom;
+    g.urx = right;
+    g.ury = top;
+    g.td = P.target_density;
+
+    // ---- node classes (PlaceDB::addNode) ----
+    std::vector<uint8_t> is_macro(nn, 0);
+    for (int i = 0; i < nn; i++) {
+        if (f_greater_h(nl->node_h[i], row_h)) {
+            is_macro[i] = 1;
+            e->n_macros++;
+        } else if (f_greater_h(row_h, nl->node_h[i])) {
+            e->err = "a node is lower than the row height (PlaceDB::addNode rejects it)";
+            return EP_ERR_ARG;
+        }
+    }
+
+    // ---- fillers (fillerInitialization) ----
+    float overlap = 0;
+    for (int t = 0; t < nt; t++) {
+        if (nl->term_is_ni && nl->term_is_ni[t]) continue;
+        for (int r = 0; r < nr; r++)
+            overlap += (float)overlap_area_h(nl->term_llx[t], nl->term_lly[t],
+                                             nl->term_llx[t] + nl->term_w[t],
+                                             nl->term_lly[t] + nl->term_h[t], nl->row_llx[r],
+                                             nl->row_lly[r], nl->row_urx[r],
+                                             (float)((double)nl->row_lly[r] + nl->row_h[r]));
+    }
+    float whitespace = total_row_area - overlap;
+    float sa = 0, ma = 0;
+    std::vector<float> areas(nn);
+    for (int i = 0; i < nn; i++) {
+        float a = nl->node_w[i] * nl->node_h[i];
+        areas[i] = a;
+        if (is_macro[i])
+            ma += a;
+        else
+            sa += a;
+    }
+    e->std_area = sa;
+    e->macro_area = ma;
+    float node_scaled = sa + ma * P.target_density;
+    float total_filler = whitespace * P.target_density - node_scaled;
+    std::sort(areas.begin(), areas.end());
+    int lo = (int)(0.05 * (float)nn), hi = (int)(0.95 * (float)nn);
+    float acc = 0;
+    for (int i = lo; i < hi; i++) acc += areas[i];
+    float filler_area = hi > lo ? acc / ((float)(hi - lo)) : (nn > 0 ? areas[nn / 2] : 1.0f);
+    e->filler_h = row_h;
+    e->filler_w = filler_area / row_h;
+    int nf = (int)(total_filler / filler_area + 0.5);
+    if (nf < 0) nf = 0;
+    e->n_fillers = nf;
+    const int no = nn + nf;
+    e->n_obj = no;
+
+    // ---- bin grid (binInitialization) ----
+    int nbx = P.bins_x, nby = P.bins_y;
+    if (nbx <= 0 || nby <= 0) {
+        nbx = nby = bin_dimension(sa, ma, nn, right - left, top - bottom, P.target_density);
+    }
+    if (nbx < 2 || nby < 2 || nbx > 4096 || nby > 4096) {
+        e->err = "bins must be in [2, 4096]";
+        return EP_ERR_ARG;
+    }
+    g.nx = nbx;
+    g.ny = nby;
+    g.sx = (right - left) / (float)nbx;
+    g.sy = (top - bottom) / (float)nby;
+    const int nb = nbx * nby;
+    const float bin_area_f = g.sx * g.sy;
+
+    // terminal density (EPlace/eplace.cpp:327-374) and base density (:385-409)
+    std::vector<float> term_d(nb, 0.0f), base_d(nb, 0.0f);
+    auto bin_box = [&](int i, int j, float &l, float &b, float &r, float &t) {
+        l = (float)i * g.sx + g.llx;
+        b = (float)j * g.sy + g.lly;
+        r = l + g.sx;
+        t = b + g.sy;
+    };
+    for (int t = 0; t < nt; t++) {
+        float llx = nl->term_llx[t], lly = nl->term_lly[t];
+        float urx = llx + nl->term_w[t], ury = lly + nl->term_h[t];
+        if (llx < g.llx || llx + nl->term_w[t] > g.urx) continue;
+        if (lly < g.lly || lly + nl->term_h[t] > g.ury) continue;
+        int i0 = (int)((llx - g.llx) / g.sx), i1 = (int)((urx - g.llx) / g.sx);
+        int j0 = (int)((lly - g.lly) / g.sy), j1 = (int)((ury - g.lly) / g.sy);
+        i1 = std::min(i1, nbx - 1);
+        j1 = std::min(j1, nby - 1);
+        for (int i = std::max(i0, 0); i <= i1; i++)
+            for (int j = std::max(j0, 0); j <= j1; j++) {
+                float l, b, r, tt;
+                bin_box(i, j, l, b, r, tt);
+                term_d[(size_t)i * nby + j] +=
+                    (float)(P.target_density * overlap_area_h(l, b, r, tt, llx, lly, urx, ury));
+            }
+    }
+    {
+        // only rows meeting a bin's y-range contribute non-zero terms; they
+        // are summed in row order, as the reference's full loop would
+        std::vector<std::vector<int>> rows_of(nby);
+        for (int j = 0; j < nby; j++) {
+            float l, b, r, t;
+            bin_box(0, j, l, b, r, t);
+            for (int rr = 0; rr < nr; rr++) {
+                double rb = nl->row_lly[rr], rt = (float)((double)nl->row_lly[rr] + nl->row_h[rr]);
+                if (overlap_len_h(b, t, rb, rt) != 0) rows_of[j].push_back(rr);
+            }
+        }
+        for (int i = 0; i < nbx; i++)
+            for (int j = 0; j < nby; j++) {
+                float l, b, r, t;
+                bin_box(i, j, l, b, r, t);
+                float avail = 0;
+                for (int rr : rows_of[j])
+                    avail += (float)overlap_area_h(l, b, r, t, nl->row_llx[rr], nl->row_lly[rr],
+                                                   nl->row_urx[rr],
+                                                   (float)((double)nl->row_lly[rr] + nl->row_h[rr]));
+                base_d[(size_t)i * nby + j] =
+                    f_equal_h(bin_area_f, avail) ? 0.0f : P.target_density * (bin_area_f - avail);
+            }
+    }
+    std::vector<float2> stat(nb);
+    for (int k = 0; k < nb; k++) stat[k] = make_float2(term_d[k], base_d[k]);
+
+    // ---- objects ----
+    e->h_size.resize(no);
+    e->h_flags.assign(no, 0);
+    std::vector<float2> pos(no + nt);
+    std::vector<float> h_area(no), h_npins(no, 0.0f);
+    for (int i = 0; i < nn; i++) {
+        e->h_size[i] = make_float2(nl->node_w[i], nl->node_h[i]);
+        h_area[i] = nl->node_w[i] * nl->node_h[i];
+        if (is_macro[i]) e->h_flags[i] |= kMacro;
+        float cx = nl->node_cx[i], cy = nl->node_cy[i];
+        clamp_center_h(g, cx, cy, nl->node_w[i], nl->node_h[i]);
+        pos[i] = make_float2(cx, cy);
+    }
+    // fillers at seeded random spots, drawn like setModuleLocation_2D_random
+    // (PlaceDB/placedb.cpp:353-379): lower-left = u * (core size - filler size)
+    for (int f = 0; f < nf; f++) {
+        int o = nn + f;
+        e->h_size[o] = make_float2(e->filler_w, e->filler_h);
+        h_area[o] = e->filler_w * e->filler_h;
+        e->h_flags[o] |= kFiller;
+        float ux = (float)((e->rng() >> 40) * (1.0 / 16777216.0));
+        float uy = (float)((e->rng() >> 40) * (1.0 / 16777216.0));
+        float llx = ux * ((g.urx - g.llx) - e->filler_w);
+        float lly = uy * ((g.ury - g.lly) - e->filler_h);
+        float cx, cy;
+        location_to_center_h(g, llx, lly, e->filler_w, e->filler_h, cx, cy);
+        pos[o] = make_float2(cx, cy);
+    }
+    for (int t = 0; t < nt; t++)
+        pos[no + t] = make_float2(nl->term_llx[t] + (float)0.5 * nl->term_w[t],
+                                  nl->term_lly[t] + (float)0.5 * nl->term_h[t]);
+    // big objects: may cover more bins than the thread-per-object path loops over
+    std::vector<int32_t> big, big_slot(no, -1);
+    for (int o = 0; o < no; o++) {
+        float w = e->h_size[o].x, h = e->h_size[o].y;
+        long sx = f_less_h(w, g.sx) ? 2 : (long)(w / g.sx) + 2;
+        long sy = f_less_h(h, g.sy) ? 2 : (long)(h / g.sy) + 2;
+        if (sx * sy > kSmallObjectBins) {
+            e->h_flags[o] |= kBig;
+            big_slot[o] = (int32_t)big.size();
+            big.push_back(o);
+        }
+    }
+
+    // ---- pins: net CSR and the object -> pin CSR (pins in id order) ----
+    std::vector<int32_t> owner(np), net_start(nnet + 1, 0);
+    std::vector<float2> off(np);
+    for (int n = 0; n <= nnet; n++) net_start[n] = nnet > 0 ? nl->net_start[n] : 0;
+    for (int p = 0; p < np; p++) {
+        int ow = nl->pin_owner[p];
+        owner[p] = ow < nn ? ow : no + (ow - nn);  // terminals follow all objects
+        off[p] = make_float2(nl->pin_dx[p], nl->pin_dy[p]);
+        if (ow < nn) h_npins[ow] += 1.0f;
+    }
+    std::vector<int32_t> ops(no + 1, 0), opins(np);
+    for (int p = 0; p < np; p++)
+        if (owner[p] < no) ops[owner[p] + 1]++;
+    for (int o = 0; o < no; o++) ops[o + 1] += ops[o];
+    {
+        std::vector<int32_t> fill(ops.begin(), ops.end() - 1);
+        for (int p = 0; p < np; p++)
+            if (owner[p] < no) opins[fill[owner[p]]++] = p;
+    }
+    std::vector<int32_t> small_nets, big_nets;
+    for (int n = 0; n < nnet; n++)
+        (net_start[n + 1] - net_start[n] <= kSmallNetDegree ? small_nets : big_nets).push_back(n);
+
+    // stage views (EPlace/eplace.cpp:190-203)
+    for (int o = 0; o < no; o++) {
+        e->h_view[EP_STAGE_MGP].push_back(o);
+        if (o >= nn) e->h_view[EP_STAGE_FILLERONLY].push_back(o);
+        if (o >= nn || !is_macro[o]) e->h_view[EP_STAGE_CGP].push_back(o);
+    }
+    e->n_cgp = (int)e->h_view[EP_STAGE_CGP].size();
+
+    // ---- fixed-point scale: every partial sum stays below 2^62 ----
+    double total_area = 0;
+    for (int o = 0; o < no; o++) total_area += (double)h_area[o];
+    int qbits = (int)std::floor(62.0 - std::log2(total_area * 1.05 + 1.0));
+    qbits = std::max(8, std::min(40, qbits));
+    KernelCtx &kc = e->kc;
+    kc.grid = g;
+    kc.qscale = std::ldexp(1.0, qbits);
+    kc.inv_qscale = std::ldexp(1.0, -qbits);
+    kc.bin_area = (double)bin_area_f;
+    kc.inv_bin_area = (double)(float)(1.0 / (double)bin_area_f);
+    kc.area_norm = (double)(sa + ma * P.target_density);
+    kc.exact_exp = P.exp_mode == EP_EXP_EXACT;
+    kc.lse = P.wl_model == EP_WL_LSE;
+
+    // ---- device ----
+    if ((s = dupload(e, e->pos, pos)) || (s = dalloc(e, e->x, no)) || (s = dalloc(e, e->g, no)) ||
+        (s = dalloc(e, e->y_prev, no)) || (s = dalloc(e, e->g_prev, no)) ||
+        (s = dupload(e, e->size, e->h_size)) || (s = dupload(e, e->pin_off, off)) ||
+        (s = dalloc(e, e->pin_grad, np)) || (s = dalloc(e, e->gd_big, big.size())) ||
+        (s = dalloc(e, e->field, nb)) || (s = dupload(e, e->static_map, stat)) ||
+        (s = dalloc(e, e->staging, no)) || (s = dalloc(e, e->flags, no)) ||
+        (s = dupload(e, e->npins, h_npins)) || (s = dupload(e, e->area, h_area)) ||
+        (s = dalloc(e, e->rho, nb)) || (s = dupload(e, e->net_start, net_start)) ||
+        (s = dupload(e, e->pin_owner, owner)) || (s = dupload(e, e->obj_pin_start, ops)) ||
+        (s = dupload(e, e->obj_pins, opins)) || (s = dupload(e, e->small_nets, small_nets)) ||
+        (s = dupload(e, e->big_nets, big_nets)) || (s = dupload(e, e->big_objs, big)) ||
+        (s = dupload(e, e->big_slot, big_slot)) || (s = dalloc(e, e->node_q, nb)) ||
+        (s = dalloc(e, e->filler_q, nb)) || (s = dalloc(e, e->S, 1)))
+        return s;
+    for (int v = 0; v < 3; v++)
+        if ((s = dupload(e, e->view_idx[v], e->h_view[v]))) return s;
+    if (P.keep_maps) {
+        if ((s = dalloc(e, e->node_f, nb)) || (s = dalloc(e, e->filler_f, nb)) ||
+            (s = dalloc(e, e->phi, nb)) || (s = dalloc(e, e->dump_gd, no)) ||
+            (s = dalloc(e, e->dump_gwl, no)))
+            return s;
+    }
+    CK(cudaMemset(e->node_q, 0, sizeof(unsigned long long) * nb));
+    CK(cudaMemset(e->filler_q, 0, sizeof(unsigned long long) * nb));
+    CK(cudaMemset(e->g, 0, sizeof(float2) * no));
+    CK(cudaMemset(e->g_prev, 0, sizeof(float2) * no));
+    CK(cudaMemset(e->y_prev, 0, sizeof(float2) * no));
+    CK(cudaMemset(e->x, 0, sizeof(float2) * no));
+    CK(cudaMemset(e->pin_grad, 0, sizeof(float2) * std::max(np, 1)));
+    CK(cudaMallocHost((void **)&e->hS, sizeof(DevScalars)));
+    std::memset(e->hS, 0, sizeof(DevScalars));
+    e->hS->a = 1.0;
+    e->hS->stage = EP_STAGE_MGP;
+    e->hS->max_iter = P.max_iterations > 0 ? P.max_iterations : 1000;
+    e->hS->target_overflow = P.target_overflow > 0 ? P.target_overflow : 0.10f;
+    e->hS->step_rule = P.step_rule;
+    CK(cudaMemcpy(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice));
+
+    DeviceNetlist &d = e->dn;
+    d.n_obj = no;
+    d.n_nodes = nn;
+    d.n_terms = nt;
+    d.n_nets = nnet;
+    d.n_pins = np;
+    d.pos = e->pos;
+    d.size = e->size;
+    d.flags = e->flags;
+    d.npins = e->npins;
+    d.area = e->area;
+    d.net_start = e->net_start;
+    d.pin_owner = e->pin_owner;
+    d.pin_off = e->pin_off;
+    d.obj_pin_start = e->obj_pin_start;
+    d.obj_pins = e->obj_pins;
+    d.small_nets = e->small_nets;
+    d.big_nets = e->big_nets;
+    d.n_small_nets = (int)small_nets.size();
+    d.n_big_nets = (int)big_nets.size();
+    d.big_objs = e->big_objs;
+    d.big_slot = e->big_slot;
+    d.n_big_objs = (int)big.size();
+    if ((s = dalloc(e, kc.part_prep, (size_t)prep_blocks(g))) ||
+        (s = dalloc(e, kc.part_wl, (size_t)2 * std::max(1, reduction_blocks(d, 0)))) ||
+        (s = dalloc(e, kc.part_comb, (size_t)5 * std::max(1, reduction_blocks(d, 1)))) ||
+        (s = dalloc(e, kc.part_hp, (size_t)2 * std::max(1, reduction_blocks(d, 0)))))
+        return s;
+
+    int rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, P.dct_mode, e->err);
+    if (rc) return (ep_status)rc;
+    e->stage = EP_STAGE_MGP;
+    s = upload_view(e, EP_STAGE_MGP);
+    if (s) return s;
+    CK(cudaDeviceSynchronize());
+    return EP_OK;
+}
+
+void ep_destroy(ep_engine *e) {
+    if (!e) return;
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    dct_plan_free(e->dct);
+    for (void *p : e->allocs) cudaFree(p);
+    if (e->hS) cudaFreeHost(e->hS);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->own_stream && e->st) cudaStreamDestroy(e->st);
+    delete e;
+}
+
+ep_status ep_get_info(const ep_engine *e, ep_info *info) {
+    if (!e || !info) return EP_ERR_ARG;
+    info->num_nodes = e->n_nodes;
+    info->num_fillers = e->n_fillers;
+    info->num_objects = e->n_obj;
+    info->num_terminals = e->n_terms;
+    info->num_nets = e->n_nets;
+    info->num_pins = e->n_pins;
+    info->num_macros = e->n_macros;
+    info->num_cells_and_fillers = e->n_cgp;
+    info->bins_x = e->grid.nx;
+    info->bins_y = e->grid.ny;
+    info->bin_step_x = e->grid.sx;
+    info->bin_step_y = e->grid.sy;
+    info->core_llx = e->grid.llx;
+    info->core_lly = e->grid.lly;
+    info->core_urx = e->grid.urx;
+    info->core_ury = e->grid.ury;
+    info->filler_w = e->filler_w;
+    info->filler_h = e->filler_h;
+    info->std_area = e->std_area;
+    info->macro_area = e->macro_area;
+    info->total_row_area = e->total_row_area;
+    info->density_scale = e->kc.qscale;
+    return EP_OK;
+}
+
+ep_status ep_set_stream(ep_engine *e, void *stream) {
+    if (!e) return EP_ERR_ARG;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    if (stream) {
+        if (e->own_stream && e->st) cudaStreamDestroy(e->st);
+        e->st = (cudaStream_t)stream;
+        e->own_stream = false;
+    } else if (!e->own_stream) {
+        CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        e->own_stream = true;
+    }
+    return EP_OK;
+}
+
+ep_status ep_synchronize(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count) {
+    if (!e || !xy) return EP_ERR_ARG;
+    ep_status s = check_view(e, view, count);
+    if (s) return s;
+    if (count == 0) return EP_OK;
+    k_gather_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->view_idx[view], count, e->pos, e->staging);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(xy, e->staging, sizeof(float2) * count, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count) {
+    if (!e || !xy) return EP_ERR_ARG;
+    ep_status s = check_view(e, view, count);
+    if (s) return s;
+    if (count == 0) return EP_OK;
+    CK(cudaMemcpyAsync(e->staging, xy, sizeof(float2) * count, cudaMemcpyHostToDevice, e->st));
+    k_scatter_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[view], count,
+                                                           e->staging, e->size, e->pos);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_eval_gradient(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    enqueue_eval(e, 0);
+    CK(cudaGetLastError());
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    return device_status(e);
+}
+
+ep_status ep_initialize(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    ep_status s = update_scalars(e, [](DevScalars &h) {
+        h.lambda0_mode = 1;
+        h.lambda = 0.0;
+        h.status = 0;
+        h.done = 0;
+    });
+    if (s) return s;
+    enqueue_eval(e, 0);
+    CK(cudaGetLastError());
+    s = fetch_scalars(e);
+    if (s) return s;
+    e->initialized = true;
+    return device_status(e);
+}
+
+ep_status ep_get_gradient(ep_engine *e, int32_t view, float *xy, int32_t count) {
+    if (!e || !xy) return EP_ERR_ARG;
+    ep_status s = check_view(e, view, count);
+    if (s) return s;
+    if (count == 0) return EP_OK;
+    k_gather_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->view_idx[view], count, e->g, e->staging);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(xy, e->staging, sizeof(float2) * count, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wirelength_xy) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->prm.keep_maps) {
+        e->err = "component gradients need keep_maps";
+        return EP_ERR_STATE;
+    }
+    if (density_xy)
+        CK(cudaMemcpyAsync(density_xy, e->dump_gd, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+    if (wirelength_xy)
+        CK(cudaMemcpyAsync(wirelength_xy, e->dump_gwl, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *terminal, float *base,
+                          float *ex, float *ey, float *phi) {
+    if (!e) return EP_ERR_ARG;
+    const int nb = e->grid.nx * e->grid.ny;
+    if ((node || filler || ex || ey || phi) && !e->prm.keep_maps) {
+        e->err = "node/filler/field maps need keep_maps";
+        return EP_ERR_STATE;
+    }
+    if (node) CK(cudaMemcpyAsync(node, e->node_f, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+    if (filler) CK(cudaMemcpyAsync(filler, e->filler_f, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+    if (phi) CK(cudaMemcpyAsync(phi, e->phi, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+    std::vector<float2> tmp;
+    if (terminal || base || ex || ey) tmp.resize(nb);
+    if (terminal || base) {
+        CK(cudaMemcpyAsync(tmp.data(), e->static_map, sizeof(float2) * nb, cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        for (int k = 0; k < nb; k++) {
+            if (terminal) terminal[k] = tmp[k].x;
+            if (base) base[k] = tmp[k].y;
+        }
+    }
+    if (ex || ey) {
+        CK(cudaMemcpyAsync(tmp.data(), e->field, sizeof(float2) * nb, cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        for (int k = 0; k < nb; k++) {
+            if (ex) ex[k] = tmp[k].x;
+            if (ey) ey[k] = tmp[k].y;
+        }
+    }
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_get_density_fixed(ep_engine *e, int64_t *node, int64_t *filler) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->prm.keep_maps) {
+        e->err = "fixed-point maps need keep_maps";
+        return EP_ERR_STATE;
+    }
+    const int nb = e->grid.nx * e->grid.ny;
+    if (node) CK(cudaMemcpyAsync(node, e->node_q, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, e->st));
+    if (filler) CK(cudaMemcpyAsync(filler, e->filler_q, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_query(ep_engine *e, ep_scalars *out) {
+    if (!e || !out) return EP_ERR_ARG;
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    const DevScalars &h = *e->hS;
+    out->overflow = h.tau;
+    out->lambda = h.lambda;
+    out->hpwl = h.hpwl;
+    out->last_hpwl = h.last_hpwl;
+    out->inv_gamma_x = h.inv_gamma_x;
+    out->inv_gamma_y = h.inv_gamma_y;
+    out->wirelength = h.wirelength;
+    out->step = h.step;
+    out->ns_param = h.a;
+    out->iteration = h.iter;
+    out->stage = h.stage;
+    out->mgp_iterations = h.mgp_iterations;
+    out->done = h.done;
+    return device_status(e);
+}
+
+ep_status ep_set_lambda(ep_engine *e, double lambda) {
+    if (!e) return EP_ERR_ARG;
+    return update_scalars(e, [lambda](DevScalars &h) { h.lambda = lambda; });
+}
+
+ep_status ep_penalty_init(ep_engine *e) {
+    // lambda_0 from the component gradients of the last evaluation needs them
+    // resident; the engine computes it inside ep_initialize's evaluation.
+    if (!e) return EP_ERR_ARG;
+    ep_status s = update_scalars(e, [](DevScalars &h) { h.lambda0_mode = 1; });
+    if (s) return s;
+    enqueue_eval(e, 0);
+    CK(cudaGetLastError());
+    s = fetch_scalars(e);
+    if (s) return s;
+    return device_status(e);
+}
+
+ep_status ep_penalty_update(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    launch_hpwl(e->kc, e->dn, 1, e->S, e->st);
+    CK(cudaGetLastError());
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    return device_status(e);
+}
+
+ep_status ep_hpwl(ep_engine *e, double *hpwl) {
+    if (!e || !hpwl) return EP_ERR_ARG;
+    launch_hpwl(e->kc, e->dn, 0, e->S, e->st);
+    CK(cudaGetLastError());
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    *hpwl = e->hS->hpwl_query;
+    return EP_OK;
+}
+
+ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy) {
+    if (!e) return EP_ERR_ARG;
+    if (stage < 0 || stage > 2) {
+        e->err = "unknown stage";
+        return EP_ERR_ARG;
+    }
+    ep_status s;
+    if (stage == EP_STAGE_FILLERONLY && e->n_fillers > 0) {
+        // switch2FillerOnly: fillers re-spread at random (EPlace/eplace.cpp:887-894)
+        std::vector<float2> fp(e->n_fillers);
+        for (int f = 0; f < e->n_fillers; f++) {
+            float llx, lly;
+            if (filler_xy) {
+                llx = filler_xy[2 * f];
+                lly = filler_xy[2 * f + 1];
+            } else {
+                float ux = (float)((e->rng() >> 40) * (1.0 / 16777216.0));
+                float uy = (float)((e->rng() >> 40) * (1.0 / 16777216.0));
+                llx = ux * ((e->grid.urx - e->grid.llx) - e->filler_w);
+                lly = uy * ((e->grid.ury - e->grid.lly) - e->filler_h);
+            }
+            float cx, cy;
+            location_to_center_h(e->grid, llx, lly, e->filler_w, e->filler_h, cx, cy);
+            fp[f] = make_float2(cx, cy);
+        }
+        CK(cudaMemcpyAsync(e->pos + e->n_nodes, fp.data(), sizeof(float2) * e->n_fillers,
+                           cudaMemcpyHostToDevice, e->st));
+    }
+    s = update_scalars(e, [stage](DevScalars &h) {
+        if (stage == EP_STAGE_CGP) h.lambda = h.lambda / std::pow(1.1, h.mgp_iterations * 0.1);
+        h.stage = stage;
+    });
+    if (s) return s;
+    e->stage = stage;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    return upload_view(e, stage);
+}
+
+ep_status ep_nesterov_begin(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->initialized) {
+        e->err = "ep_initialize must run before the optimizer";
+        return EP_ERR_STATE;
+    }
+    ep_status s = update_scalars(e, [](DevScalars &h) { h.step_cap = 0; });
+    if (s) return s;
+    launch_stage_begin(e->dn, e->pos, e->x, e->S, e->st);
+    CK(cudaGetLastError());
+    e->in_run = true;
+    return EP_OK;
+}
+
+ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->in_run) {
+        e->err = "ep_nesterov_begin must run first";
+        return EP_ERR_STATE;
+    }
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    if (e->hS->done) {
+        if (stopped) *stopped = 1;
+        return device_status(e);
+    }
+    if (stopped) *stopped = 0;
+    if (e->prm.step_rule == EP_STEP_BKTRK) {
+        e->err = "backtracking step runs through ep_nesterov_run only";
+        return EP_ERR_UNSUPPORTED;
+    }
+    enqueue_step(e);
+    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);  // updatePenaltyFactor
+    CK(cudaGetLastError());
+    s = fetch_scalars(e);
+    if (s) return s;
+    return device_status(e);
+}
+
+ep_status ep_nesterov_end(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->in_run) return EP_OK;
+    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);
+    launch_wrap_up(e->kc, e->dn, e->pos, e->x, e->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(e->st));
+    e->in_run = false;
+    return EP_OK;
+}
+
+ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) {
+    if (!e) return EP_ERR_ARG;
+    ep_status s = ep_nesterov_begin(e);
+    if (s) return s;
+    s = update_scalars(e, [max_steps](DevScalars &h) { h.step_cap = max_steps > 0 ? max_steps : 0; });
+    if (s) return s;
+    const int K = 8;
+    if (!e->graph || e->graph_iters != K) {
+        s = build_graph(e, K);
+        if (s) return s;
+    }
+    CK(cudaEventRecord(e->ev0, e->st));
+    const int cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + K;
+    int launched = 0;
+    while (true) {
+        CK(cudaGraphLaunch(e->graph, e->st));
+        launched += K;
+        CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        if (e->hS->done || launched > cap + K) break;
+    }
+    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);  // the lambda update owed by the last step
+    launch_wrap_up(e->kc, e->dn, e->pos, e->x, e->st);
+    CK(cudaEventRecord(e->ev1, e->st));
+    launch_hpwl(e->kc, e->dn, 0, e->S, e->st);
+    CK(cudaGetLastError());
+    s = fetch_scalars(e);
+    e->in_run = false;
+    if (s) return s;
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+        stats->iterations = e->hS->iter;
+        stats->overflow = e->hS->tau;
+        stats->hpwl = e->hS->hpwl_query;
+        stats->lambda = e->hS->lambda;
+        stats->seconds = ms * 1e-3;
+    }
+    return device_status(e);
+}
+
+}  // extern "C"

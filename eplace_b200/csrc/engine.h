@@ -1,0 +1,98 @@
+// engine.h -- internal declarations shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/eplace_gpu.h"
+#include "common.cuh"
+
+namespace ep {
+
+// Nets up to this degree take the thread-per-net path (sequential float sums
+// in pin order, as Net::calcWirelengthWA_2D does); larger nets a warp each.
+constexpr int kSmallNetDegree = 16;
+// Objects whose bin footprint may exceed this many bins take the
+// block-per-object scatter / gather path.
+constexpr int kSmallObjectBins = 16;
+
+// ---- DCT / Poisson plan (dct.cu, dct_tc.cu) ---------------------------------
+struct DctPlan {
+    int nx = 0, ny = 0;
+    int mode = 0;  // ep_dct_mode
+    // FP32 operand tables (see dct.cu for their definitions)
+    float *Cy = nullptr, *Cx = nullptr, *K = nullptr, *B3 = nullptr, *A4 = nullptr;
+    // intermediates
+    float *Tt = nullptr, *P = nullptr, *T3 = nullptr;
+    // tensor-core path (bf16 hi/lo planes + TMA descriptors), dct_tc.cu
+    void *tc = nullptr;
+};
+
+int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode,
+                  std::string &err);
+void dct_plan_free(DctPlan &p);
+// rho (fp32 [nx][ny]) -> field (float2 [nx][ny]) and, when phi != nullptr, phi.
+int dct_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S,
+            cudaStream_t st);
+// The tensor-core path reads rho as bf16 hi/lo planes written by the prep kernel.
+void *dct_tc_rho_planes(DctPlan &p);
+
+// ---- kernels (kernels.cu) ---------------------------------------------------
+struct DeviceNetlist {
+    int n_obj, n_nodes, n_terms;
+    int n_nets, n_pins;
+    const float2 *pos;       // [n_obj + n_terms] centres; terminals after objects
+    const float2 *size;      // [n_obj] (w, h)
+    const uint8_t *flags;    // [n_obj]
+    const float *npins;      // [n_obj] pin count (float, as the preconditioner reads it)
+    const float *area;       // [n_obj] Module::area
+    const int32_t *net_start, *pin_owner;
+    const float2 *pin_off;
+    const int32_t *obj_pin_start, *obj_pins;
+    const int32_t *small_nets, *big_nets;
+    int n_small_nets, n_big_nets;
+    const int32_t *big_objs;  // indices of kBig objects
+    const int32_t *big_slot;  // object -> index in big_objs (or -1)
+    int n_big_objs;
+};
+
+struct KernelCtx {
+    Grid grid;
+    double qscale, inv_qscale;
+    double bin_area, inv_bin_area;
+    double area_norm;  // stdArea + macroArea * td (overflow denominator)
+    int exact_exp, lse;
+    // per-block partials of the deterministic grid reductions
+    double *part_prep, *part_wl, *part_comb, *part_hp;
+};
+int prep_blocks(const Grid &g);
+// grid sizes of the reductions: 0 = per-net passes (both kernels), 1 = combine
+int reduction_blocks(const DeviceNetlist &d, int which);
+
+void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, unsigned long long *node_q,
+                    unsigned long long *filler_q, const DevScalars *S, cudaStream_t st);
+void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long long *filler_q,
+                 const float2 *static_map, float *rho, void *rho_bf16, float *node_f,
+                 float *filler_f, int zero_maps, DevScalars *S, cudaStream_t st);
+void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad,
+                       DevScalars *S, cudaStream_t st);
+void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
+                       float2 *gd_big, const DevScalars *S, cudaStream_t st);
+void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
+                    const float2 *gd_big, const float2 *pin_grad, float2 *g, const float2 *g_prev,
+                    const float2 *y_prev, float2 *dump_gd, float2 *dump_gwl, int stepping,
+                    DevScalars *S, cudaStream_t st);
+void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
+                   const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S, cudaStream_t st);
+void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
+                        cudaStream_t st);
+void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, const float2 *x,
+                    cudaStream_t st);
+// HPWL at the current positions; mode 0 stores it, mode 1 also applies the
+// updatePenaltyFactor rule, mode 2 applies it only if a lambda update is pending.
+void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
+                 cudaStream_t st);
+
+}  // namespace ep

@@ -1,0 +1,381 @@
+"""Host-side mirror of the reference's global-placement call surface.
+
+``EPlacer2D`` keeps the method names of EPlacer_2D (EPlace/eplace.h:95-200) and
+``EplaceNesterovOpt`` those of the optimizer (Optimization/nesterov.hpp:59-77,
+Optimization/opt.hpp:19-36), so a driver written against the reference
+(main/ePlace_main.cpp:141-211) reads the same.  Every call goes through the
+C-ABI of include/eplace_gpu.h into ``libeplace_b200.so``; there is no CPU
+fallback: without the CUDA library or a GPU the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libeplace_b200.so")
+
+EP_OK, EP_ERR_ARG, EP_ERR_CUDA, EP_ERR_NAN, EP_ERR_TIMEOUT, EP_ERR_STATE, EP_ERR_NOMEM, EP_ERR_UNSUPPORTED = range(8)
+STATUS_NAMES = ["EP_OK", "EP_ERR_ARG", "EP_ERR_CUDA", "EP_ERR_NAN", "EP_ERR_TIMEOUT", "EP_ERR_STATE",
+                "EP_ERR_NOMEM", "EP_ERR_UNSUPPORTED"]
+MGP, FILLERONLY, CGP = 0, 1, 2
+WL_WA, WL_LSE = 0, 1
+EXP_FAST, EXP_EXACT = 0, 1
+STEP_LIPSCHITZ, STEP_BB, STEP_BKTRK = 0, 1, 2
+DCT_FP32, DCT_BF16X3 = 0, 1
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class EPError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else status}: {msg}")
+
+
+class Netlist(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int32), ("num_terminals", ctypes.c_int32),
+                ("num_nets", ctypes.c_int32), ("num_rows", ctypes.c_int32),
+                ("node_w", _f32p), ("node_h", _f32p), ("node_cx", _f32p), ("node_cy", _f32p),
+                ("term_llx", _f32p), ("term_lly", _f32p), ("term_w", _f32p), ("term_h", _f32p),
+                ("term_is_ni", _u8p), ("net_start", _i32p), ("pin_owner", _i32p),
+                ("pin_dx", _f32p), ("pin_dy", _f32p), ("row_llx", _f32p), ("row_lly", _f32p),
+                ("row_urx", _f32p), ("row_h", _f32p), ("common_row_height", ctypes.c_float)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("target_density", ctypes.c_float), ("target_overflow", ctypes.c_float),
+                ("bins_x", ctypes.c_int32), ("bins_y", ctypes.c_int32),
+                ("max_iterations", ctypes.c_int32), ("wl_model", ctypes.c_int32),
+                ("exp_mode", ctypes.c_int32), ("step_rule", ctypes.c_int32),
+                ("dct_mode", ctypes.c_int32), ("filler_seed", ctypes.c_uint64),
+                ("device", ctypes.c_int32), ("keep_maps", ctypes.c_int32)]
+
+
+class Scalars(ctypes.Structure):
+    _fields_ = [("overflow", ctypes.c_double), ("lambda_", ctypes.c_double), ("hpwl", ctypes.c_double),
+                ("last_hpwl", ctypes.c_double), ("inv_gamma_x", ctypes.c_double),
+                ("inv_gamma_y", ctypes.c_double), ("wirelength", ctypes.c_double),
+                ("step", ctypes.c_double), ("ns_param", ctypes.c_double),
+                ("iteration", ctypes.c_int32), ("stage", ctypes.c_int32),
+                ("mgp_iterations", ctypes.c_int32), ("done", ctypes.c_int32)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int32), ("num_fillers", ctypes.c_int32),
+                ("num_objects", ctypes.c_int32), ("num_terminals", ctypes.c_int32),
+                ("num_nets", ctypes.c_int32), ("num_pins", ctypes.c_int32),
+                ("num_macros", ctypes.c_int32), ("num_cells_and_fillers", ctypes.c_int32),
+                ("bins_x", ctypes.c_int32), ("bins_y", ctypes.c_int32),
+                ("bin_step_x", ctypes.c_float), ("bin_step_y", ctypes.c_float),
+                ("core_llx", ctypes.c_float), ("core_lly", ctypes.c_float),
+                ("core_urx", ctypes.c_float), ("core_ury", ctypes.c_float),
+                ("filler_w", ctypes.c_float), ("filler_h", ctypes.c_float),
+                ("std_area", ctypes.c_double), ("macro_area", ctypes.c_double),
+                ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double)]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("overflow", ctypes.c_double),
+                ("hpwl", ctypes.c_double), ("lambda_", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+# every symbol include/eplace_gpu.h declares
+EXPORTS = (
+    "ep_default_params", "ep_abi_version", "ep_create", "ep_destroy", "ep_last_error", "ep_get_info",
+    "ep_set_stream", "ep_synchronize", "ep_get_positions", "ep_set_positions", "ep_initialize",
+    "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
+    "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
+    "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
+    "ep_nesterov_end",
+)
+
+_lib = None
+
+
+def load():
+    """Load the engine library; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m eplace_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.ep_default_params.argtypes = [ctypes.POINTER(Params)]
+    L.ep_default_params.restype = None
+    L.ep_abi_version.restype = ctypes.c_int32
+    L.ep_create.argtypes = [ctypes.POINTER(Netlist), ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.ep_destroy.argtypes = [vp]
+    L.ep_destroy.restype = None
+    L.ep_last_error.argtypes = [vp]
+    L.ep_last_error.restype = ctypes.c_char_p
+    L.ep_get_info.argtypes = [vp, ctypes.POINTER(Info)]
+    L.ep_set_stream.argtypes = [vp, vp]
+    L.ep_synchronize.argtypes = [vp]
+    for n in ("ep_get_positions", "ep_set_positions", "ep_get_gradient"):
+        getattr(L, n).argtypes = [vp, ctypes.c_int32, _f32p, ctypes.c_int32]
+    for n in ("ep_initialize", "ep_eval_gradient", "ep_penalty_init", "ep_penalty_update",
+              "ep_nesterov_begin", "ep_nesterov_end"):
+        getattr(L, n).argtypes = [vp]
+    L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
+    L.ep_get_bin_maps.argtypes = [vp] + [_f32p] * 7
+    L.ep_get_density_fixed.argtypes = [vp, _i64p, _i64p]
+    L.ep_query.argtypes = [vp, ctypes.POINTER(Scalars)]
+    L.ep_set_lambda.argtypes = [vp, ctypes.c_double]
+    L.ep_hpwl.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ep_switch_stage.argtypes = [vp, ctypes.c_int32, _f32p]
+    L.ep_nesterov_run.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(RunStats)]
+    L.ep_nesterov_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    _lib = L
+    return L
+
+
+def default_params(**kw):
+    p = Params()
+    load().ep_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class Engine:
+    """One ep_engine handle (device-resident netlist and placer state)."""
+
+    def __init__(self, nl, params=None, **kw):
+        L = load()
+        self._L = L
+        if params is None:
+            params = default_params(target_density=float(nl.target_density),
+                                    bins_x=int(nl.bins), bins_y=int(nl.bins))
+        for k, v in kw.items():
+            setattr(params, k, v)
+        self.params = params
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        self._keep = k = dict(
+            node_w=f(nl.node_w), node_h=f(nl.node_h), node_cx=f(nl.node_cx), node_cy=f(nl.node_cy),
+            term_llx=f(nl.term_llx), term_lly=f(nl.term_lly), term_w=f(nl.term_w), term_h=f(nl.term_h),
+            term_ni=np.ascontiguousarray(nl.term_is_ni, dtype=np.uint8),
+            net_start=np.ascontiguousarray(nl.net_start, dtype=np.int32),
+            pin_owner=np.ascontiguousarray(nl.pin_owner, dtype=np.int32),
+            pin_dx=f(nl.pin_dx), pin_dy=f(nl.pin_dy), row_llx=f(nl.row_llx), row_lly=f(nl.row_lly),
+            row_urx=f(nl.row_urx), row_h=f(nl.row_h))
+        c = Netlist(nl.num_nodes, nl.num_terminals, nl.num_nets, nl.num_rows,
+                    _p(k["node_w"], _f32p), _p(k["node_h"], _f32p), _p(k["node_cx"], _f32p),
+                    _p(k["node_cy"], _f32p), _p(k["term_llx"], _f32p), _p(k["term_lly"], _f32p),
+                    _p(k["term_w"], _f32p), _p(k["term_h"], _f32p), _p(k["term_ni"], _u8p),
+                    _p(k["net_start"], _i32p), _p(k["pin_owner"], _i32p), _p(k["pin_dx"], _f32p),
+                    _p(k["pin_dy"], _f32p), _p(k["row_llx"], _f32p), _p(k["row_lly"], _f32p),
+                    _p(k["row_urx"], _f32p), _p(k["row_h"], _f32p), 0.0)
+        h = ctypes.c_void_p()
+        rc = L.ep_create(ctypes.byref(c), ctypes.byref(params), ctypes.byref(h))
+        self.h = h
+        if rc != EP_OK:
+            msg = L.ep_last_error(h).decode() if h.value else "ep_create failed"
+            self.close()
+            raise EPError(rc, msg)
+        self.info = Info()
+        self._check(L.ep_get_info(self.h, ctypes.byref(self.info)))
+
+    def _check(self, rc):
+        if rc != EP_OK:
+            raise EPError(rc, self._L.ep_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self._L.ep_destroy(self.h)
+        self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- sizes ----
+    def view_size(self, view):
+        i = self.info
+        return [i.num_objects, i.num_fillers, i.num_cells_and_fillers][view]
+
+    # ---- wrappers ----
+    def get_positions(self, view=MGP):
+        n = self.view_size(view)
+        xy = np.zeros((n, 2), np.float32)
+        self._check(self._L.ep_get_positions(self.h, view, _p(xy, _f32p), n))
+        return xy
+
+    def set_positions(self, xy, view=MGP):
+        xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+        self._check(self._L.ep_set_positions(self.h, view, _p(xy, _f32p), xy.shape[0]))
+
+    def get_gradient(self, view=MGP):
+        n = self.view_size(view)
+        g = np.zeros((n, 2), np.float32)
+        self._check(self._L.ep_get_gradient(self.h, view, _p(g, _f32p), n))
+        return g
+
+    def component_gradients(self):
+        n = self.info.num_objects
+        gd = np.zeros((n, 2), np.float32)
+        gw = np.zeros((n, 2), np.float32)
+        self._check(self._L.ep_get_component_gradients(self.h, _p(gd, _f32p), _p(gw, _f32p)))
+        return gd, gw
+
+    def bin_maps(self, which=("node", "filler", "terminal", "base", "ex", "ey", "phi")):
+        nx, ny = self.info.bins_x, self.info.bins_y
+        out = {k: np.zeros((nx, ny), np.float32) for k in which}
+        args = [_p(out[k], _f32p) if k in out else None
+                for k in ("node", "filler", "terminal", "base", "ex", "ey", "phi")]
+        self._check(self._L.ep_get_bin_maps(self.h, *args))
+        return out
+
+    def density_fixed(self):
+        nx, ny = self.info.bins_x, self.info.bins_y
+        a = np.zeros((nx, ny), np.int64)
+        b = np.zeros((nx, ny), np.int64)
+        self._check(self._L.ep_get_density_fixed(self.h, _p(a, _i64p), _p(b, _i64p)))
+        return a, b
+
+    def query(self):
+        s = Scalars()
+        self._check(self._L.ep_query(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in Scalars._fields_}
+
+    def initialize(self):
+        self._check(self._L.ep_initialize(self.h))
+
+    def eval_gradient(self):
+        self._check(self._L.ep_eval_gradient(self.h))
+
+    def set_lambda(self, v):
+        self._check(self._L.ep_set_lambda(self.h, float(v)))
+
+    def penalty_init(self):
+        self._check(self._L.ep_penalty_init(self.h))
+
+    def penalty_update(self):
+        self._check(self._L.ep_penalty_update(self.h))
+
+    def hpwl(self):
+        v = ctypes.c_double()
+        self._check(self._L.ep_hpwl(self.h, ctypes.byref(v)))
+        return v.value
+
+    def switch_stage(self, stage, filler_ll=None):
+        a = None if filler_ll is None else np.ascontiguousarray(filler_ll, np.float32)
+        self._check(self._L.ep_switch_stage(self.h, stage, _p(a, _f32p)))
+
+    def nesterov_run(self, max_steps=0):
+        st = RunStats()
+        self._check(self._L.ep_nesterov_run(self.h, int(max_steps), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in RunStats._fields_}
+
+    def nesterov_begin(self):
+        self._check(self._L.ep_nesterov_begin(self.h))
+
+    def nesterov_step(self):
+        stopped = ctypes.c_int32(0)
+        self._check(self._L.ep_nesterov_step(self.h, ctypes.byref(stopped)))
+        return bool(stopped.value)
+
+    def nesterov_end(self):
+        self._check(self._L.ep_nesterov_end(self.h))
+
+    def synchronize(self):
+        self._check(self._L.ep_synchronize(self.h))
+
+
+class EPlacer2D:
+    """EPlacer_2D's call surface (EPlace/eplace.h:164-194) over one Engine."""
+
+    def __init__(self, netlist, **params):
+        self.netlist = netlist
+        self._params = params
+        self.targetDensity = float(params.pop("target_density", netlist.target_density))
+        self.engine = None
+
+    def setTargetDensity(self, v):
+        self.targetDensity = float(v)
+
+    # initialization(): fillers + bins (ep_create), first gradient, lambda_0
+    def initialization(self):
+        nl = self.netlist
+        p = default_params(target_density=self.targetDensity, bins_x=int(nl.bins), bins_y=int(nl.bins))
+        for k, v in self._params.items():
+            setattr(p, k, v)
+        self.engine = Engine(nl, p)
+        self.engine.initialize()
+
+    def totalGradientUpdate(self):
+        self.engine.eval_gradient()
+
+    def getGradient(self):
+        return self.engine.get_gradient(self.placementStage)
+
+    def getPosition(self):
+        return self.engine.get_positions(self.placementStage)
+
+    def setPosition(self, xy):
+        self.engine.set_positions(xy, self.placementStage)
+
+    def penaltyFactorInitilization(self):
+        self.engine.penalty_init()
+
+    def updatePenaltyFactor(self):
+        self.engine.penalty_update()
+
+    def switch2FillerOnly(self, filler_ll=None):
+        self.engine.switch_stage(FILLERONLY, filler_ll)
+
+    def switch2cGP(self):
+        self.engine.switch_stage(CGP)
+
+    def showInfo(self):
+        s = self.engine.query()
+        print(f"Overflow: {s['overflow']}\npenalty factor: {s['lambda_']:.6f}\nHPWL: {s['last_hpwl']}\n")
+
+    # public fields read by callers (EPlace/eplace.h:108-136)
+    @property
+    def globalDensityOverflow(self):
+        return self.engine.query()["overflow"]
+
+    @property
+    def lambda_(self):
+        return self.engine.query()["lambda_"]
+
+    @property
+    def placementStage(self):
+        return self.engine.query()["stage"]
+
+    @property
+    def mGPIterationCount(self):
+        return self.engine.query()["mgp_iterations"]
+
+    @property
+    def binDimension(self):
+        return (self.engine.info.bins_x, self.engine.info.bins_y)
+
+    @property
+    def binStep(self):
+        return (self.engine.info.bin_step_x, self.engine.info.bin_step_y)
+
+
+class EplaceNesterovOpt:
+    """FirstOrderOptimizer<T>::opt with EplaceNesterovOpt's steps
+    (Optimization/opt.hpp:30-36, Optimization/nesterov.hpp:86-415); the loop
+    itself runs on the device."""
+
+    def __init__(self, placer):
+        self.placer = placer
+        self.last_run = None
+
+    def opt(self, max_steps=0):
+        self.last_run = self.placer.engine.nesterov_run(max_steps)
+        return self.last_run

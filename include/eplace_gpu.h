@@ -1,0 +1,204 @@
+/* eplace_gpu.h -- C-ABI of the B200-native ePlace global-placement engine.
+ *
+ * Drop-in boundary for the Xinyu-lumos/ePlace global-placement inner loop.
+ * Each entry point names the reference interface it replaces.  The engine
+ * owns all device memory; inputs and outputs at this boundary are plain host
+ * arrays (positions and gradients are centres, interleaved x,y, float32).
+ * Every call returns an ep_status; the engine never calls exit() and never
+ * traps the GPU.  One host thread per engine handle; all work is ordered on
+ * the engine's CUDA stream (ep_set_stream).
+ *
+ * Object order follows the reference (EPlace/eplace.cpp:190-203): the
+ * movable nodes of the netlist (dbNodes order), then the fillers the engine
+ * creates.  Stage views (ep_stage) pick subsets of that order exactly as
+ * EPlacer_2D::getPosition / getGradient do (EPlace/eplace.cpp:742-773).
+ */
+#ifndef EPLACE_GPU_H
+#define EPLACE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EP_ABI_VERSION 1
+
+typedef enum ep_status {
+    EP_OK = 0,
+    EP_ERR_ARG = 1,     /* bad argument or netlist */
+    EP_ERR_CUDA = 2,    /* a CUDA call failed (see ep_last_error) */
+    EP_ERR_NAN = 3,     /* a non-finite value appeared in a reduction */
+    EP_ERR_TIMEOUT = 4, /* a bounded device wait gave up */
+    EP_ERR_STATE = 5,   /* call out of order (e.g. step before initialize) */
+    EP_ERR_NOMEM = 6,   /* device allocation failed */
+    EP_ERR_UNSUPPORTED = 7
+} ep_status;
+
+/* PLACEMENT_STAGE, EPlace/eplace.h:21-27. */
+typedef enum ep_stage { EP_STAGE_MGP = 0, EP_STAGE_FILLERONLY = 1, EP_STAGE_CGP = 2 } ep_stage;
+
+/* Wirelength model: WA (default) or LSE (gArg "LSE", EPlace/eplace.cpp:512-549). */
+typedef enum ep_wl_model { EP_WL_WA = 0, EP_WL_LSE = 1 } ep_wl_model;
+
+/* Exponential used by the wirelength model: the reference's fastExp
+ * (1+a/1024)^1024 (PlaceCommon/global.h:457-471) or the exact exp. */
+typedef enum ep_exp_mode { EP_EXP_FAST = 0, EP_EXP_EXACT = 1 } ep_exp_mode;
+
+/* Step rule of EplaceNesterovOpt::opt_step (Optimization/nesterov.hpp:151-168):
+ * 1/L (default), Barzilai-Borwein (gArg "bb"), backtracking (gArg "bktrk"). */
+typedef enum ep_step_rule { EP_STEP_LIPSCHITZ = 0, EP_STEP_BB = 1, EP_STEP_BKTRK = 2 } ep_step_rule;
+
+/* Arithmetic of the DCT/IDCT Poisson solve (replaces FFT_2D::doFFT,
+ * FFT/fft.cpp:191-284): dense GEMMs in FP32 on the CUDA cores, or on the
+ * tcgen05 tensor cores with 3xBF16 split products (FP32 accumulate). */
+typedef enum ep_dct_mode { EP_DCT_FP32 = 0, EP_DCT_BF16X3 = 1 } ep_dct_mode;
+
+/* Netlist in plain arrays (what Parser/parser.cpp:44-97 builds into PlaceDB).
+ * Nodes are movable; a node is a macro iff its height exceeds
+ * common_row_height (PlaceDB/placedb.cpp:96-114).  Terminals are fixed.
+ * Pins are listed net by net (net_start, CSR); pin_owner < num_nodes names a
+ * node, otherwise terminal (pin_owner - num_nodes); pin offsets are from the
+ * owner's centre (PlaceCommon/objects.cpp:454-459).  Rows are the site rows
+ * of the .scl file (start.x, bottom, end.x, height). */
+typedef struct ep_netlist {
+    int32_t num_nodes;
+    int32_t num_terminals;
+    int32_t num_nets;
+    int32_t num_rows;
+    const float *node_w, *node_h;     /* [num_nodes] */
+    const float *node_cx, *node_cy;   /* [num_nodes] initial centres */
+    const float *term_llx, *term_lly; /* [num_terminals] lower-left corners */
+    const float *term_w, *term_h;     /* [num_terminals] */
+    const uint8_t *term_is_ni;        /* [num_terminals] "terminal_NI", may be NULL */
+    const int32_t *net_start;         /* [num_nets + 1] */
+    const int32_t *pin_owner;         /* [net_start[num_nets]] */
+    const float *pin_dx, *pin_dy;     /* [net_start[num_nets]] */
+    const float *row_llx, *row_lly, *row_urx, *row_h; /* [num_rows] */
+    float common_row_height;          /* 0 = height of the last row (parser.cpp:271) */
+} ep_netlist;
+
+typedef struct ep_params {
+    float target_density;   /* EPlacer_2D::setTargetDensity (EPlace/eplace.cpp:27-31) */
+    float target_overflow;  /* mGP stop, gArg "targetOverflow", default 0.10 (nesterov.hpp:89-97) */
+    int32_t bins_x, bins_y; /* 0 = the reference's rule (EPlace/eplace.cpp:237-261) */
+    int32_t max_iterations; /* MAX_ITERATION, default 1000 (nesterov.hpp:36) */
+    int32_t wl_model;       /* ep_wl_model */
+    int32_t exp_mode;       /* ep_exp_mode */
+    int32_t step_rule;      /* ep_step_rule */
+    int32_t dct_mode;       /* ep_dct_mode */
+    uint64_t filler_seed;   /* seed of the engine's own filler placement */
+    int32_t device;         /* CUDA device ordinal */
+    int32_t keep_maps;      /* 1 = keep per-evaluation bin maps queryable (tests) */
+} ep_params;
+
+/* Scalars of EPlacer_2D (EPlace/eplace.h:108-136) and the optimizer. */
+typedef struct ep_scalars {
+    double overflow;       /* globalDensityOverflow (tau) of the last evaluation */
+    double lambda;         /* penalty factor */
+    double hpwl;           /* HPWL of the last evaluation (bound-pin HPWL) */
+    double last_hpwl;      /* lastHPWL of updatePenaltyFactor */
+    double inv_gamma_x, inv_gamma_y;
+    double wirelength;     /* smooth (WA/LSE) wirelength of the last evaluation */
+    double step;           /* last step size */
+    double ns_param;       /* Nesterov a_k */
+    int32_t iteration;     /* iter_count of the current stage */
+    int32_t stage;         /* placementStage */
+    int32_t mgp_iterations; /* mGPIterationCount */
+    int32_t done;          /* stop condition reached */
+} ep_scalars;
+
+typedef struct ep_info {
+    int32_t num_nodes, num_fillers, num_objects, num_terminals, num_nets, num_pins;
+    int32_t num_macros, num_cells_and_fillers;
+    int32_t bins_x, bins_y;
+    float bin_step_x, bin_step_y;
+    float core_llx, core_lly, core_urx, core_ury;
+    float filler_w, filler_h;
+    double std_area, macro_area;  /* ePlaceStdCellArea / ePlaceMacroArea */
+    double total_row_area;
+    double density_scale;         /* fixed-point units per unit area of the bin maps */
+} ep_info;
+
+typedef struct ep_run_stats {
+    int32_t iterations;   /* steps taken in this run */
+    double overflow;      /* tau at the stop */
+    double hpwl;          /* exact HPWL of the final (main-solution) positions */
+    double lambda;
+    double seconds;       /* device time of the run, CUDA events */
+} ep_run_stats;
+
+typedef struct ep_engine ep_engine;
+
+/* ep_params with the reference defaults (rho_t 1.0, overflow 0.10, 1000 iterations). */
+void ep_default_params(ep_params *p);
+int32_t ep_abi_version(void);
+
+/* PlaceDB + EPlacer_2D construction: copies the netlist to the device, sizes
+ * the fillers (fillerInitialization, EPlace/eplace.cpp:61-208), builds the
+ * bin grid and its static terminal / base density (binInitialization,
+ * EPlace/eplace.cpp:221-412). */
+ep_status ep_create(const ep_netlist *netlist, const ep_params *params, ep_engine **out);
+void ep_destroy(ep_engine *e);
+const char *ep_last_error(const ep_engine *e);
+ep_status ep_get_info(const ep_engine *e, ep_info *info);
+/* Use this CUDA stream (cudaStream_t) for all later work; NULL = engine's own. */
+ep_status ep_set_stream(ep_engine *e, void *stream);
+ep_status ep_synchronize(ep_engine *e);
+
+/* EPlacer_2D::getPosition / setPosition (EPlace/eplace.cpp:759-804) for a
+ * stage view; setPosition clamps into the core (PlaceDB::setModuleCenter_2D,
+ * PlaceDB/placedb.cpp:253-288).  xy has 2*count floats. */
+ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count);
+ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count);
+
+/* EPlacer_2D::initialization tail (EPlace/eplace.cpp:47-49): first
+ * totalGradientUpdate with lambda 0, then penaltyFactorInitilization. */
+ep_status ep_initialize(ep_engine *e);
+/* EPlacer_2D::totalGradientUpdate (EPlace/eplace.cpp:687-738). */
+ep_status ep_eval_gradient(ep_engine *e);
+/* EPlacer_2D::getGradient (EPlace/eplace.cpp:742-756): the preconditioned
+ * descent direction of the last evaluation for a stage view. */
+ep_status ep_get_gradient(ep_engine *e, int32_t view, float *xy, int32_t count);
+/* densityGradient / wirelengthGradient of the last evaluation, all objects
+ * (keep_maps must be set). */
+ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wirelength_xy);
+/* Bin maps of the last evaluation, x-major [bins_x][bins_y] (keep_maps must
+ * be set for node/filler/field): nodeDensity, fillerDensity,
+ * terminalDensity, baseDensity (areas), E.x, E.y, phi.  Any may be NULL. */
+ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *terminal, float *base,
+                          float *ex, float *ey, float *phi);
+/* Raw fixed-point node / filler maps (int64, units of 1/density_scale). */
+ep_status ep_get_density_fixed(ep_engine *e, int64_t *node, int64_t *filler);
+
+ep_status ep_query(ep_engine *e, ep_scalars *s);
+ep_status ep_set_lambda(ep_engine *e, double lambda);
+/* penaltyFactorInitilization / updatePenaltyFactor (EPlace/eplace.cpp:812-883). */
+ep_status ep_penalty_init(ep_engine *e);
+ep_status ep_penalty_update(ep_engine *e);
+/* PlaceDB::calcHPWL (PlaceDB/placedb.cpp:424-432) at the current positions. */
+ep_status ep_hpwl(ep_engine *e, double *hpwl);
+
+/* switch2FillerOnly / switch2cGP (EPlace/eplace.cpp:887-904).  For
+ * EP_STAGE_FILLERONLY, filler_xy (2*num_fillers floats, lower-left corners as
+ * setModuleLocation_2D_random writes them) may be NULL: the engine then draws
+ * its own seeded positions. */
+ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy);
+
+/* FirstOrderOptimizer::opt (Optimization/opt.hpp:30-36) with
+ * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:
+ * init, steps until the stage's stop condition (or max_steps > 0 steps),
+ * wrap_up.  The loop runs on the device (captured CUDA graphs, step size,
+ * lambda and the stop test decided on the GPU). */
+ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats);
+/* The same loop one call at a time: begin = init(), step = "if
+ * (!stop_condition()) opt_step(); updatePenaltyFactor()", end = wrap_up().
+ * *stopped is set when the stop condition held and no step was taken. */
+ep_status ep_nesterov_begin(ep_engine *e);
+ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped);
+ep_status ep_nesterov_end(ep_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,124 @@
+"""Generate the golden fixtures of tests/golden/ from the REFERENCE itself.
+
+Runs in the build container only (it needs /root/reference and the harness
+library oracle/_ref/libeplace_ref.so built by `make -C oracle`).  For each
+design it records, at full float precision, what the unmodified reference
+computes on the same netlist and starting positions:
+
+  * initialization(): filler count / size, bin grid, every bin map
+    (node, filler, terminal, base density, E_x, E_y, phi), density /
+    wirelength / total gradients, tau, 1/gamma, HPWL and lambda_0;
+  * a second totalGradientUpdate with lambda_0 (the preconditioned direction);
+  * the first optimizer steps (positions, tau, lambda after each);
+  * the whole mGP run (iterations, final tau, HPWL).
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from eplace_b200 import bookshelf, synth  # noqa: E402
+from oracle import refharness as R  # noqa: E402
+
+REF_SMOKE = "/root/reference/examples/smoke/smoke.aux"
+TRAJ_STEPS = 5
+
+
+def designs():
+    # the reference's own example, started from the reference's QP like its flow
+    yield "ref_smoke", bookshelf.read_aux(REF_SMOKE, target_density=0.8), True
+    yield "stdcell_2k", synth.blob_start(synth.standard_cell(2000, seed=3)), False
+    yield "mixed_5k", synth.blob_start(synth.mixed_size(5000, 6, 3, seed=5)), False
+
+
+def netlist_arrays(nl):
+    keys = ("node_w", "node_h", "node_cx", "node_cy", "term_llx", "term_lly", "term_w", "term_h",
+            "term_is_ni", "net_start", "pin_owner", "pin_dx", "pin_dy", "row_llx", "row_lly",
+            "row_urx", "row_h", "row_site_w")
+    return {"nl_" + k: getattr(nl, k) for k in keys}
+
+
+def record(name, nl, use_qp):
+    ref = R.RefPlacer(nl)
+    if use_qp:
+        ref.qp()
+        cx, cy = ref.node_centers()
+        nl = nl.with_positions(cx, cy)
+    out = dict(netlist_arrays(nl))
+    out["target_density"] = np.float32(nl.target_density)
+    out["node_is_macro"] = ref.node_is_macro()
+    ref.initialization(nl.target_density)
+    info = ref.info()
+    for k, v in info.items():
+        out["info_" + k] = np.float64(v)
+    cx, cy = ref.positions()
+    out["init_cx"], out["init_cy"] = cx, cy
+    maps = ref.bins()
+    for k, v in maps.items():
+        out["init_" + k] = v
+    wl, dens, tot = ref.gradients()
+    out["init_grad_wl"], out["init_grad_density"], out["init_grad_total"] = wl, dens, tot
+    # second evaluation at the same positions, now with lambda_0
+    ref.total_gradient_update()
+    wl2, dens2, tot2 = ref.gradients()
+    out["eval2_grad_total"] = tot2
+    out["eval2_lambda"] = np.float64(ref.info()["lambda"])
+    # optimizer: first steps, then the rest of the stage
+    ref.opt_begin()
+    tcx, tcy, tlam, ttau, thp = [], [], [], [], []
+    for _ in range(TRAJ_STEPS):
+        stopped, _ = ref.opt_step()
+        if stopped:
+            break
+        x, y = ref.positions()
+        i = ref.info()
+        tcx.append(x)
+        tcy.append(y)
+        tlam.append(i["lambda"])
+        ttau.append(i["overflow"])
+        thp.append(i["last_hpwl"])
+    out["traj_cx"], out["traj_cy"] = np.array(tcx), np.array(tcy)
+    out["traj_lambda"], out["traj_tau"], out["traj_hpwl"] = np.array(tlam), np.array(ttau), np.array(thp)
+    while True:
+        stopped, _ = ref.opt_step()
+        if stopped:
+            break
+    ref.opt_end()
+    i = ref.info()
+    out["run_iterations"] = np.int64(i["iter_count"])
+    out["run_overflow"] = np.float64(i["overflow"])
+    out["run_hpwl"] = np.float64(ref.hpwl())
+    out["run_lambda"] = np.float64(i["lambda"])
+    fx, fy = ref.positions()
+    out["run_cx"], out["run_cy"] = fx, fy
+    ref.close()
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"{name}: {i['num_nodes']:.0f} nodes, {i['num_fillers']:.0f} fillers, bins {i['bins_x']:.0f}, "
+          f"{int(out['run_iterations'])} iterations, tau {float(out['run_overflow']):.6f}, "
+          f"HPWL {float(out['run_hpwl']):.3f} -> {os.path.getsize(path) // 1024} KB")
+
+
+def check_reader():
+    """The array netlist read by eplace_b200.bookshelf drives the reference to
+    the same state as the reference's own Bookshelf parser."""
+    a = R.RefPlacer(aux=REF_SMOKE)
+    b = R.RefPlacer(bookshelf.read_aux(REF_SMOKE, target_density=0.8))
+    for p in (a, b):
+        p.qp()
+        p.initialization(0.8)
+    ia, ib = a.info(), b.info()
+    assert ia["num_fillers"] == ib["num_fillers"] and ia["last_hpwl"] == ib["last_hpwl"], (ia, ib)
+    assert np.array_equal(a.gradients()[2], b.gradients()[2])
+
+
+if __name__ == "__main__":
+    check_reader()
+    for name, nl, qp in designs():
+        record(name, nl, qp)
