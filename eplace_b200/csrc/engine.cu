@@ -66,6 +66,10 @@ struct ep_engine {
     int graph_iters = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mt19937_64 rng;
+    float2 *snap = nullptr;   // ep_save_positions
+    bool has_snap = false;
+    int64_t launches = 0;     // engine kernels launched so far
+    int64_t graph_kernels = 0;  // kernels in one replay of the step graph
 };
 
 namespace {
@@ -246,8 +250,18 @@ ep_status device_status(ep_engine *e) {
     return EP_OK;
 }
 
+// Kernels one enqueue_eval launches (the DCT is four GEMMs).
+int kernels_per_eval(const ep_engine *e) {
+    const DeviceNetlist &d = e->dn;
+    return 1 + (d.n_big_objs > 0) + 1 + 4 + (d.n_small_nets > 0) + (d.n_big_nets > 0) +
+           (d.n_big_objs > 0) + 1;
+}
+
+int kernels_per_hpwl(const ep_engine *e) { return (e->dn.n_small_nets > 0) + (e->dn.n_big_nets > 0); }
+
 // totalGradientUpdate: enqueue one gradient evaluation at the current positions.
 void enqueue_eval(ep_engine *e, int stepping) {
+    e->launches += kernels_per_eval(e);
     cudaStream_t st = e->st;
     bool keep = e->prm.keep_maps != 0;
     if (keep) {
@@ -268,6 +282,12 @@ void enqueue_eval(ep_engine *e, int stepping) {
 void enqueue_step(ep_engine *e) {
     enqueue_eval(e, 1);
     launch_update(e->kc, e->dn, e->pos, e->x, e->g, e->y_prev, e->g_prev, e->S, e->st);
+    e->launches += 1;
+}
+
+void enqueue_hpwl(ep_engine *e, int mode) {
+    launch_hpwl(e->kc, e->dn, mode, e->S, e->st);
+    e->launches += kernels_per_hpwl(e);
 }
 
 ep_status build_graph(ep_engine *e, int iters) {
@@ -276,9 +296,12 @@ ep_status build_graph(ep_engine *e, int iters) {
         e->graph = nullptr;
     }
     cudaGraph_t g = nullptr;
+    int64_t before = e->launches;
     CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < iters; i++) enqueue_step(e);
     CK(cudaStreamEndCapture(e->st, &g));
+    e->graph_kernels = e->launches - before;  // counted per replay, not at capture
+    e->launches = before;
     cudaError_t rc = cudaGraphInstantiate(&e->graph, g, 0);
     cudaGraphDestroy(g);
     if (rc != cudaSuccess) {
@@ -918,7 +941,7 @@ ep_status ep_penalty_init(ep_engine *e) {
 
 ep_status ep_penalty_update(ep_engine *e) {
     if (!e) return EP_ERR_ARG;
-    launch_hpwl(e->kc, e->dn, 1, e->S, e->st);
+    enqueue_hpwl(e, 1);
     CK(cudaGetLastError());
     ep_status s = fetch_scalars(e);
     if (s) return s;
@@ -927,7 +950,7 @@ ep_status ep_penalty_update(ep_engine *e) {
 
 ep_status ep_hpwl(ep_engine *e, double *hpwl) {
     if (!e || !hpwl) return EP_ERR_ARG;
-    launch_hpwl(e->kc, e->dn, 0, e->S, e->st);
+    enqueue_hpwl(e, 0);
     CK(cudaGetLastError());
     ep_status s = fetch_scalars(e);
     if (s) return s;
@@ -985,6 +1008,7 @@ ep_status ep_nesterov_begin(ep_engine *e) {
     ep_status s = update_scalars(e, [](DevScalars &h) { h.step_cap = 0; });
     if (s) return s;
     launch_stage_begin(e->dn, e->pos, e->x, e->S, e->st);
+    e->launches += 1;
     CK(cudaGetLastError());
     e->in_run = true;
     return EP_OK;
@@ -1008,7 +1032,7 @@ ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
         return EP_ERR_UNSUPPORTED;
     }
     enqueue_step(e);
-    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);  // updatePenaltyFactor
+    enqueue_hpwl(e, 2);  // updatePenaltyFactor
     CK(cudaGetLastError());
     s = fetch_scalars(e);
     if (s) return s;
@@ -1018,8 +1042,9 @@ ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
 ep_status ep_nesterov_end(ep_engine *e) {
     if (!e) return EP_ERR_ARG;
     if (!e->in_run) return EP_OK;
-    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);
+    enqueue_hpwl(e, 2);
     launch_wrap_up(e->kc, e->dn, e->pos, e->x, e->st);
+    e->launches += 1;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e->st));
     e->in_run = false;
@@ -1037,20 +1062,23 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
         s = build_graph(e, K);
         if (s) return s;
     }
+    const int64_t launches0 = e->launches - 1;  // include the stage-begin kernel
     CK(cudaEventRecord(e->ev0, e->st));
     const int cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + K;
     int launched = 0;
     while (true) {
         CK(cudaGraphLaunch(e->graph, e->st));
+        e->launches += e->graph_kernels;
         launched += K;
         CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
         CK(cudaStreamSynchronize(e->st));
         if (e->hS->done || launched > cap + K) break;
     }
-    launch_hpwl(e->kc, e->dn, 2, e->S, e->st);  // the lambda update owed by the last step
+    enqueue_hpwl(e, 2);  // the lambda update owed by the last step
     launch_wrap_up(e->kc, e->dn, e->pos, e->x, e->st);
+    e->launches += 1;
     CK(cudaEventRecord(e->ev1, e->st));
-    launch_hpwl(e->kc, e->dn, 0, e->S, e->st);
+    enqueue_hpwl(e, 0);
     CK(cudaGetLastError());
     s = fetch_scalars(e);
     e->in_run = false;
@@ -1063,8 +1091,133 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
         stats->hpwl = e->hS->hpwl_query;
         stats->lambda = e->hS->lambda;
         stats->seconds = ms * 1e-3;
+        stats->kernel_launches = e->launches - launches0;
     }
     return device_status(e);
+}
+
+ep_status ep_save_positions(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->snap) {
+        ep_status s = dalloc(e, e->snap, e->n_obj);
+        if (s) return s;
+    }
+    CK(cudaMemcpyAsync(e->snap, e->pos, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    e->has_snap = true;
+    return EP_OK;
+}
+
+ep_status ep_load_positions(ep_engine *e) {
+    if (!e) return EP_ERR_ARG;
+    if (!e->has_snap) {
+        e->err = "ep_save_positions must run first";
+        return EP_ERR_STATE;
+    }
+    CK(cudaMemcpyAsync(e->pos, e->snap, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
+    return EP_OK;
+}
+
+ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
+    if (!e || !out || reps <= 0) return EP_ERR_ARG;
+    std::memset(out, 0, sizeof(*out));
+    const int no = e->n_obj, np = e->n_pins, nb = e->grid.nx * e->grid.ny;
+    const DeviceNetlist &d = e->dn;
+    // state the timed launches mutate, restored at the end
+    std::vector<float2> keep[5];
+    float2 *bufs[5] = {e->pos, e->x, e->g, e->y_prev, e->g_prev};
+    for (int k = 0; k < 5; k++) {
+        keep[k].resize(no);
+        CK(cudaMemcpyAsync(keep[k].data(), bufs[k], sizeof(float2) * no, cudaMemcpyDeviceToHost, e->st));
+    }
+    ep_status s = fetch_scalars(e);
+    if (s) return s;
+    DevScalars saved = *e->hS;
+    s = update_scalars(e, [](DevScalars &h) {
+        h.done = 0;
+        h.lambda0_mode = 0;
+        h.step_cap = 0;
+    });
+    if (s) return s;
+    const bool keep_maps = e->prm.keep_maps != 0;
+    const bool tc = e->dct.mode == EP_DCT_BF16X3;
+    void *bf = tc ? dct_tc_rho_planes(e->dct) : nullptr;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    auto timed = [&](const char *name, int launches, double bytes, double flops, auto &&fn,
+                     auto &&before) -> ep_status {
+        int k = out->count++;
+        std::snprintf(out->names[k], sizeof(out->names[k]), "%s", name);
+        double tot = 0;
+        for (int r = 0; r < reps; r++) {
+            before();
+            CK(cudaEventRecord(a, e->st));
+            fn();
+            CK(cudaEventRecord(b, e->st));
+            CK(cudaEventSynchronize(b));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            tot += ms;
+        }
+        out->ms[k] = tot / reps;
+        out->bytes[k] = bytes;
+        out->flops[k] = flops;
+        out->launches[k] = launches;
+        return EP_OK;
+    };
+    auto nothing = [] {};
+    auto zero_maps = [&] {
+        cudaMemsetAsync(e->node_q, 0, sizeof(unsigned long long) * nb, e->st);
+        cudaMemsetAsync(e->filler_q, 0, sizeof(unsigned long long) * nb, e->st);
+    };
+    const double nobj = no, npin = np, nnet = e->n_nets, nbin = nb;
+    const double nx = e->grid.nx, ny = e->grid.ny;
+    // algorithmic bytes: compulsory reads + writes of each group, per launch
+    s = timed("scatter", 1 + (d.n_big_objs > 0), 17.0 * nobj + 16.0 * nbin, 0.0,
+              [&] { launch_scatter(e->kc, d, e->node_q, e->filler_q, e->S, e->st); }, zero_maps);
+    if (s) return s;
+    s = timed("prep", 1, 8.0 * nbin + 8.0 * nbin + (tc ? 4.0 : 4.0) * nbin + (keep_maps ? 0.0 : 16.0 * nbin), 0.0,
+              [&] {
+                  launch_prep(e->kc, e->node_q, e->filler_q, e->static_map, bf ? nullptr : e->rho, bf,
+                              nullptr, nullptr, keep_maps ? 0 : 1, e->S, e->st);
+              }, nothing);
+    if (s) return s;
+    // G1 2nx*ny*ny + G2 2nx*nx*ny + G3 2nx*2ny*ny + G4 2*(2nx*ny*nx)
+    double dct_flops = 2 * nx * ny * ny + 2 * nx * nx * ny + 4 * nx * ny * ny + 4 * nx * ny * nx;
+    s = timed("poisson_dct", 4, 16.0 * nbin, dct_flops,
+              [&] { dct_run(e->dct, e->rho, e->field, nullptr, e->S, e->st); }, nothing);
+    if (s) return s;
+    s = timed("wirelength", (d.n_small_nets > 0) + (d.n_big_nets > 0), 28.0 * npin + 8.0 * nnet, 0.0,
+              [&] { launch_wirelength(e->kc, d, e->pin_grad, e->S, e->st); }, nothing);
+    if (s) return s;
+    if (d.n_big_objs > 0) {
+        s = timed("gather_big", 1, 0.0, 0.0,
+                  [&] { launch_gather_big(e->kc, d, e->field, e->gd_big, e->S, e->st); }, nothing);
+        if (s) return s;
+    }
+    s = timed("combine", 1, 85.0 * nobj + 12.0 * npin, 0.0,
+              [&] {
+                  launch_combine(e->kc, d, e->field, e->gd_big, e->pin_grad, e->g, e->g_prev,
+                                 e->y_prev, nullptr, nullptr, 1, e->S, e->st);
+              }, nothing);
+    if (s) return s;
+    s = timed("update", 1, 65.0 * nobj, 0.0,
+              [&] { launch_update(e->kc, d, e->pos, e->x, e->g, e->y_prev, e->g_prev, e->S, e->st); },
+              [&] {
+                  // a pending stop would make the following repetitions no-ops
+                  cudaMemsetAsync(&e->S->stop_pending, 0, sizeof(int), e->st);
+              });
+    if (s) return s;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (int k = 0; k < 5; k++)
+        CK(cudaMemcpyAsync(bufs[k], keep[k].data(), sizeof(float2) * no, cudaMemcpyHostToDevice, e->st));
+    *e->hS = saved;
+    CK(cudaMemcpyAsync(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice, e->st));
+    if (!keep_maps) zero_maps();
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
 }
 
 }  // extern "C"

@@ -80,7 +80,17 @@ class Info(ctypes.Structure):
 
 class RunStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("overflow", ctypes.c_double),
-                ("hpwl", ctypes.c_double), ("lambda_", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("hpwl", ctypes.c_double), ("lambda_", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("kernel_launches", ctypes.c_int64)]
+
+
+MAX_TIMED = 12
+
+
+class KernelTimes(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int32), ("names", (ctypes.c_char * 24) * MAX_TIMED),
+                ("ms", ctypes.c_double * MAX_TIMED), ("bytes", ctypes.c_double * MAX_TIMED),
+                ("flops", ctypes.c_double * MAX_TIMED), ("launches", ctypes.c_int32 * MAX_TIMED)]
 
 
 # every symbol include/eplace_gpu.h declares
@@ -90,7 +100,7 @@ EXPORTS = (
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
-    "ep_nesterov_end",
+    "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels",
 )
 
 _lib = None
@@ -119,8 +129,9 @@ def load():
     for n in ("ep_get_positions", "ep_set_positions", "ep_get_gradient"):
         getattr(L, n).argtypes = [vp, ctypes.c_int32, _f32p, ctypes.c_int32]
     for n in ("ep_initialize", "ep_eval_gradient", "ep_penalty_init", "ep_penalty_update",
-              "ep_nesterov_begin", "ep_nesterov_end"):
+              "ep_nesterov_begin", "ep_nesterov_end", "ep_save_positions", "ep_load_positions"):
         getattr(L, n).argtypes = [vp]
+    L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
     L.ep_get_bin_maps.argtypes = [vp] + [_f32p] * 7
     L.ep_get_density_fixed.argtypes = [vp, _i64p, _i64p]
@@ -215,6 +226,13 @@ class Engine:
         xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
         self._check(self._L.ep_set_positions(self.h, view, _p(xy, _f32p), xy.shape[0]))
 
+    def set_positions_ptr(self, host_ptr, count, view=MGP):
+        """ep_set_positions from a raw host pointer (e.g. pinned memory)."""
+        self._check(self._L.ep_set_positions(self.h, view, ctypes.cast(host_ptr, _f32p), int(count)))
+
+    def get_positions_ptr(self, host_ptr, count, view=MGP):
+        self._check(self._L.ep_get_positions(self.h, view, ctypes.cast(host_ptr, _f32p), int(count)))
+
     def get_gradient(self, view=MGP):
         n = self.view_size(view)
         g = np.zeros((n, 2), np.float32)
@@ -290,6 +308,21 @@ class Engine:
 
     def synchronize(self):
         self._check(self._L.ep_synchronize(self.h))
+
+    def save_positions(self):
+        self._check(self._L.ep_save_positions(self.h))
+
+    def load_positions(self):
+        self._check(self._L.ep_load_positions(self.h))
+
+    def set_stream(self, stream_ptr):
+        self._check(self._L.ep_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def time_kernels(self, reps=20):
+        t = KernelTimes()
+        self._check(self._L.ep_time_kernels(self.h, int(reps), ctypes.byref(t)))
+        return [dict(name=t.names[i].value.decode(), ms=t.ms[i], bytes=t.bytes[i], flops=t.flops[i],
+                     launches=t.launches[i]) for i in range(t.count)]
 
 
 class EPlacer2D:

@@ -126,7 +126,19 @@ typedef struct ep_run_stats {
     double hpwl;          /* exact HPWL of the final (main-solution) positions */
     double lambda;
     double seconds;       /* device time of the run, CUDA events */
+    int64_t kernel_launches; /* engine kernels launched by this run */
 } ep_run_stats;
+
+/* Per-kernel device times of one evaluation + step (ep_time_kernels). */
+#define EP_MAX_TIMED_KERNELS 12
+typedef struct ep_kernel_times {
+    int32_t count;
+    char names[EP_MAX_TIMED_KERNELS][24];
+    double ms[EP_MAX_TIMED_KERNELS];     /* average device time per launch group */
+    double bytes[EP_MAX_TIMED_KERNELS];  /* algorithmic bytes per launch group */
+    double flops[EP_MAX_TIMED_KERNELS];  /* algorithmic flops per launch group */
+    int32_t launches[EP_MAX_TIMED_KERNELS]; /* kernels in the group */
+} ep_kernel_times;
 
 typedef struct ep_engine ep_engine;
 
@@ -151,6 +163,10 @@ ep_status ep_synchronize(ep_engine *e);
  * PlaceDB/placedb.cpp:253-288).  xy has 2*count floats. */
 ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count);
 ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count);
+/* PlaceDB::saveNodesLocation / loadNodesLocation (PlaceDB/placedb.cpp:1441-1465)
+ * for every object, kept in device memory (no host copy). */
+ep_status ep_save_positions(ep_engine *e);
+ep_status ep_load_positions(ep_engine *e);
 
 /* EPlacer_2D::initialization tail (EPlace/eplace.cpp:47-49): first
  * totalGradientUpdate with lambda 0, then penaltyFactorInitilization. */
@@ -197,6 +213,13 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats);
 ep_status ep_nesterov_begin(ep_engine *e);
 ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped);
 ep_status ep_nesterov_end(ep_engine *e);
+
+/* Measurement hook with no reference counterpart: launches each kernel group
+ * of one evaluation + step separately, reps times, timing every launch with
+ * CUDA events on the engine's stream, and reports the average device time
+ * with the group's algorithmic bytes / flops.  Positions, optimizer vectors
+ * and scalars are restored afterwards. */
+ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out);
 
 #ifdef __cplusplus
 }

@@ -399,7 +399,11 @@ double ref_opt_run(void *hp)
 
 // Step-wise form of the same loop: begin = init(), step = one
 // "if (!stop_condition()) opt_step()", end = wrap_up().
-void ref_opt_begin(void *hp) { static_cast<RefHandle *>(hp)->opt->init(); }
+void ref_opt_begin(void *hp)
+{
+    Quiet q;
+    static_cast<RefHandle *>(hp)->opt->init();
+}
 
 // Returns 1 if the loop stopped (no step taken), 0 after a step.
 int ref_opt_step(void *hp, double *seconds)
@@ -415,7 +419,11 @@ int ref_opt_step(void *hp, double *seconds)
     return 0;
 }
 
-void ref_opt_end(void *hp) { static_cast<RefHandle *>(hp)->opt->wrap_up(); }
+void ref_opt_end(void *hp)
+{
+    Quiet q;
+    static_cast<RefHandle *>(hp)->opt->wrap_up();
+}
 
 // Optimizer vectors of the current stage view (interleaved x,y).
 int ref_opt_state(void *hp, float *x, float *y, float *g, float *y_prev, float *g_prev)

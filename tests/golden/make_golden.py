@@ -118,7 +118,35 @@ def check_reader():
     assert np.array_equal(a.gradients()[2], b.gradients()[2])
 
 
+def record_bench_reference():
+    """The reference's whole mGP run on bench.py's 200k-cell design (about a
+    minute of CPU): iterations to overflow < 0.1, final overflow and HPWL.
+    bench.py scales its bounded CPU samples by this iteration count."""
+    import json
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    nl = bench.design()
+    ref = R.RefPlacer(nl)
+    t0 = time.time()
+    ref.initialization(1.0)
+    t_init = time.time() - t0
+    t0 = time.time()
+    ref.opt_run()
+    t_mgp = time.time() - t0
+    i = ref.info()
+    out = {"stdcell_200k_mgp": dict(iterations=int(i["iter_count"]), overflow=float(i["overflow"]),
+                                    hpwl=float(ref.hpwl()), fillers=int(i["num_fillers"]),
+                                    bins=int(i["bins_x"]), init_seconds=t_init, mgp_seconds=t_mgp,
+                                    note="reference CPU path, 1 thread, build container")}
+    with open(os.path.join(HERE, "reference_runs.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(out)
+
+
 if __name__ == "__main__":
     check_reader()
     for name, nl, qp in designs():
         record(name, nl, qp)
+    if "--bench" in sys.argv:
+        record_bench_reference()
