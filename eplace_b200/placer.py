@@ -101,7 +101,25 @@ EXPORTS = (
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels",
+    "ep_density_scatter_noalloc",
 )
+
+
+class ScatterGrid(ctypes.Structure):
+    _fields_ = [("bins_x", ctypes.c_int32), ("bins_y", ctypes.c_int32),
+                ("core_llx", ctypes.c_float), ("core_lly", ctypes.c_float),
+                ("bin_step_x", ctypes.c_float), ("bin_step_y", ctypes.c_float),
+                ("target_density", ctypes.c_float)]
+
+
+def density_scatter_noalloc(grid, num_objects, cx, cy, w, h, flags, node_out, filler_out, stream=0):
+    """ep_density_scatter_noalloc on raw DEVICE pointers (ints); returns (status, message)."""
+    L = load()
+    buf = ctypes.create_string_buffer(256)
+    vp = lambda p: ctypes.c_void_p(int(p)) if p else None
+    rc = L.ep_density_scatter_noalloc(ctypes.byref(grid), int(num_objects), vp(cx), vp(cy), vp(w), vp(h),
+                                      vp(flags), vp(node_out), vp(filler_out), vp(stream), buf, 256)
+    return rc, buf.value.decode()
 
 _lib = None
 
@@ -132,6 +150,8 @@ def load():
               "ep_nesterov_begin", "ep_nesterov_end", "ep_save_positions", "ep_load_positions"):
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
+    L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
+        [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
     L.ep_get_bin_maps.argtypes = [vp] + [_f32p] * 7
     L.ep_get_density_fixed.argtypes = [vp, _i64p, _i64p]

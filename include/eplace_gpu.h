@@ -221,6 +221,41 @@ ep_status ep_nesterov_end(ep_engine *e);
  * and scalars are restored afterwards. */
 ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out);
 
+/* Bin grid of ep_density_scatter_noalloc. */
+typedef struct ep_scatter_grid {
+    int32_t bins_x, bins_y;
+    float core_llx, core_lly;     /* lower-left corner of the core region */
+    float bin_step_x, bin_step_y;
+    float target_density;         /* macro contributions are scaled by it */
+} ep_scatter_grid;
+
+/* Density scatter that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a host tool whose allocator has
+ * reserved the device memory up front and forbids plugins from allocating, or
+ * a caller that must not bring the device-wide synchronisation of a
+ * cudaMalloc / cudaFree pair into its stream work.  All pointers are DEVICE
+ * memory owned by the caller: object centres cx, cy, sizes w, h and flags
+ * (bit 0 macro, bit 1 filler; NULL = all cells) for num_objects objects;
+ * outputs node_out and filler_out (NULL allowed) are [bins_x][bins_y] float
+ * maps of overlap areas, as EPlacer_2D::binNodeDensityUpdate accumulates them
+ * (EPlace/eplace.cpp:1029-1133) and ep_get_bin_maps reports them.
+ *
+ * The int64 fixed-point scratch is a fixed file-scope device array of
+ * 2 x 512 x 512 entries (4 MiB), held by every GPU that loads this library
+ * until the process exits.  Grids beyond 512 x 512 bins are rejected with
+ * EP_ERR_ARG and a message in err (err_len bytes, may be NULL); the total
+ * object area must stay below 2^30.  The first call on each device, made with
+ * that device current, looks up the scratch array's device address; make that
+ * first call before any stream capture.  Every call zeroes and reuses the same
+ * scratch, so calls that overlap on the GPU (on different streams, or from
+ * several threads) race and must be serialised by the caller.  Work is
+ * enqueued on `stream` (cudaStream_t, NULL = default stream). */
+ep_status ep_density_scatter_noalloc(const ep_scatter_grid *grid, int32_t num_objects,
+                                     const float *cx, const float *cy, const float *w,
+                                     const float *h, const uint8_t *flags, float *node_out,
+                                     float *filler_out, void *stream, char *err, int32_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
