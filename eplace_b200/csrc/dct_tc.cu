@@ -1,19 +1,446 @@
 // dct_tc.cu -- the four DCT GEMMs of dct.cu on the tcgen05 tensor cores.
+//
+// Every operand is stored as two bf16 planes, hi = bf16(v) and
+// lo = bf16(v - hi); a product is formed from three MMAs
+// (hi*hi + hi*lo + lo*hi) accumulated in FP32 in tensor memory, which keeps
+// ~2^-17 relative accuracy per product (3xBF16 split products).
+//
+// One CTA computes a 128 x BN output tile:
+//   warp 0, one thread : TMA producer (cp.async.bulk.tensor, 128B swizzle)
+//                        into a kStages-deep shared-memory ring
+//   warp 1, one thread : MMA issuer (tcgen05.mma.cta_group::1.kind::f16,
+//                        A and B from shared-memory descriptors, D in TMEM);
+//                        warp 1 also allocates / frees the TMEM columns
+//   warps 0-3          : epilogue, tcgen05.ld of their 32 TMEM lanes, then
+//                        the GEMM's store (bf16 hi/lo planes, transposed or
+//                        spectrally scaled, or the FP32 field)
+// Every wait on an mbarrier is bounded; a wait that gives up raises the
+// EP_ERR_TIMEOUT bit in DevScalars::status, the CTA drains what it issued,
+// frees its TMEM and returns.  No TMA multicast is used.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
 #include "engine.h"
 
 namespace ep {
 
-int dct_tc_init(DctPlan &p, std::string &err) {
-    err = "tensor-core DCT not built in this library";
-    return EP_ERR_UNSUPPORTED;
+namespace {
+
+constexpr int kBM = 128;            // UMMA M (TMEM lanes)
+constexpr int kBN = 64;             // UMMA N (TMEM columns)
+constexpr int kBK = 64;             // bf16 elements per 128-byte swizzle row
+constexpr int kStages = 4;
+constexpr int kATile = kBM * kBK * 2;   // 16 KiB
+constexpr int kBTile = kBN * kBK * 2;   // 8 KiB
+constexpr int kStageBytes = 2 * kATile + 2 * kBTile;
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*alignment*/;
+constexpr int kThreads = 128;
+constexpr unsigned kWaitLimit = 1u << 22;  // try_wait rounds before giving up
+
+enum TcEpi { kTcTransposed = 0, kTcSpectral = 1, kTcField = 2 };
+
+struct TcGemmParams {
+    CUtensorMap a_hi[3], a_lo[3], b_hi[3], b_lo[3];
+    int M, N, K;
+    int epi;
+    uint16_t *out_hi, *out_lo;  // bf16 planes (kTcTransposed / kTcSpectral)
+    int ldo;
+    const float *kscale;        // spectral scale [M][N]
+    float2 *field;              // kTcField, batches 0 (x) and 1 (y)
+    float *phi;                 // kTcField, batch 2
+};
+
+// ---- PTX wrappers -------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-void dct_tc_free(DctPlan &p) { p.tc = nullptr; }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; returns false (and raises the abort flag) when it gives up or
+// when another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    for (unsigned it = 0; it < kWaitLimit; it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,
+                                            int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, 128B swizzle: 8-row x 128 B atoms,
+// stride between 8-row groups (SBO) 1024 B, version 1, layout type 2.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;            // LBO (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;  // SBO
+    d |= (uint64_t)1 << 46;            // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void bf16_split(float v, uint16_t &hi, uint16_t &lo) {
+    uint32_t u = __float_as_uint(v);
+    uint32_t r = u + 0x7fffu + ((u >> 16) & 1u);
+    hi = (uint16_t)(r >> 16);
+    float rem = v - __uint_as_float((uint32_t)hi << 16);
+    uint32_t u2 = __float_as_uint(rem);
+    lo = (uint16_t)((u2 + 0x7fffu + ((u2 >> 16) & 1u)) >> 16);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    if (S && S->done) return;
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + kStages * kStageBytes);
+    uint64_t *empty = full + kStages;
+    uint64_t *done = empty + kStages;
+    volatile uint32_t *tmem_slot = (volatile uint32_t *)(done + 1);
+    volatile int *abort = (volatile int *)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bz = blockIdx.z;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const int nk = p.K / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32((const void *)tmem_slot)), "r"(kBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // ---- TMA producer ----
+        int issued = 0;
+        for (int kb = 0; kb < nk; kb++) {
+            int s = kb % kStages, use = kb / kStages;
+            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, abort)) break;
+            uint8_t *st = smem + s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_2d(st, &p.a_hi[bz], &full[s], kb * kBK, m0);
+            tma_load_2d(st + kATile, &p.a_lo[bz], &full[s], kb * kBK, m0);
+            tma_load_2d(st + 2 * kATile, &p.b_hi[bz], &full[s], kb * kBK, n0);
+            tma_load_2d(st + 2 * kATile + kBTile, &p.b_lo[bz], &full[s], kb * kBK, n0);
+            issued = kb + 1;
+        }
+        if (*abort) {
+            // drain: the last loads issued into each stage must land before exit
+            for (int kb = issued - kStages > 0 ? issued - kStages : 0; kb < issued; kb++)
+                for (unsigned it = 0; it < kWaitLimit && !mbar_try_wait(&full[kb % kStages], (kb / kStages) & 1); it++) {
+                }
+        }
+    } else if (threadIdx.x == 32) {
+        // ---- MMA issuer ----
+        const uint32_t idesc = umma_idesc(kBM, kBN);
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            int s = kb % kStages, use = kb / kStages;
+            if (!mbar_wait(&full[s], use & 1, abort)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint8_t *st = smem + s * kStageBytes;
+            uint32_t ah = smem_u32(st), al = smem_u32(st + kATile);
+            uint32_t bh = smem_u32(st + 2 * kATile), bl = smem_u32(st + 2 * kATile + kBTile);
+#pragma unroll
+            for (int k = 0; k < kBK / 16; k++) {
+                uint32_t off = k * 32;  // 16 bf16 = 32 bytes along K inside the swizzle atom
+                umma_bf16(tmem, umma_desc(ah + off), umma_desc(bl + off), idesc, (kb | k) != 0);
+                umma_bf16(tmem, umma_desc(al + off), umma_desc(bh + off), idesc, 1);
+                umma_bf16(tmem, umma_desc(ah + off), umma_desc(bh + off), idesc, 1);
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);  // also fences the MMAs issued before an abort
+    }
+    __syncwarp();
+
+    // ---- epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows ----
+    // lane 0 waits, the warp follows its verdict (tcgen05.ld is warp-aligned)
+    int ready = 0;
+    if (lane == 0) ready = mbar_wait(done, 0, abort) && !*abort;
+    ready = __shfl_sync(0xffffffffu, ready, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ready) {
+        const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kBN; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                const int n = n0 + c0 + c;
+                float v = __uint_as_float(r[c]);
+                if (p.epi == kTcTransposed) {
+                    uint16_t hi, lo;
+                    bf16_split(v, hi, lo);
+                    p.out_hi[(size_t)n * p.ldo + m] = hi;
+                    p.out_lo[(size_t)n * p.ldo + m] = lo;
+                } else if (p.epi == kTcSpectral) {
+                    uint16_t hi, lo;
+                    bf16_split(v * p.kscale[(size_t)m * p.N + n], hi, lo);
+                    p.out_hi[(size_t)m * p.ldo + n] = hi;
+                    p.out_lo[(size_t)m * p.ldo + n] = lo;
+                } else {
+                    if (bz == 0)
+                        p.field[(size_t)m * p.N + n].x = v;
+                    else if (bz == 1)
+                        p.field[(size_t)m * p.N + n].y = v;
+                    else
+                        p.phi[(size_t)m * p.N + n] = v;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
+    }
+    if (threadIdx.x == 0 && *abort && S) atomicOr(&S->status, 1 << EP_ERR_TIMEOUT);
+}
+
+// ---- host side ------------------------------------------------------------------
+struct TcPlan {
+    // bf16 planes (hi, lo contiguous: lo = hi + rows*cols)
+    uint16_t *rho = nullptr, *Cy = nullptr, *Cx = nullptr, *Tt = nullptr, *P = nullptr;
+    uint16_t *B3 = nullptr, *A4 = nullptr, *T3 = nullptr;
+    TcGemmParams g[4];
+};
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+bool load_encoder(std::string &err) {
+    if (g_encode) return true;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        err = "cuTensorMapEncodeTiled is not available from the driver";
+        return false;
+    }
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return true;
+}
+
+// Row-major bf16 plane [rows][cols] (cols contiguous = K), box of box_rows x 64.
+bool make_map(CUtensorMap *m, const uint16_t *base, int rows, int cols, int box_rows, std::string &err) {
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult rc = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS) {
+        err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)rc) + ")";
+        return false;
+    }
+    return true;
+}
+
+void split_host(const std::vector<float> &v, std::vector<uint16_t> &out) {
+    size_t n = v.size();
+    out.resize(2 * n);
+    for (size_t i = 0; i < n; i++) {
+        uint32_t u;
+        std::memcpy(&u, &v[i], 4);
+        uint32_t r = u + 0x7fffu + ((u >> 16) & 1u);
+        uint16_t hi = (uint16_t)(r >> 16);
+        uint32_t hu = (uint32_t)hi << 16;
+        float hf;
+        std::memcpy(&hf, &hu, 4);
+        float rem = v[i] - hf;
+        uint32_t u2;
+        std::memcpy(&u2, &rem, 4);
+        out[i] = hi;
+        out[n + i] = (uint16_t)((u2 + 0x7fffu + ((u2 >> 16) & 1u)) >> 16);
+    }
+}
+
+bool upload_planes(uint16_t *&dst, const float *dev_src, size_t n, std::string &err) {
+    std::vector<float> h(n);
+    if (cudaMemcpy(h.data(), dev_src, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        err = "reading DCT tables failed";
+        return false;
+    }
+    std::vector<uint16_t> s;
+    split_host(h, s);
+    if (cudaMalloc(&dst, s.size() * 2) != cudaSuccess) {
+        err = "cudaMalloc failed for bf16 DCT planes";
+        return false;
+    }
+    return cudaMemcpy(dst, s.data(), s.size() * 2, cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+}  // namespace
+
+int dct_tc_init(DctPlan &p, std::string &err) {
+    const int nx = p.nx, ny = p.ny;
+    if (nx % kBM || ny % kBM || nx % kBK || ny % kBK) {
+        err = "tensor-core DCT needs bins_x and bins_y to be multiples of 128";
+        return EP_ERR_UNSUPPORTED;
+    }
+    if (!load_encoder(err)) return EP_ERR_UNSUPPORTED;
+    TcPlan *t = new TcPlan();
+    p.tc = t;
+    const size_t nb = (size_t)nx * ny;
+    if (!upload_planes(t->Cy, p.Cy, (size_t)ny * ny, err) || !upload_planes(t->Cx, p.Cx, (size_t)nx * nx, err) ||
+        !upload_planes(t->B3, p.B3, (size_t)2 * ny * ny, err) ||
+        !upload_planes(t->A4, p.A4, (size_t)2 * nx * nx, err))
+        return EP_ERR_NOMEM;
+    if (cudaMalloc(&t->rho, 2 * nb * 2) != cudaSuccess || cudaMalloc(&t->Tt, 2 * nb * 2) != cudaSuccess ||
+        cudaMalloc(&t->P, 2 * nb * 2) != cudaSuccess || cudaMalloc(&t->T3, 2 * 2 * nb * 2) != cudaSuccess) {
+        err = "cudaMalloc failed for bf16 DCT intermediates";
+        return EP_ERR_NOMEM;
+    }
+    auto lo = [](uint16_t *base, size_t n) { return base + n; };
+    // G1: Tt[v][x] = sum_y rho[x][y] Cy[v][y]
+    TcGemmParams &g1 = t->g[0];
+    std::memset(&g1, 0, sizeof(g1));
+    g1.M = nx; g1.N = ny; g1.K = ny; g1.epi = kTcTransposed;
+    g1.out_hi = t->Tt; g1.out_lo = lo(t->Tt, nb); g1.ldo = nx;
+    bool ok = make_map(&g1.a_hi[0], t->rho, nx, ny, kBM, err) && make_map(&g1.a_lo[0], lo(t->rho, nb), nx, ny, kBM, err) &&
+              make_map(&g1.b_hi[0], t->Cy, ny, ny, kBN, err) && make_map(&g1.b_lo[0], lo(t->Cy, (size_t)ny * ny), ny, ny, kBN, err);
+    // G2: P[u][v] = K[u][v] sum_x Cx[u][x] Tt[v][x]
+    TcGemmParams &g2 = t->g[1];
+    std::memset(&g2, 0, sizeof(g2));
+    g2.M = nx; g2.N = ny; g2.K = nx; g2.epi = kTcSpectral;
+    g2.out_hi = t->P; g2.out_lo = lo(t->P, nb); g2.ldo = ny; g2.kscale = p.K;
+    ok = ok && make_map(&g2.a_hi[0], t->Cx, nx, nx, kBM, err) && make_map(&g2.a_lo[0], lo(t->Cx, (size_t)nx * nx), nx, nx, kBM, err) &&
+         make_map(&g2.b_hi[0], t->Tt, ny, nx, kBN, err) && make_map(&g2.b_lo[0], lo(t->Tt, nb), ny, nx, kBN, err);
+    // G3: T3[n][u] = sum_v P[u][v] B3[n][v]
+    TcGemmParams &g3 = t->g[2];
+    std::memset(&g3, 0, sizeof(g3));
+    g3.M = nx; g3.N = 2 * ny; g3.K = ny; g3.epi = kTcTransposed;
+    g3.out_hi = t->T3; g3.out_lo = lo(t->T3, 2 * nb); g3.ldo = nx;
+    ok = ok && make_map(&g3.a_hi[0], t->P, nx, ny, kBM, err) && make_map(&g3.a_lo[0], lo(t->P, nb), nx, ny, kBM, err) &&
+         make_map(&g3.b_hi[0], t->B3, 2 * ny, ny, kBN, err) && make_map(&g3.b_lo[0], lo(t->B3, (size_t)2 * ny * ny), 2 * ny, ny, kBN, err);
+    // G4: field[x][y] = sum_u A4{x,y}[x][u] {Ut,Vt}[y][u]; batch 2 = phi (A4y with Ut)
+    TcGemmParams &g4 = t->g[3];
+    std::memset(&g4, 0, sizeof(g4));
+    g4.M = nx; g4.N = ny; g4.K = nx; g4.epi = kTcField;
+    const size_t a4 = (size_t)2 * nx * nx;  // lo plane offset of A4
+    const size_t t3 = (size_t)2 * nb;       // lo plane offset of T3
+    uint16_t *A4x = t->A4, *A4y = t->A4 + (size_t)nx * nx;
+    uint16_t *Ut = t->T3, *Vt = t->T3 + nb;
+    uint16_t *As[3] = {A4x, A4y, A4y}, *Bs[3] = {Ut, Vt, Ut};
+    for (int b = 0; b < 3 && ok; b++)
+        ok = make_map(&g4.a_hi[b], As[b], nx, nx, kBM, err) && make_map(&g4.a_lo[b], As[b] + a4, nx, nx, kBM, err) &&
+             make_map(&g4.b_hi[b], Bs[b], ny, nx, kBN, err) && make_map(&g4.b_lo[b], Bs[b] + t3, ny, nx, kBN, err);
+    if (!ok) return EP_ERR_UNSUPPORTED;
+    if (cudaFuncSetAttribute(k_umma_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess) {
+        err = "cannot raise the dynamic shared memory limit of the tcgen05 GEMM";
+        return EP_ERR_CUDA;
+    }
+    return EP_OK;
+}
+
+void dct_tc_free(DctPlan &p) {
+    TcPlan *t = (TcPlan *)p.tc;
+    if (!t) return;
+    for (uint16_t *q : {t->rho, t->Cy, t->Cx, t->Tt, t->P, t->B3, t->A4, t->T3})
+        if (q) cudaFree(q);
+    delete t;
+    p.tc = nullptr;
+}
+
+void *dct_tc_rho_planes(DctPlan &p) { return p.tc ? ((TcPlan *)p.tc)->rho : nullptr; }
 
 int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaStream_t st) {
-    return EP_ERR_UNSUPPORTED;
+    TcPlan *t = (TcPlan *)p.tc;
+    DevScalars *s = const_cast<DevScalars *>(S);
+    for (int i = 0; i < 4; i++) {
+        TcGemmParams &g = t->g[i];
+        int batch = 1;
+        if (i == 3) {
+            g.field = field;
+            g.phi = phi;
+            batch = phi ? 3 : 2;
+        }
+        dim3 grid(g.N / kBN, g.M / kBM, batch);
+        k_umma_nt<<<grid, kThreads, kSmemBytes, st>>>(g, s);
+    }
+    return EP_OK;
 }
-
-void *dct_tc_rho_planes(DctPlan &p) { return nullptr; }
 
 }  // namespace ep
