@@ -17,6 +17,8 @@ enum ObjFlag : uint8_t {
     kFiller = 2,    // Module::isFiller
     kInView = 4,    // member of the current stage view
     kBig = 8,       // spans more bins than a thread handles: block-per-object path
+    kSmoothX = 16,  // narrower than a bin: widened to one bin (local smoothing)
+    kSmoothY = 32,  // lower than a bin
 };
 
 // Device-resident scalars of one engine (EPlacer_2D + EplaceNesterovOpt state
@@ -57,6 +59,7 @@ struct Grid {
     float llx, lly, urx, ury;  // core region
     float sx, sy;              // bin step
     float td;                  // target density
+    float isx, isy;            // 1 / bin step (gather only)
 };
 
 // getOverlap/getOverlapArea (PlaceCommon/global.h:477-518), FP64.
@@ -139,15 +142,24 @@ __device__ __forceinline__ double rect_bin_overlap(const Grid &g, const Rect &r,
     return overlap_area(l, b, rr, t, r.llx, r.lly, r.urx, r.ury);
 }
 
-// fastExp, PlaceCommon/global.h:457-471 (float, ten squarings).
+// fastExp, PlaceCommon/global.h:457-471 (float, ten squarings).  a / 1024 is
+// an exact power-of-two scaling, so the multiply rounds identically to the
+// reference's division.
 __device__ __forceinline__ float fast_exp(float a) {
-    a = __fadd_rn(1.0f, __fdiv_rn(a, 1024.0f));
+    a = __fadd_rn(1.0f, __fmul_rn(a, 0x1p-10f));
 #pragma unroll
     for (int i = 0; i < 10; i++) a = __fmul_rn(a, a);
     return a;
 }
 
-__device__ __forceinline__ float wl_exp(float a, int exact) { return exact ? expf(a) : fast_exp(a); }
+// ----- programmatic dependent launch ---------------------------------------------
+// Every kernel of the loop starts with pdl_begin(): wait until the previous
+// grid in the stream has completed and its writes are visible, then allow the
+// next grid to be scheduled (its blocks wait in their own pdl_begin).
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // ----- reductions ------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

@@ -51,6 +51,7 @@ constexpr int BM = 64, BN = 64, BK = 16;
 template <int EPI>
 __global__ void __launch_bounds__(256)
 k_sgemm_nt(int M, int N, int K, GemmArgs a, const DevScalars *__restrict__ S) {
+    pdl_begin();
     if (S && S->done) return;
     const int bz = blockIdx.z;
     const float *__restrict__ A = a.A[bz];
@@ -113,7 +114,7 @@ k_sgemm_nt(int M, int N, int K, GemmArgs a, const DevScalars *__restrict__ S) {
 template <int EPI>
 void sgemm(int M, int N, int K, int batch, const GemmArgs &a, const DevScalars *S, cudaStream_t st) {
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
-    k_sgemm_nt<EPI><<<grid, 256, 0, st>>>(M, N, K, a, S);
+    launch_k(k_sgemm_nt<EPI>, grid, 256, 0, st, M, N, K, a, S);
 }
 
 template <typename T>

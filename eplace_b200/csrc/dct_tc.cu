@@ -12,8 +12,9 @@
 //                        A and B from shared-memory descriptors, D in TMEM);
 //                        warp 1 also allocates / frees the TMEM columns
 //   warps 0-3          : epilogue, tcgen05.ld of their 32 TMEM lanes, then
-//                        the GEMM's store (bf16 hi/lo planes, transposed or
-//                        spectrally scaled, or the FP32 field)
+//                        the GEMM's store, always transposed (lane-contiguous):
+//                        bf16 hi/lo planes, optionally spectrally scaled, or
+//                        the FP32 field
 // Every wait on an mbarrier is bounded; a wait that gives up raises the
 // EP_ERR_TIMEOUT bit in DevScalars::status, the CTA drains what it issued,
 // frees its TMEM and returns.  No TMA multicast is used.
@@ -50,7 +51,7 @@ struct TcGemmParams {
     int epi;
     uint16_t *out_hi, *out_lo;  // bf16 planes (kTcTransposed / kTcSpectral)
     int ldo;
-    const float *kscale;        // spectral scale [M][N]
+    const float *kscale;        // spectral scale, laid out like the output
     float2 *field;              // kTcField, batches 0 (x) and 1 (y)
     float *phi;                 // kTcField, batch 2
 };
@@ -153,6 +154,7 @@ __device__ __forceinline__ void bf16_split(float v, uint16_t &hi, uint16_t &lo) 
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
+    pdl_begin();
     if (S && S->done) return;
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + kStages * kStageBytes);
@@ -234,7 +236,9 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     __syncwarp();
 
     // ---- epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows ----
-    // lane 0 waits, the warp follows its verdict (tcgen05.ld is warp-aligned)
+    // lane 0 waits, the warp follows its verdict (tcgen05.ld is warp-aligned).
+    // Every GEMM stores its tile transposed, C[m][n] -> out[n * ldo + m], so
+    // the 32 lanes of a warp (consecutive m) write consecutive addresses.
     int ready = 0;
     if (lane == 0) ready = mbar_wait(done, 0, abort) && !*abort;
     ready = __shfl_sync(0xffffffffu, ready, 0);
@@ -243,29 +247,32 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
         const int m = m0 + warp * 32 + lane;
 #pragma unroll 1
         for (int c0 = 0; c0 < kBN; c0 += 16) {
+            // spectral scale of these 16 columns, loaded before the stores
+            // so the loads do not queue behind them
+            float ks[16];
+            if (p.epi == kTcSpectral) {
+#pragma unroll
+                for (int c = 0; c < 16; c++) ks[c] = __ldg(&p.kscale[(size_t)(n0 + c0 + c) * p.ldo + m]);
+            }
             uint32_t r[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
 #pragma unroll
             for (int c = 0; c < 16; c++) {
-                const int n = n0 + c0 + c;
+                const size_t o = (size_t)(n0 + c0 + c) * p.ldo + m;
                 float v = __uint_as_float(r[c]);
-                if (p.epi == kTcTransposed) {
+                if (p.epi == kTcField) {
+                    if (bz == 0)
+                        p.field[o].x = v;
+                    else if (bz == 1)
+                        p.field[o].y = v;
+                    else
+                        p.phi[o] = v;
+                } else {
+                    if (p.epi == kTcSpectral) v *= ks[c];
                     uint16_t hi, lo;
                     bf16_split(v, hi, lo);
-                    p.out_hi[(size_t)n * p.ldo + m] = hi;
-                    p.out_lo[(size_t)n * p.ldo + m] = lo;
-                } else if (p.epi == kTcSpectral) {
-                    uint16_t hi, lo;
-                    bf16_split(v * p.kscale[(size_t)m * p.N + n], hi, lo);
-                    p.out_hi[(size_t)m * p.ldo + n] = hi;
-                    p.out_lo[(size_t)m * p.ldo + n] = lo;
-                } else {
-                    if (bz == 0)
-                        p.field[(size_t)m * p.N + n].x = v;
-                    else if (bz == 1)
-                        p.field[(size_t)m * p.N + n].y = v;
-                    else
-                        p.phi[(size_t)m * p.N + n] = v;
+                    p.out_hi[o] = hi;
+                    p.out_lo[o] = lo;
                 }
             }
         }
@@ -381,13 +388,14 @@ int dct_tc_init(DctPlan &p, std::string &err) {
     g1.out_hi = t->Tt; g1.out_lo = lo(t->Tt, nb); g1.ldo = nx;
     bool ok = make_map(&g1.a_hi[0], t->rho, nx, ny, kBM, err) && make_map(&g1.a_lo[0], lo(t->rho, nb), nx, ny, kBM, err) &&
               make_map(&g1.b_hi[0], t->Cy, ny, ny, kBN, err) && make_map(&g1.b_lo[0], lo(t->Cy, (size_t)ny * ny), ny, ny, kBN, err);
-    // G2: P[u][v] = K[u][v] sum_x Cx[u][x] Tt[v][x]
+    // G2: P[u][v] = K[u][v] sum_x Tt[v][x] Cx[u][x], run as C[v][u] (A = Tt,
+    // B = Cx) so the transposed store writes P[u][v]; K has P's layout
     TcGemmParams &g2 = t->g[1];
     std::memset(&g2, 0, sizeof(g2));
-    g2.M = nx; g2.N = ny; g2.K = nx; g2.epi = kTcSpectral;
+    g2.M = ny; g2.N = nx; g2.K = nx; g2.epi = kTcSpectral;
     g2.out_hi = t->P; g2.out_lo = lo(t->P, nb); g2.ldo = ny; g2.kscale = p.K;
-    ok = ok && make_map(&g2.a_hi[0], t->Cx, nx, nx, kBM, err) && make_map(&g2.a_lo[0], lo(t->Cx, (size_t)nx * nx), nx, nx, kBM, err) &&
-         make_map(&g2.b_hi[0], t->Tt, ny, nx, kBN, err) && make_map(&g2.b_lo[0], lo(t->Tt, nb), ny, nx, kBN, err);
+    ok = ok && make_map(&g2.a_hi[0], t->Tt, ny, nx, kBM, err) && make_map(&g2.a_lo[0], lo(t->Tt, nb), ny, nx, kBM, err) &&
+         make_map(&g2.b_hi[0], t->Cx, nx, nx, kBN, err) && make_map(&g2.b_lo[0], lo(t->Cx, (size_t)nx * nx), nx, nx, kBN, err);
     // G3: T3[n][u] = sum_v P[u][v] B3[n][v]
     TcGemmParams &g3 = t->g[2];
     std::memset(&g3, 0, sizeof(g3));
@@ -395,18 +403,20 @@ int dct_tc_init(DctPlan &p, std::string &err) {
     g3.out_hi = t->T3; g3.out_lo = lo(t->T3, 2 * nb); g3.ldo = nx;
     ok = ok && make_map(&g3.a_hi[0], t->P, nx, ny, kBM, err) && make_map(&g3.a_lo[0], lo(t->P, nb), nx, ny, kBM, err) &&
          make_map(&g3.b_hi[0], t->B3, 2 * ny, ny, kBN, err) && make_map(&g3.b_lo[0], lo(t->B3, (size_t)2 * ny * ny), 2 * ny, ny, kBN, err);
-    // G4: field[x][y] = sum_u A4{x,y}[x][u] {Ut,Vt}[y][u]; batch 2 = phi (A4y with Ut)
+    // G4: field[x][y] = sum_u {Ut,Vt}[y][u] A4{x,y}[x][u], run as C[y][x]
+    // (A = Ut / Vt, B = A4x / A4y) so the transposed store writes field[x][y];
+    // batch 2 = phi (Ut with A4y)
     TcGemmParams &g4 = t->g[3];
     std::memset(&g4, 0, sizeof(g4));
-    g4.M = nx; g4.N = ny; g4.K = nx; g4.epi = kTcField;
+    g4.M = ny; g4.N = nx; g4.K = nx; g4.epi = kTcField; g4.ldo = ny;
     const size_t a4 = (size_t)2 * nx * nx;  // lo plane offset of A4
     const size_t t3 = (size_t)2 * nb;       // lo plane offset of T3
     uint16_t *A4x = t->A4, *A4y = t->A4 + (size_t)nx * nx;
     uint16_t *Ut = t->T3, *Vt = t->T3 + nb;
-    uint16_t *As[3] = {A4x, A4y, A4y}, *Bs[3] = {Ut, Vt, Ut};
+    uint16_t *As[3] = {Ut, Vt, Ut}, *Bs[3] = {A4x, A4y, A4y};
     for (int b = 0; b < 3 && ok; b++)
-        ok = make_map(&g4.a_hi[b], As[b], nx, nx, kBM, err) && make_map(&g4.a_lo[b], As[b] + a4, nx, nx, kBM, err) &&
-             make_map(&g4.b_hi[b], Bs[b], ny, nx, kBN, err) && make_map(&g4.b_lo[b], Bs[b] + t3, ny, nx, kBN, err);
+        ok = make_map(&g4.a_hi[b], As[b], ny, nx, kBM, err) && make_map(&g4.a_lo[b], As[b] + t3, ny, nx, kBM, err) &&
+             make_map(&g4.b_hi[b], Bs[b], nx, nx, kBN, err) && make_map(&g4.b_lo[b], Bs[b] + a4, nx, nx, kBN, err);
     if (!ok) return EP_ERR_UNSUPPORTED;
     if (cudaFuncSetAttribute(k_umma_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess) {
         err = "cannot raise the dynamic shared memory limit of the tcgen05 GEMM";
@@ -438,7 +448,7 @@ int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaS
             batch = phi ? 3 : 2;
         }
         dim3 grid(g.N / kBN, g.M / kBM, batch);
-        k_umma_nt<<<grid, kThreads, kSmemBytes, st>>>(g, s);
+        launch_k(k_umma_nt, grid, kThreads, kSmemBytes, st, g, s);
     }
     return EP_OK;
 }

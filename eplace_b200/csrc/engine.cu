@@ -46,9 +46,11 @@ struct ep_engine {
     float2 *staging = nullptr;
     uint8_t *flags = nullptr;
     float *npins = nullptr, *area = nullptr, *rho = nullptr, *node_f = nullptr, *filler_f = nullptr;
+    float *sxy = nullptr;
     float *phi = nullptr;
-    int32_t *net_start = nullptr, *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pins = nullptr;
-    int32_t *small_nets = nullptr, *big_nets = nullptr, *big_objs = nullptr, *big_slot = nullptr;
+    int32_t *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pin_dev = nullptr;
+    int32_t *big_objs = nullptr, *big_slot = nullptr;
+    int4 *net_tasks = nullptr;
     int32_t *view_idx[3] = {nullptr, nullptr, nullptr};
     unsigned long long *node_q = nullptr, *filler_q = nullptr;
     DevScalars *S = nullptr;
@@ -253,11 +255,10 @@ ep_status device_status(ep_engine *e) {
 // Kernels one enqueue_eval launches (the DCT is four GEMMs).
 int kernels_per_eval(const ep_engine *e) {
     const DeviceNetlist &d = e->dn;
-    return 1 + (d.n_big_objs > 0) + 1 + 4 + (d.n_small_nets > 0) + (d.n_big_nets > 0) +
-           (d.n_big_objs > 0) + 1;
+    return 1 + (d.n_big_objs > 0) + 1 + 4 + (d.n_net_tasks > 0) + (d.n_big_objs > 0) + 1;
 }
 
-int kernels_per_hpwl(const ep_engine *e) { return (e->dn.n_small_nets > 0) + (e->dn.n_big_nets > 0); }
+int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
 
 // totalGradientUpdate: enqueue one gradient evaluation at the current positions.
 void enqueue_eval(ep_engine *e, int stepping) {
@@ -492,6 +493,8 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     g.ny = nby;
     g.sx = (right - left) / (float)nbx;
     g.sy = (top - bottom) / (float)nby;
+    g.isx = 1.0f / g.sx;
+    g.isy = 1.0f / g.sy;
     const int nb = nbx * nby;
     const float bin_area_f = g.sx * g.sy;
 
@@ -579,10 +582,23 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     for (int t = 0; t < nt; t++)
         pos[no + t] = make_float2(nl->term_llx[t] + (float)0.5 * nl->term_w[t],
                                   nl->term_lly[t] + (float)0.5 * nl->term_h[t]);
-    // big objects: may cover more bins than the thread-per-object path loops over
+    // big objects: may cover more bins than the thread-per-object path loops over.
+    // Local smoothing depends on the size only, so its flags and sx*sy scale
+    // are fixed here (EPlace/eplace.cpp:1061-1072, float division and product).
     std::vector<int32_t> big, big_slot(no, -1);
+    std::vector<float> h_sxy(no);
     for (int o = 0; o < no; o++) {
         float w = e->h_size[o].x, h = e->h_size[o].y;
+        float fsx = 1.0f, fsy = 1.0f;
+        if (f_less_h(w, g.sx)) {
+            e->h_flags[o] |= kSmoothX;
+            fsx = w / g.sx;
+        }
+        if (f_less_h(h, g.sy)) {
+            e->h_flags[o] |= kSmoothY;
+            fsy = h / g.sy;
+        }
+        h_sxy[o] = fsx * fsy;
         long sx = f_less_h(w, g.sx) ? 2 : (long)(w / g.sx) + 2;
         long sy = f_less_h(h, g.sy) ? 2 : (long)(h / g.sy) + 2;
         if (sx * sy > kSmallObjectBins) {
@@ -602,18 +618,63 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         off[p] = make_float2(nl->pin_dx[p], nl->pin_dy[p]);
         if (ow < nn) h_npins[ow] += 1.0f;
     }
-    std::vector<int32_t> ops(no + 1, 0), opins(np);
+    // each object's pins in the reference's pin order (pin_slot: place of a
+    // pin in that list), so the gradient sum runs in the reference's order
+    std::vector<int32_t> ops(no + 1, 0), pin_slot(np, -1);
     for (int p = 0; p < np; p++)
         if (owner[p] < no) ops[owner[p] + 1]++;
     for (int o = 0; o < no; o++) ops[o + 1] += ops[o];
     {
         std::vector<int32_t> fill(ops.begin(), ops.end() - 1);
         for (int p = 0; p < np; p++)
-            if (owner[p] < no) opins[fill[owner[p]]++] = p;
+            if (owner[p] < no) pin_slot[p] = fill[owner[p]]++;
     }
-    std::vector<int32_t> small_nets, big_nets;
-    for (int n = 0; n < nnet; n++)
-        (net_start[n + 1] - net_start[n] <= kSmallNetDegree ? small_nets : big_nets).push_back(n);
+    // Device pin order for the per-net pass (kernels.cu): nets above
+    // kWarpPins pins first, largest first (a warp each), then degree
+    // kWarpPins down to 1, floor(kWarpPins / degree) nets per warp; original
+    // order inside a degree.  Nets without pins take no task.
+    std::vector<int4> net_tasks;
+    std::vector<int32_t> dev_owner(np), dev_of_pin(np);
+    std::vector<float2> dev_off(np);
+    {
+        std::vector<std::vector<int>> by_deg(kWarpPins + 1);
+        std::vector<int> big_list;
+        for (int n = 0; n < nnet; n++) {
+            int deg = net_start[n + 1] - net_start[n];
+            (deg > kWarpPins ? big_list : by_deg[deg]).push_back(n);
+        }
+        std::stable_sort(big_list.begin(), big_list.end(), [&](int a, int b) {
+            return net_start[a + 1] - net_start[a] > net_start[b + 1] - net_start[b];
+        });
+        int q = 0;
+        auto put_net = [&](int n) {
+            int a = net_start[n], deg = net_start[n + 1] - a;
+            for (int k = 0; k < deg; k++) {
+                dev_owner[q + k] = owner[a + k];
+                dev_off[q + k] = off[a + k];
+                dev_of_pin[a + k] = q + k;
+            }
+            int at = q;
+            q += deg;
+            return at;
+        };
+        for (int n : big_list) {
+            int at = put_net(n);
+            net_tasks.push_back(make_int4(net_start[n + 1] - net_start[n], at, 1, 0));
+        }
+        for (int d = kWarpPins; d >= 1; d--) {
+            const size_t per = kWarpPins / d;
+            for (size_t i = 0; i < by_deg[d].size(); i += per) {
+                int first = q, count = (int)std::min(per, by_deg[d].size() - i);
+                for (int j = 0; j < count; j++) put_net(by_deg[d][i + j]);
+                net_tasks.push_back(make_int4(d, first, count, (65536 + d - 1) / d));
+            }
+        }
+    }
+    // each object's pins (reference order) -> their device positions
+    std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0);
+    for (int p = 0; p < np; p++)
+        if (pin_slot[p] >= 0) obj_pin_dev[pin_slot[p]] = dev_of_pin[p];
 
     // stage views (EPlace/eplace.cpp:190-203)
     for (int o = 0; o < no; o++) {
@@ -637,19 +698,20 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     kc.area_norm = (double)(sa + ma * P.target_density);
     kc.exact_exp = P.exp_mode == EP_EXP_EXACT;
     kc.lse = P.wl_model == EP_WL_LSE;
+    kc.want_wl_value = P.keep_maps ? 1 : 0;
 
     // ---- device ----
     if ((s = dupload(e, e->pos, pos)) || (s = dalloc(e, e->x, no)) || (s = dalloc(e, e->g, no)) ||
         (s = dalloc(e, e->y_prev, no)) || (s = dalloc(e, e->g_prev, no)) ||
-        (s = dupload(e, e->size, e->h_size)) || (s = dupload(e, e->pin_off, off)) ||
+        (s = dupload(e, e->size, e->h_size)) || (s = dupload(e, e->pin_off, dev_off)) ||
         (s = dalloc(e, e->pin_grad, np)) || (s = dalloc(e, e->gd_big, big.size())) ||
         (s = dalloc(e, e->field, nb)) || (s = dupload(e, e->static_map, stat)) ||
         (s = dalloc(e, e->staging, no)) || (s = dalloc(e, e->flags, no)) ||
         (s = dupload(e, e->npins, h_npins)) || (s = dupload(e, e->area, h_area)) ||
-        (s = dalloc(e, e->rho, nb)) || (s = dupload(e, e->net_start, net_start)) ||
-        (s = dupload(e, e->pin_owner, owner)) || (s = dupload(e, e->obj_pin_start, ops)) ||
-        (s = dupload(e, e->obj_pins, opins)) || (s = dupload(e, e->small_nets, small_nets)) ||
-        (s = dupload(e, e->big_nets, big_nets)) || (s = dupload(e, e->big_objs, big)) ||
+        (s = dalloc(e, e->rho, nb)) || (s = dupload(e, e->sxy, h_sxy)) ||
+        (s = dupload(e, e->pin_owner, dev_owner)) || (s = dupload(e, e->obj_pin_start, ops)) ||
+        (s = dupload(e, e->obj_pin_dev, obj_pin_dev)) || (s = dupload(e, e->net_tasks, net_tasks)) ||
+        (s = dupload(e, e->big_objs, big)) ||
         (s = dupload(e, e->big_slot, big_slot)) || (s = dalloc(e, e->node_q, nb)) ||
         (s = dalloc(e, e->filler_q, nb)) || (s = dalloc(e, e->S, 1)))
         return s;
@@ -688,15 +750,13 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     d.flags = e->flags;
     d.npins = e->npins;
     d.area = e->area;
-    d.net_start = e->net_start;
+    d.sxy = e->sxy;
     d.pin_owner = e->pin_owner;
     d.pin_off = e->pin_off;
     d.obj_pin_start = e->obj_pin_start;
-    d.obj_pins = e->obj_pins;
-    d.small_nets = e->small_nets;
-    d.big_nets = e->big_nets;
-    d.n_small_nets = (int)small_nets.size();
-    d.n_big_nets = (int)big_nets.size();
+    d.obj_pin_dev = e->obj_pin_dev;
+    d.net_tasks = e->net_tasks;
+    d.n_net_tasks = (int)net_tasks.size();
     d.big_objs = e->big_objs;
     d.big_slot = e->big_slot;
     d.n_big_objs = (int)big.size();
@@ -1149,18 +1209,25 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
                      auto &&before) -> ep_status {
         int k = out->count++;
         std::snprintf(out->names[k], sizeof(out->names[k]), "%s", name);
-        double tot = 0;
+        // reps back-to-back launches (as in the loop: no host gaps), minus
+        // the same number of the per-repetition setup alone
+        before();
+        fn();
+        float ms_all = 0, ms_setup = 0;
+        CK(cudaEventRecord(a, e->st));
         for (int r = 0; r < reps; r++) {
             before();
-            CK(cudaEventRecord(a, e->st));
             fn();
-            CK(cudaEventRecord(b, e->st));
-            CK(cudaEventSynchronize(b));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, a, b);
-            tot += ms;
         }
-        out->ms[k] = tot / reps;
+        CK(cudaEventRecord(b, e->st));
+        CK(cudaEventSynchronize(b));
+        cudaEventElapsedTime(&ms_all, a, b);
+        CK(cudaEventRecord(a, e->st));
+        for (int r = 0; r < reps; r++) before();
+        CK(cudaEventRecord(b, e->st));
+        CK(cudaEventSynchronize(b));
+        cudaEventElapsedTime(&ms_setup, a, b);
+        out->ms[k] = std::max(0.0, (double)ms_all - (double)ms_setup) / reps;
         out->bytes[k] = bytes;
         out->flops[k] = flops;
         out->launches[k] = launches;
@@ -1188,7 +1255,7 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
     s = timed("poisson_dct", 4, 16.0 * nbin, dct_flops,
               [&] { dct_run(e->dct, e->rho, e->field, nullptr, e->S, e->st); }, nothing);
     if (s) return s;
-    s = timed("wirelength", (d.n_small_nets > 0) + (d.n_big_nets > 0), 28.0 * npin + 8.0 * nnet, 0.0,
+    s = timed("wirelength", d.n_net_tasks > 0, 28.0 * npin + 16.0 * d.n_net_tasks, 0.0,
               [&] { launch_wirelength(e->kc, d, e->pin_grad, e->S, e->st); }, nothing);
     if (s) return s;
     if (d.n_big_objs > 0) {

@@ -6,14 +6,36 @@
 #include <string>
 #include <vector>
 
-#include "../../include/eplace_gpu.h"
+#include "eplace_gpu.h"
 #include "common.cuh"
 
 namespace ep {
 
-// Nets up to this degree take the thread-per-net path (sequential float sums
-// in pin order, as Net::calcWirelengthWA_2D does); larger nets a warp each.
-constexpr int kSmallNetDegree = 16;
+// Launch with programmatic stream serialization (the kernel's pdl_begin()
+// orders it after the previous grid); captured into graphs as programmatic
+// edges.
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+// Per-net pass: one warp per task.  Nets of up to kWarpPins pins share a warp
+// (floor(kWarpPins / degree) nets of one degree, a pin per lane); larger nets
+// take a warp each, their first kStagedPins pins staged in shared memory.
+constexpr int kWarpPins = 32;
+constexpr int kStagedPins = 256;
+constexpr int kNetWarps = 8;  // warps per block of the per-net pass
 // Objects whose bin footprint may exceed this many bins take the
 // block-per-object scatter / gather path.
 constexpr int kSmallObjectBins = 16;
@@ -48,11 +70,16 @@ struct DeviceNetlist {
     const uint8_t *flags;    // [n_obj]
     const float *npins;      // [n_obj] pin count (float, as the preconditioner reads it)
     const float *area;       // [n_obj] Module::area
-    const int32_t *net_start, *pin_owner;
+    const float *sxy;        // [n_obj] local-smoothing scale sx*sy (EPlace/eplace.cpp:1061-1072)
+    // pins in DEVICE order: nets grouped by degree (see the per-net pass in
+    // kernels.cu); obj_pin_dev maps each object's pins to their positions
+    const int32_t *pin_owner;
     const float2 *pin_off;
-    const int32_t *obj_pin_start, *obj_pins;
-    const int32_t *small_nets, *big_nets;
-    int n_small_nets, n_big_nets;
+    const int32_t *obj_pin_start;  // [n_obj + 1] object -> its pins (reference pin order)
+    const int32_t *obj_pin_dev;    // device position of each of those pins
+    const int4 *net_tasks;         // per warp of the per-net pass: degree, first pin, nets,
+                                   // ceil(2^16 / degree) (0 for nets above kWarpPins pins)
+    int n_net_tasks;
     const int32_t *big_objs;  // indices of kBig objects
     const int32_t *big_slot;  // object -> index in big_objs (or -1)
     int n_big_objs;
@@ -64,6 +91,7 @@ struct KernelCtx {
     double bin_area, inv_bin_area;
     double area_norm;  // stdArea + macroArea * td (overflow denominator)
     int exact_exp, lse;
+    int want_wl_value;  // also sum the smooth wirelength value (off in the hot loop)
     // per-block partials of the deterministic grid reductions
     double *part_prep, *part_wl, *part_comb, *part_hp;
 };

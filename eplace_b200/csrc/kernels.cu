@@ -56,6 +56,7 @@ k_scatter_small(Grid g, const float2 *__restrict__ pos, const float2 *__restrict
                 const uint8_t *__restrict__ flags, int n, double qscale,
                 unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
                 const DevScalars *__restrict__ S) {
+    pdl_begin();
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
@@ -76,6 +77,7 @@ k_scatter_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__
               const uint8_t *__restrict__ flags, const int32_t *__restrict__ big, double qscale,
               unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
               const DevScalars *__restrict__ S) {
+    pdl_begin();
     if (S->done) return;
     int o = big[blockIdx.x];
     uint8_t f = flags[o];
@@ -119,6 +121,7 @@ k_prep(Grid g, unsigned long long *__restrict__ node_q, unsigned long long *__re
        uint16_t *__restrict__ rho_lo, float *__restrict__ node_f, float *__restrict__ filler_f,
        int zero, double inv_q, double inv_bin_area, double bin_area, double area_norm,
        double *__restrict__ partials, DevScalars *__restrict__ S) {
+    pdl_begin();
     __shared__ double sh[32];
     if (S->done) return;
     int nb = g.nx * g.ny;
@@ -186,83 +189,82 @@ struct NetSums {
     float nmx, dmx, nnx, dnx, nmy, dmy, nny, dny;
 };
 
-// Per-pin gradient of the WA model (objects.cpp:359-415) or LSE (:423-437).
-__device__ __forceinline__ float2 pin_gradient(float2 xy, float x1, float x0, float y1, float y0,
-                                               float igx, float igy, const NetSums &s, int exact,
-                                               int lse) {
-    float amx = __fmul_rn(__fsub_rn(xy.x, x1), igx);
-    float anx = __fmul_rn(__fsub_rn(x0, xy.x), igx);
-    float amy = __fmul_rn(__fsub_rn(xy.y, y1), igy);
-    float any = __fmul_rn(__fsub_rn(y0, xy.y), igy);
-    bool fmx = amx > (float)kNegMaxExp, fnx = anx > (float)kNegMaxExp;
-    bool fmy = amy > (float)kNegMaxExp, fny = any > (float)kNegMaxExp;
-    float emx = fmx ? wl_exp(amx, exact) : 0.0f;
-    float enx = fnx ? wl_exp(anx, exact) : 0.0f;
-    float emy = fmy ? wl_exp(amy, exact) : 0.0f;
-    float eny = fny ? wl_exp(any, exact) : 0.0f;
-    float2 gr;
-    if (lse) {
-        gr.x = __fsub_rn(__fdiv_rn(emx, s.dmx), __fdiv_rn(enx, s.dnx));
-        gr.y = __fsub_rn(__fdiv_rn(emy, s.dmy), __fdiv_rn(eny, s.dny));
-        return gr;
-    }
-    float gmx = 0.f, gnx = 0.f, gmy = 0.f, gny = 0.f;
-    if (fmx) {
-        float dd = __fmul_rn(igx, emx);
-        float nd = __fadd_rn(emx, __fmul_rn(xy.x, dd));
-        gmx = __fdiv_rn(__fsub_rn(__fmul_rn(nd, s.dmx), __fmul_rn(dd, s.nmx)), __fmul_rn(s.dmx, s.dmx));
-    }
-    if (fmy) {
-        float dd = __fmul_rn(igy, emy);
-        float nd = __fadd_rn(emy, __fmul_rn(xy.y, dd));
-        gmy = __fdiv_rn(__fsub_rn(__fmul_rn(nd, s.dmy), __fmul_rn(dd, s.nmy)), __fmul_rn(s.dmy, s.dmy));
-    }
-    if (fnx) {
-        float dd = __fmul_rn(igx, enx);
-        float nd = __fsub_rn(enx, __fmul_rn(xy.x, dd));
-        gnx = __fdiv_rn(__fadd_rn(__fmul_rn(nd, s.dnx), __fmul_rn(dd, s.nnx)), __fmul_rn(s.dnx, s.dnx));
-    }
-    if (fny) {
-        float dd = __fmul_rn(igy, eny);
-        float nd = __fsub_rn(eny, __fmul_rn(xy.y, dd));
-        gny = __fdiv_rn(__fadd_rn(__fmul_rn(nd, s.dny), __fmul_rn(dd, s.nny)), __fmul_rn(s.dny, s.dny));
-    }
-    gr.x = __fsub_rn(gmx, gnx);
-    gr.y = __fsub_rn(gmy, gny);
-    return gr;
+// Exponential terms of one pin (calcWirelengthWA_2D, objects.cpp:275-332):
+// arguments <= -300 make the term zero.
+struct PinExp {
+    float emx, enx, emy, eny;
+};
+
+template <bool EXACT>
+__device__ __forceinline__ float term_exp(float a) {
+    if (!(a > (float)kNegMaxExp)) return 0.0f;
+    return EXACT ? expf(a) : fast_exp(a);
 }
 
-// Accumulate one pin into the net sums (calcWirelengthWA_2D order).
-__device__ __forceinline__ void add_pin(NetSums &s, float2 xy, float x1, float x0, float y1,
-                                        float y0, float igx, float igy, int exact) {
-    float amx = __fmul_rn(__fsub_rn(xy.x, x1), igx);
-    float anx = __fmul_rn(__fsub_rn(x0, xy.x), igx);
-    float amy = __fmul_rn(__fsub_rn(xy.y, y1), igy);
-    float any = __fmul_rn(__fsub_rn(y0, xy.y), igy);
-    if (amx > (float)kNegMaxExp) {
-        float e = wl_exp(amx, exact);
-        s.nmx = __fadd_rn(s.nmx, __fmul_rn(xy.x, e));
-        s.dmx = __fadd_rn(s.dmx, e);
-    }
-    if (anx > (float)kNegMaxExp) {
-        float e = wl_exp(anx, exact);
-        s.nnx = __fadd_rn(s.nnx, __fmul_rn(xy.x, e));
-        s.dnx = __fadd_rn(s.dnx, e);
-    }
-    if (amy > (float)kNegMaxExp) {
-        float e = wl_exp(amy, exact);
-        s.nmy = __fadd_rn(s.nmy, __fmul_rn(xy.y, e));
-        s.dmy = __fadd_rn(s.dmy, e);
-    }
-    if (any > (float)kNegMaxExp) {
-        float e = wl_exp(any, exact);
-        s.nny = __fadd_rn(s.nny, __fmul_rn(xy.y, e));
-        s.dny = __fadd_rn(s.dny, e);
-    }
+template <bool EXACT>
+__device__ __forceinline__ PinExp pin_exps(float2 xy, float x1, float x0, float y1, float y0, float igx,
+                                           float igy) {
+    PinExp e;
+    e.emx = term_exp<EXACT>(__fmul_rn(__fsub_rn(xy.x, x1), igx));
+    e.enx = term_exp<EXACT>(__fmul_rn(__fsub_rn(x0, xy.x), igx));
+    e.emy = term_exp<EXACT>(__fmul_rn(__fsub_rn(xy.y, y1), igy));
+    e.eny = term_exp<EXACT>(__fmul_rn(__fsub_rn(y0, xy.y), igy));
+    return e;
+}
+
+// Add one pin's terms to a running sum set (calcWirelengthWA_2D's sums).
+__device__ __forceinline__ void add_terms(float (&s)[8], const PinExp &e, float2 xy) {
+    s[0] = __fadd_rn(s[0], __fmul_rn(xy.x, e.emx));
+    s[1] = __fadd_rn(s[1], e.emx);
+    s[2] = __fadd_rn(s[2], __fmul_rn(xy.x, e.enx));
+    s[3] = __fadd_rn(s[3], e.enx);
+    s[4] = __fadd_rn(s[4], __fmul_rn(xy.y, e.emy));
+    s[5] = __fadd_rn(s[5], e.emy);
+    s[6] = __fadd_rn(s[6], __fmul_rn(xy.y, e.eny));
+    s[7] = __fadd_rn(s[7], e.eny);
+}
+
+// Per-net factors of the gradient: 1 / (sum of exponentials) and the
+// exponentially weighted mean coordinate of each of the four terms.  Every
+// denominator holds the bound pin's exp(0) = 1, so it is >= 1.
+struct NetCoef {
+    float rmx, mmx, rnx, mnx, rmy, mmy, rny, mny;
+};
+
+__device__ __forceinline__ NetCoef net_coef(const NetSums &s) {
+    NetCoef c;
+    c.rmx = __frcp_rn(s.dmx);
+    c.rnx = __frcp_rn(s.dnx);
+    c.rmy = __frcp_rn(s.dmy);
+    c.rny = __frcp_rn(s.dny);
+    c.mmx = s.nmx * c.rmx;
+    c.mnx = s.nnx * c.rnx;
+    c.mmy = s.nmy * c.rmy;
+    c.mny = s.nny * c.rny;
+    return c;
+}
+
+// Per-pin gradient of the WA model (objects.cpp:359-415).  The reference's
+// (nd * d - dd * n) / d^2 equals e / d * (1 + (x - n / d) / gamma) for the max
+// term and e / d * (1 - (x - n / d) / gamma) for the min term; this form
+// subtracts the weighted mean from the coordinate before scaling, which
+// avoids the cancellation of the expanded quotient (the two agree to the
+// reference's own rounding).  A zero exponential (argument <= -300) gives a
+// zero term as in the reference.  LSE (:423-437): e / d per term.
+template <bool LSE>
+__device__ __forceinline__ float2 pin_gradient(const PinExp &e, float2 xy, float igx, float igy,
+                                               const NetCoef &c) {
+    if (LSE)
+        return make_float2(e.emx * c.rmx - e.enx * c.rnx, e.emy * c.rmy - e.eny * c.rny);
+    const float gmx = e.emx * c.rmx * fmaf(igx, xy.x - c.mmx, 1.0f);
+    const float gnx = e.enx * c.rnx * fmaf(-igx, xy.x - c.mnx, 1.0f);
+    const float gmy = e.emy * c.rmy * fmaf(igy, xy.y - c.mmy, 1.0f);
+    const float gny = e.eny * c.rny * fmaf(-igy, xy.y - c.mny, 1.0f);
+    return make_float2(gmx - gnx, gmy - gny);
 }
 
 __device__ __forceinline__ double net_value(const NetSums &s, float x1, float x0, float y1,
-                                            float y0, float igx, float igy, int lse) {
+                                            float y0, float igx, float igy, bool lse) {
     if (lse)
         return ((double)x1 - x0 + log((double)s.dmx) / igx + log((double)s.dnx) / igx) +
                ((double)y1 - y0 + log((double)s.dmy) / igy + log((double)s.dny) / igy);
@@ -300,99 +302,170 @@ __device__ void finish_hpwl(DevScalars *S, double hp, int mode) {
     }
 }
 
-// Thread per net (sequential float sums in pin order, as the reference).
-// WL = false computes only the HPWL, with the same thread layout and
-// reduction tree, so both passes give bitwise the same HPWL.
-template <bool WL>
-__global__ void __launch_bounds__(kThreads)
-k_wl_small(const int32_t *__restrict__ nets, int n_list, const int32_t *__restrict__ net_start,
-           PinCtx pc, float2 *__restrict__ pin_grad, int exact, int lse, unsigned total_blocks,
-           unsigned block_base, double *__restrict__ partials, int mode, DevScalars *__restrict__ S) {
-    __shared__ double sh[64];
-    if (WL && S->done) return;
-    float igx = (float)S->inv_gamma_x, igy = (float)S->inv_gamma_y;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[2] = {0.0, 0.0};
-    if (t < n_list) {
-        int n = nets[t];
-        int a = net_start[n], b = net_start[n + 1];
-        // bound pins (Net::calcBoundPin): strict compares keep the first pin
-        float x0 = 3.4e38f, x1 = -3.4e38f, y0 = 3.4e38f, y1 = -3.4e38f;
-        for (int p = a; p < b; p++) {
-            float2 xy = pin_xy(pc, p);
-            if (xy.x < x0) x0 = xy.x;
-            if (xy.x > x1) x1 = xy.x;
-            if (xy.y < y0) y0 = xy.y;
-            if (xy.y > y1) y1 = xy.y;
-        }
-        acc[0] = ((double)x1 - (double)x0) + ((double)y1 - (double)y0);
-        if (WL) {
-            NetSums s = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (int p = a; p < b; p++) add_pin(s, pin_xy(pc, p), x1, x0, y1, y0, igx, igy, exact);
-            acc[1] = net_value(s, x1, x0, y1, y0, igx, igy, lse);
-            for (int p = a; p < b; p++)
-                pin_grad[p] = pin_gradient(pin_xy(pc, p), x1, x0, y1, y0, igx, igy, s, exact, lse);
-        }
-    }
-    if (grid_sum<2>(acc, sh, partials, WL ? &S->cnt_wl : &S->cnt_hp, total_blocks,
-                    block_base + blockIdx.x) &&
-        threadIdx.x == 0) {
-        if (WL)
-            finish_wirelength(S, acc[0], acc[1]);
-        else
-            finish_hpwl(S, acc[0], mode);
+// ---- the per-net pass ---------------------------------------------------------
+// On the device the nets are ordered by degree and each warp runs one task
+// (tasks[w] = degree D, first pin, nets, m):
+//   D <= kWarpPins: the task's nets (up to floor(32 / D), all of degree D)
+//       sit on lanes s*D .. s*D+D-1, one pin per lane (s = lane * m >> 16,
+//       m = ceil(2^16 / D), exact for lanes < 32), and the bound pins and
+//       exponential sums are segmented shuffle reductions over those lanes;
+//   D >  kWarpPins: one net; the warp strides over its pins, keeping the
+//       first kStagedPins of them in shared memory between the passes.
+// Nets above kWarpPins pins come first (largest first), then degree 32 down
+// to 1, so the long tasks start early.  The sums are FP32 as in
+// Net::calcWirelengthWA_2D, added in a fixed tree order instead of pin order
+// (a few ulps apart).  Pin gradients are written in device pin order
+// (coalesced); the combine kernel gathers them back in each object's
+// reference pin order.  WL = false computes only the HPWL with the same
+// layout and reduction tree, so both passes give bitwise the same HPWL.
+struct NetOut {
+    double hpwl, value;
+};
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Bound pins of each aligned segment of D lanes (segment base `base`, this
+// lane's index k in it); every lane of the segment gets them.  The windows
+// double cyclically, which is exact for max / min.
+__device__ __forceinline__ void seg_bounds(float &x1, float &x0, float &y1, float &y0, int D,
+                                           int base, int k) {
+    for (int o = 1; o < D; o <<= 1) {
+        const int j = k + o;
+        const int src = base + (j < D ? j : j - D);
+        x1 = fmaxf(x1, __shfl_sync(kFull, x1, src));
+        x0 = fminf(x0, __shfl_sync(kFull, x0, src));
+        y1 = fmaxf(y1, __shfl_sync(kFull, y1, src));
+        y0 = fminf(y0, __shfl_sync(kFull, y0, src));
     }
 }
 
-// Warp per net for high-degree nets (lane-strided pins, tree reductions).
-template <bool WL>
-__global__ void __launch_bounds__(kThreads)
-k_wl_big(const int32_t *__restrict__ nets, int n_list, const int32_t *__restrict__ net_start,
-         PinCtx pc, float2 *__restrict__ pin_grad, int exact, int lse, unsigned total_blocks,
-         unsigned block_base, double *__restrict__ partials, int mode, DevScalars *__restrict__ S) {
-    __shared__ double sh[64];
-    if (WL && S->done) return;
-    float igx = (float)S->inv_gamma_x, igy = (float)S->inv_gamma_y;
-    int lane = threadIdx.x & 31;
-    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    double acc[2] = {0.0, 0.0};
-    if (w < n_list) {
-        int n = nets[w];
-        int a = net_start[n], b = net_start[n + 1];
-        float x0 = 3.4e38f, x1 = -3.4e38f, y0 = 3.4e38f, y1 = -3.4e38f;
-        for (int p = a + lane; p < b; p += 32) {
-            float2 xy = pin_xy(pc, p);
-            x0 = fminf(x0, xy.x);
-            x1 = fmaxf(x1, xy.x);
-            y0 = fminf(y0, xy.y);
-            y1 = fmaxf(y1, xy.y);
-        }
-        x0 = warp_min(x0);
-        x1 = warp_max(x1);
-        y0 = warp_min(y0);
-        y1 = warp_max(y1);
-        NetSums s = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (WL) {
-            for (int p = a + lane; p < b; p += 32) add_pin(s, pin_xy(pc, p), x1, x0, y1, y0, igx, igy, exact);
-            s.nmx = warp_sum_f(s.nmx);
-            s.dmx = warp_sum_f(s.dmx);
-            s.nnx = warp_sum_f(s.nnx);
-            s.dnx = warp_sum_f(s.dnx);
-            s.nmy = warp_sum_f(s.nmy);
-            s.dmy = warp_sum_f(s.dmy);
-            s.nny = warp_sum_f(s.nny);
-            s.dny = warp_sum_f(s.dny);
-            for (int p = a + lane; p < b; p += 32)
-                pin_grad[p] = pin_gradient(pin_xy(pc, p), x1, x0, y1, y0, igx, igy, s, exact, lse);
-        }
-        if (lane == 0) {
-            acc[0] = ((double)x1 - (double)x0) + ((double)y1 - (double)y0);
-            if (WL) acc[1] = net_value(s, x1, x0, y1, y0, igx, igy, lse);
+// The eight exponential sums of each segment, every lane of the segment gets
+// bitwise the same totals: a butterfly when D is a power of two, else a tree
+// into the segment's first lane and a broadcast.
+__device__ __forceinline__ void seg_sums(float (&s)[8], int D, int base, int k) {
+    if ((D & (D - 1)) == 0) {
+        for (int o = D >> 1; o > 0; o >>= 1)
+#pragma unroll
+            for (int i = 0; i < 8; i++) s[i] = __fadd_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
+        return;
+    }
+    for (int o = 1; o < D; o <<= 1) {
+        const bool take = k + o < D;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float t = __shfl_down_sync(kFull, s[i], o);
+            if (take) s[i] = __fadd_rn(s[i], t);
         }
     }
-    if (grid_sum<2>(acc, sh, partials, WL ? &S->cnt_wl : &S->cnt_hp, total_blocks,
-                    block_base + blockIdx.x) &&
-        threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) s[i] = __shfl_sync(kFull, s[i], base);
+}
+
+__device__ __forceinline__ NetSums net_sums(const float (&s)[8]) {
+    return NetSums{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7]};
+}
+
+// Nets of degree D <= 32 packed on the lanes of one warp.
+template <bool WL, bool EXACT, bool LSE>
+__device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const PinCtx &pc,
+                                               float2 *__restrict__ out, float igx, float igy,
+                                               int want_value) {
+    const int D = t.x, p0 = t.y;
+    const int seg = (lane * t.w) >> 16, base = seg * D, k = lane - base;
+    const bool act = seg < t.z;
+    const float2 xy = act ? pin_xy(pc, p0 + lane) : make_float2(0.f, 0.f);
+    // bound pins (Net::calcBoundPin, PlaceCommon/objects.cpp:75-144)
+    float x1 = xy.x, x0 = xy.x, y1 = xy.y, y0 = xy.y;
+    seg_bounds(x1, x0, y1, y0, D, base, k);
+    NetOut r{0.0, 0.0};
+    if (act && k == 0) r.hpwl = ((double)x1 - (double)x0) + ((double)y1 - (double)y0);
+    if (WL) {
+        const PinExp e = pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy);
+        float s[8] = {__fmul_rn(xy.x, e.emx), e.emx, __fmul_rn(xy.x, e.enx), e.enx,
+                      __fmul_rn(xy.y, e.emy), e.emy, __fmul_rn(xy.y, e.eny), e.eny};
+        seg_sums(s, D, base, k);
+        const NetSums ns = net_sums(s);
+        if (act) out[p0 + lane] = pin_gradient<LSE>(e, xy, igx, igy, net_coef(ns));
+        if (want_value && act && k == 0) r.value = net_value(ns, x1, x0, y1, y0, igx, igy, LSE);
+    }
+    return r;
+}
+
+// One net of D > 32 pins on one warp; `stage` holds kStagedPins pin positions.
+template <bool WL, bool EXACT, bool LSE>
+__device__ __forceinline__ NetOut net_in_warp(const int4 t, int lane, const PinCtx &pc,
+                                              float2 *__restrict__ out, float igx, float igy,
+                                              int want_value, float2 *__restrict__ stage) {
+    const int D = t.x, p0 = t.y;
+    float x1 = -3.4e38f, x0 = 3.4e38f, y1 = -3.4e38f, y0 = 3.4e38f;
+#pragma unroll 4
+    for (int k = lane; k < D; k += 32) {
+        const float2 xy = pin_xy(pc, p0 + k);
+        if (k < kStagedPins) stage[k] = xy;  // read back by this lane only
+        x1 = fmaxf(x1, xy.x);
+        x0 = fminf(x0, xy.x);
+        y1 = fmaxf(y1, xy.y);
+        y0 = fminf(y0, xy.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        x1 = fmaxf(x1, __shfl_xor_sync(kFull, x1, o));
+        x0 = fminf(x0, __shfl_xor_sync(kFull, x0, o));
+        y1 = fmaxf(y1, __shfl_xor_sync(kFull, y1, o));
+        y0 = fminf(y0, __shfl_xor_sync(kFull, y0, o));
+    }
+    NetOut r{lane == 0 ? ((double)x1 - (double)x0) + ((double)y1 - (double)y0) : 0.0, 0.0};
+    if (WL) {
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int k = lane; k < D; k += 32) {
+            const float2 xy = k < kStagedPins ? stage[k] : pin_xy(pc, p0 + k);
+            add_terms(s, pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy), xy);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int i = 0; i < 8; i++) s[i] = __fadd_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
+        const NetSums ns = net_sums(s);
+        const NetCoef c = net_coef(ns);
+        for (int k = lane; k < D; k += 32) {
+            const float2 xy = k < kStagedPins ? stage[k] : pin_xy(pc, p0 + k);
+            out[p0 + k] = pin_gradient<LSE>(pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy), xy, igx, igy, c);
+        }
+        if (want_value && lane == 0) r.value = net_value(ns, x1, x0, y1, y0, igx, igy, LSE);
+    }
+    return r;
+}
+
+template <bool WL, bool EXACT, bool LSE>
+__global__ void __launch_bounds__(kNetWarps * 32)
+k_wl(const int4 *__restrict__ tasks, int n_tasks, PinCtx pc, float2 *__restrict__ out,
+     int want_value, double *__restrict__ partials, int mode, DevScalars *__restrict__ S) {
+    pdl_begin();
+    __shared__ double sh[64];
+    __shared__ float2 stage[WL ? kNetWarps : 1][WL ? kStagedPins : 1];
+    if (WL && S->done) return;
+    const float igx = (float)S->inv_gamma_x, igy = (float)S->inv_gamma_y;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int w = blockIdx.x * kNetWarps + wid;
+    NetOut r{0.0, 0.0};
+    if (w < n_tasks) {  // warp-uniform
+        const int4 t = tasks[w];
+        r = t.x <= kWarpPins ? nets_in_warp<WL, EXACT, LSE>(t, lane, pc, out, igx, igy, want_value)
+                             : net_in_warp<WL, EXACT, LSE>(t, lane, pc, out, igx, igy, want_value,
+                                                           stage[WL ? wid : 0]);
+    }
+    // the smooth wirelength value rides along only when asked for
+    bool last;
+    double acc[2] = {r.hpwl, r.value};
+    if (WL && want_value) {
+        last = grid_sum<2>(acc, sh, partials, &S->cnt_wl, gridDim.x, blockIdx.x);
+    } else {
+        double a1[1] = {r.hpwl};
+        last = grid_sum<1>(a1, sh, partials, WL ? &S->cnt_wl : &S->cnt_hp, gridDim.x, blockIdx.x);
+        acc[0] = a1[0];
+        acc[1] = 0.0;
+    }
+    if (last && threadIdx.x == 0) {
         if (WL)
             finish_wirelength(S, acc[0], acc[1]);
         else
@@ -401,29 +474,55 @@ k_wl_big(const int32_t *__restrict__ nets, int n_list, const int32_t *__restrict
 }
 
 // ---------------------------------------------------------------- gather --
-__device__ __forceinline__ float2 gather_bin(const Grid &g, const Rect &r, float sxy, int i, int j,
+// Field gather (EPlace/eplace.cpp:599-674) in FP32: the same smoothed
+// rectangle and bin range as the scatter, the overlap in float, and the
+// static smoothing scale sx*sy of the object.  (The scatter keeps the
+// reference's exact FP64 overlap arithmetic because its maps are compared
+// bit for bit; the gather is compared within tolerance.)
+struct FRect {
+    float l, b, r, t;
+};
+
+__device__ __forceinline__ FRect gather_rect(const Grid &g, float2 p, float2 s, uint8_t f) {
+    const float hw = 0.5f * ((f & kSmoothX) ? g.sx : s.x);
+    const float hh = 0.5f * ((f & kSmoothY) ? g.sy : s.y);
+    return FRect{p.x - hw, p.y - hh, p.x + hw, p.y + hh};
+}
+
+__device__ __forceinline__ void gather_range(const Grid &g, const FRect &r, int &i0, int &i1, int &j0,
+                                             int &j1) {
+    i0 = max(0, (int)((r.l - g.llx) * g.isx));
+    i1 = min(g.nx - 1, (int)((r.r - g.llx) * g.isx));
+    j0 = max(0, (int)((r.b - g.lly) * g.isy));
+    j1 = min(g.ny - 1, (int)((r.t - g.lly) * g.isy));
+}
+
+__device__ __forceinline__ float2 gather_bin(const Grid &g, const FRect &r, float sxy, int i, int j,
                                              const float2 *__restrict__ field) {
-    // overlapArea = (sx*sy) * getOverlapArea (double) stored to float
-    double ovd = rect_bin_overlap(g, r, i, j);
-    float ov = (float)__dmul_rn((double)sxy, ovd);
-    float2 e = field[(size_t)i * g.ny + j];
-    return make_float2(__fmul_rn(ov, e.x), __fmul_rn(ov, e.y));
+    const float bl = fmaf((float)i, g.sx, g.llx), bb = fmaf((float)j, g.sy, g.lly);
+    const float ox = fminf(r.r, bl + g.sx) - fmaxf(r.l, bl);
+    const float oy = fminf(r.t, bb + g.sy) - fmaxf(r.b, bb);
+    if (ox <= 0.0f || oy <= 0.0f) return make_float2(0.f, 0.f);
+    const float ov = sxy * ox * oy;
+    const float2 e = field[(size_t)i * g.ny + j];
+    return make_float2(ov * e.x, ov * e.y);
 }
 
 __global__ void __launch_bounds__(128)
 k_gather_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
+             const uint8_t *__restrict__ flags, const float *__restrict__ sxy_of,
              const int32_t *__restrict__ big, const float2 *__restrict__ field,
              float2 *__restrict__ out, const DevScalars *__restrict__ S) {
+    pdl_begin();
     __shared__ float shx[4], shy[4];
     if (S->done) return;
-    int o = big[blockIdx.x];
-    float2 p = pos[o], s = size[o];
-    Rect r = object_rect(g, p.x, p.y, s.x, s.y);
+    const int o = big[blockIdx.x];
+    const FRect r = gather_rect(g, pos[o], size[o], flags[o]);
+    const float sxy = sxy_of[o];
     int i0, i1, j0, j1;
-    bin_range(g, r, i0, i1, j0, j1);
-    float sxy = __fmul_rn(r.sx, r.sy);
-    int wy = j1 - j0 + 1;
-    int nb = (i1 >= i0 && j1 >= j0) ? (i1 - i0 + 1) * wy : 0;
+    gather_range(g, r, i0, i1, j0, j1);
+    const int wy = j1 - j0 + 1;
+    const int nb = (i1 >= i0 && j1 >= j0) ? (i1 - i0 + 1) * wy : 0;
     float gx = 0.f, gy = 0.f;
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
         float2 v = gather_bin(g, r, sxy, i0 + t / wy, j0 + t % wy, field);
@@ -456,6 +555,7 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
           const float2 *__restrict__ y_prev, float2 *__restrict__ dump_gd,
           float2 *__restrict__ dump_gwl, int stepping, double *__restrict__ partials,
           DevScalars *__restrict__ S) {
+    pdl_begin();
     __shared__ double sh[32 * 5];
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -471,23 +571,22 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
             gdx = v.x;
             gdy = v.y;
         } else {
-            float2 s = d.size[o];
-            Rect r = object_rect(g, p.x, p.y, s.x, s.y);
+            const FRect r = gather_rect(g, p, d.size[o], f);
+            const float sxy = d.sxy[o];
             int i0, i1, j0, j1;
-            bin_range(g, r, i0, i1, j0, j1);
-            float sxy = __fmul_rn(r.sx, r.sy);
+            gather_range(g, r, i0, i1, j0, j1);
             for (int i = i0; i <= i1; i++)
                 for (int j = j0; j <= j1; j++) {
                     float2 v = gather_bin(g, r, sxy, i, j, field);
-                    gdx = __fadd_rn(gdx, v.x);
-                    gdy = __fadd_rn(gdy, v.y);
+                    gdx += v.x;
+                    gdy += v.y;
                 }
         }
         // wirelength gradient: the module's pins in pin order (eplace.cpp:539-547)
         float wx = 0.f, wy = 0.f;
         if (!(f & kFiller)) {
             for (int k = d.obj_pin_start[o]; k < d.obj_pin_start[o + 1]; k++) {
-                float2 v = pin_grad[d.obj_pins[k]];
+                float2 v = pin_grad[d.obj_pin_dev[k]];
                 wx = __fadd_rn(wx, v.x);
                 wy = __fadd_rn(wy, v.y);
             }
@@ -587,6 +686,7 @@ __global__ void __launch_bounds__(kThreads)
 k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
          float2 *__restrict__ pos, float2 *__restrict__ x, const float2 *__restrict__ gin,
          float2 *__restrict__ y_prev, float2 *__restrict__ g_prev, DevScalars *__restrict__ S) {
+    pdl_begin();
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o < n && (flags[o] & kInView)) {
@@ -614,6 +714,7 @@ k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restr
 __global__ void k_stage_begin(int n, const uint8_t *__restrict__ flags,
                               const float2 *__restrict__ pos, float2 *__restrict__ x,
                               DevScalars *__restrict__ S) {
+    pdl_begin();
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x)
         if (flags[o] & kInView) x[o] = pos[o];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -639,6 +740,7 @@ __global__ void k_stage_begin(int n, const uint8_t *__restrict__ flags,
 __global__ void k_wrap_up(Grid g, int n, const uint8_t *__restrict__ flags,
                           const float2 *__restrict__ size, float2 *__restrict__ pos,
                           const float2 *__restrict__ x) {
+    pdl_begin();
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o < n && (flags[o] & kInView)) pos[o] = clamp_center(g, x[o], size[o]);
 }
@@ -650,18 +752,18 @@ int prep_blocks(const Grid &g) { return std::min(blocks_for(g.nx * g.ny, kThread
 
 int reduction_blocks(const DeviceNetlist &d, int which) {
     switch (which) {
-        case 0: return blocks_for(d.n_small_nets, kThreads) + blocks_for(d.n_big_nets * 32, kThreads);
+        case 0: return blocks_for(d.n_net_tasks, kNetWarps);
         default: return blocks_for(d.n_obj, kThreads);
     }
 }
 
 void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, unsigned long long *node_q,
                     unsigned long long *filler_q, const DevScalars *S, cudaStream_t st) {
-    k_scatter_small<<<blocks_for(d.n_obj, kThreads), kThreads, 0, st>>>(
-        c.grid, d.pos, d.size, d.flags, d.n_obj, c.qscale, node_q, filler_q, S);
+    launch_k(k_scatter_small, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.pos, d.size,
+             d.flags, d.n_obj, c.qscale, node_q, filler_q, S);
     if (d.n_big_objs > 0)
-        k_scatter_big<<<d.n_big_objs, 128, 0, st>>>(c.grid, d.pos, d.size, d.flags, d.big_objs,
-                                                    c.qscale, node_q, filler_q, S);
+        launch_k(k_scatter_big, d.n_big_objs, 128, 0, st, c.grid, d.pos, d.size, d.flags, d.big_objs,
+                 c.qscale, node_q, filler_q, S);
 }
 
 void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long long *filler_q,
@@ -671,71 +773,66 @@ void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long l
     int blocks = prep_blocks(c.grid);
     uint16_t *hi = (uint16_t *)rho_bf16;
     uint16_t *lo = hi ? hi + nb : nullptr;
-    k_prep<<<blocks, kThreads, 0, st>>>(c.grid, node_q, filler_q, static_map, rho, hi, lo, node_f,
-                                        filler_f, zero_maps, c.inv_qscale, c.inv_bin_area,
-                                        c.bin_area, c.area_norm, c.part_prep, S);
+    launch_k(k_prep, blocks, kThreads, 0, st, c.grid, node_q, filler_q, static_map, rho, hi, lo, node_f,
+             filler_f, zero_maps, c.inv_qscale, c.inv_bin_area, c.bin_area, c.area_norm, c.part_prep, S);
 }
 
-template <bool WL>
+template <bool WL, bool EXACT, bool LSE>
 void launch_nets(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad, double *partials,
                  int mode, DevScalars *S, cudaStream_t st) {
     PinCtx pc{d.pin_owner, d.pin_off, d.pos};
-    int bs = blocks_for(d.n_small_nets, kThreads);
-    int bb = blocks_for(d.n_big_nets * 32, kThreads);
-    unsigned total = (unsigned)(bs + bb);
-    if (total == 0) return;
-    if (bb > 0)
-        k_wl_big<WL><<<bb, kThreads, 0, st>>>(d.big_nets, d.n_big_nets, d.net_start, pc, pin_grad,
-                                              c.exact_exp, c.lse, total, 0u, partials, mode, S);
-    if (bs > 0)
-        k_wl_small<WL><<<bs, kThreads, 0, st>>>(d.small_nets, d.n_small_nets, d.net_start, pc,
-                                                pin_grad, c.exact_exp, c.lse, total, (unsigned)bb,
-                                                partials, mode, S);
+    if (d.n_net_tasks == 0) return;
+    launch_k(k_wl<WL, EXACT, LSE>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, d.net_tasks,
+             d.n_net_tasks, pc, pin_grad, c.want_wl_value, partials, mode, S);
 }
 
 void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad,
                        DevScalars *S, cudaStream_t st) {
-    launch_nets<true>(c, d, pin_grad, c.part_wl, 0, S, st);
+    if (c.exact_exp)
+        c.lse ? launch_nets<true, true, true>(c, d, pin_grad, c.part_wl, 0, S, st)
+              : launch_nets<true, true, false>(c, d, pin_grad, c.part_wl, 0, S, st);
+    else
+        c.lse ? launch_nets<true, false, true>(c, d, pin_grad, c.part_wl, 0, S, st)
+              : launch_nets<true, false, false>(c, d, pin_grad, c.part_wl, 0, S, st);
 }
 
 void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
                        float2 *gd_big, const DevScalars *S, cudaStream_t st) {
     if (d.n_big_objs > 0)
-        k_gather_big<<<d.n_big_objs, 128, 0, st>>>(c.grid, d.pos, d.size, d.big_objs, field,
-                                                   gd_big, S);
+        launch_k(k_gather_big, d.n_big_objs, 128, 0, st, c.grid, d.pos, d.size, d.flags, d.sxy,
+                 d.big_objs, field, gd_big, S);
 }
 
 void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
                     const float2 *gd_big, const float2 *pin_grad, float2 *g, const float2 *g_prev,
                     const float2 *y_prev, float2 *dump_gd, float2 *dump_gwl, int stepping,
                     DevScalars *S, cudaStream_t st) {
-    k_combine<<<blocks_for(d.n_obj, kThreads), kThreads, 0, st>>>(
-        c.grid, d, field, gd_big, pin_grad, g, g_prev, y_prev, dump_gd, dump_gwl, stepping,
-        c.part_comb, S);
+    launch_k(k_combine, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d, field, gd_big,
+             pin_grad, g, g_prev, y_prev, dump_gd, dump_gwl, stepping, c.part_comb, S);
 }
 
 void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
                    const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S,
                    cudaStream_t st) {
-    k_update<<<blocks_for(d.n_obj, kThreads), kThreads, 0, st>>>(c.grid, d.n_obj, d.flags, d.size,
-                                                                  pos, x, g, y_prev, g_prev, S);
+    launch_k(k_update, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+             pos, x, g, y_prev, g_prev, S);
 }
 
 void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
                         cudaStream_t st) {
-    k_stage_begin<<<std::min(blocks_for(d.n_obj, kThreads), 148 * 4), kThreads, 0, st>>>(
-        d.n_obj, d.flags, pos, x, S);
+    launch_k(k_stage_begin, std::min(blocks_for(d.n_obj, kThreads), 148 * 4), kThreads, 0, st, d.n_obj,
+             d.flags, pos, x, S);
 }
 
 void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, const float2 *x,
                     cudaStream_t st) {
-    k_wrap_up<<<blocks_for(d.n_obj, kThreads), kThreads, 0, st>>>(c.grid, d.n_obj, d.flags, d.size,
-                                                                   pos, x);
+    launch_k(k_wrap_up, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+             pos, x);
 }
 
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
                  cudaStream_t st) {
-    launch_nets<false>(c, d, nullptr, c.part_hp, mode, S, st);
+    launch_nets<false, false, false>(c, d, nullptr, c.part_hp, mode, S, st);
 }
 
 }  // namespace ep

@@ -99,7 +99,8 @@ typedef struct ep_scalars {
     double hpwl;           /* HPWL of the last evaluation (bound-pin HPWL) */
     double last_hpwl;      /* lastHPWL of updatePenaltyFactor */
     double inv_gamma_x, inv_gamma_y;
-    double wirelength;     /* smooth (WA/LSE) wirelength of the last evaluation */
+    double wirelength;     /* smooth (WA/LSE) wirelength of the last evaluation;
+                              summed only when ep_params.keep_maps is set, else 0 */
     double step;           /* last step size */
     double ns_param;       /* Nesterov a_k */
     int32_t iteration;     /* iter_count of the current stage */
@@ -215,10 +216,11 @@ ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped);
 ep_status ep_nesterov_end(ep_engine *e);
 
 /* Measurement hook with no reference counterpart: launches each kernel group
- * of one evaluation + step separately, reps times, timing every launch with
- * CUDA events on the engine's stream, and reports the average device time
- * with the group's algorithmic bytes / flops.  Positions, optimizer vectors
- * and scalars are restored afterwards. */
+ * of one evaluation + step separately, reps times back to back between two
+ * CUDA events on the engine's stream (less the time of any per-repetition
+ * setup, such as clearing the density maps before a scatter), and reports the
+ * average device time per launch with the group's algorithmic bytes / flops.
+ * Positions, optimizer vectors and scalars are restored afterwards. */
 ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out);
 
 /* Bin grid of ep_density_scatter_noalloc. */
