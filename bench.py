@@ -102,7 +102,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -190,7 +190,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--dct", default="auto", choices=["auto", "fp32", "bf16x3"])
@@ -233,13 +233,15 @@ def main():
         eng.initialize()
         return eng.nesterov_run()
 
+    # the clock sampler starts before the warm-up, so it is already reading
+    # when the timed region begins (nvidia-smi takes a moment to start)
+    sampler = ClockSampler(local)
+    sampler.start()
     for _ in range(args.warmup):
         solve()
-    sampler = ClockSampler(local)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler.start()
     times, runs = [], []
     for _ in range(args.steps):
         flush.zero_()

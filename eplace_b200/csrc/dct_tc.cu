@@ -18,6 +18,7 @@
 // Every wait on an mbarrier is bounded; a wait that gives up raises the
 // EP_ERR_TIMEOUT bit in DevScalars::status, the CTA drains what it issued,
 // frees its TMEM and returns.  No TMA multicast is used.
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -35,11 +36,13 @@ namespace {
 constexpr int kBM = 128;            // UMMA M (TMEM lanes)
 constexpr int kBN = 64;             // UMMA N (TMEM columns)
 constexpr int kBK = 64;             // bf16 elements per 128-byte swizzle row
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kATile = kBM * kBK * 2;   // 16 KiB
 constexpr int kBTile = kBN * kBK * 2;   // 8 KiB
 constexpr int kStageBytes = 2 * kATile + 2 * kBTile;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*alignment*/;
+// split-K reduction slots, [split][kBM][kBN / split + 4] floats (largest at split 4)
+constexpr int kRedBytes = 4 * kBM * (kBN / 4 + 4) * 4;
+constexpr int kSmemBytes = kStages * kStageBytes + kRedBytes + 1024 /*barriers*/ + 1024 /*alignment*/;
 constexpr int kThreads = 128;
 constexpr unsigned kWaitLimit = 1u << 22;  // try_wait rounds before giving up
 
@@ -48,6 +51,7 @@ enum TcEpi { kTcTransposed = 0, kTcSpectral = 1, kTcField = 2 };
 struct TcGemmParams {
     CUtensorMap a_hi[3], a_lo[3], b_hi[3], b_lo[3];
     int M, N, K;
+    int split;                  // CTAs per cluster sharing one tile (split-K), 1 = none
     int epi;
     uint16_t *out_hi, *out_lo;  // bf16 planes (kTcTransposed / kTcSpectral)
     int ldo;
@@ -151,13 +155,33 @@ __device__ __forceinline__ void bf16_split(float v, uint16_t &hi, uint16_t &lo) 
     lo = (uint16_t)((u2 + 0x7fffu + ((u2 >> 16) & 1u)) >> 16);
 }
 
+// Output store of one accumulator value: C[m][n] -> out[n * ldo + m].
+__device__ __forceinline__ void store_out(const TcGemmParams &p, int bz, int n, int m, float v) {
+    const size_t o = (size_t)n * p.ldo + m;
+    if (p.epi == kTcField) {
+        if (bz == 0)
+            p.field[o].x = v;
+        else if (bz == 1)
+            p.field[o].y = v;
+        else
+            p.phi[o] = v;
+    } else {
+        uint16_t hi, lo;
+        bf16_split(v, hi, lo);
+        p.out_hi[o] = hi;
+        p.out_lo[o] = lo;
+    }
+}
+
+template <int SPLIT>
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     pdl_begin();
-    if (S && S->done) return;
+    if (S && S->done) return;  // uniform over the grid: no cluster member is left waiting
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = (uint64_t *)(smem + kStages * kStageBytes);
+    float *red = (float *)(smem + kStages * kStageBytes);  // split-K reduction slots
+    uint64_t *full = (uint64_t *)(smem + kStages * kStageBytes + kRedBytes);
     uint64_t *empty = full + kStages;
     uint64_t *done = empty + kStages;
     volatile uint32_t *tmem_slot = (volatile uint32_t *)(done + 1);
@@ -165,8 +189,12 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bz = blockIdx.z;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    const int nk = p.K / kBK;
+    // split-K: the `split` CTAs of a cluster (consecutive in x) share one
+    // output tile and take consecutive K ranges
+    constexpr int split = SPLIT;
+    const int part = blockIdx.x % split;
+    const int m0 = blockIdx.y * kBM, n0 = (blockIdx.x / split) * kBN;
+    const int nk = p.K / kBK / split, kb0 = part * nk;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) {
@@ -195,11 +223,12 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
             int s = kb % kStages, use = kb / kStages;
             if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, abort)) break;
             uint8_t *st = smem + s * kStageBytes;
+            const int kc = (kb0 + kb) * kBK;
             mbar_expect_tx(&full[s], kStageBytes);
-            tma_load_2d(st, &p.a_hi[bz], &full[s], kb * kBK, m0);
-            tma_load_2d(st + kATile, &p.a_lo[bz], &full[s], kb * kBK, m0);
-            tma_load_2d(st + 2 * kATile, &p.b_hi[bz], &full[s], kb * kBK, n0);
-            tma_load_2d(st + 2 * kATile + kBTile, &p.b_lo[bz], &full[s], kb * kBK, n0);
+            tma_load_2d(st, &p.a_hi[bz], &full[s], kc, m0);
+            tma_load_2d(st + kATile, &p.a_lo[bz], &full[s], kc, m0);
+            tma_load_2d(st + 2 * kATile, &p.b_hi[bz], &full[s], kc, n0);
+            tma_load_2d(st + 2 * kATile + kBTile, &p.b_lo[bz], &full[s], kc, n0);
             issued = kb + 1;
         }
         if (*abort) {
@@ -243,37 +272,80 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     if (lane == 0) ready = mbar_wait(done, 0, abort) && !*abort;
     ready = __shfl_sync(0xffffffffu, ready, 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ready) {
-        const int m = m0 + warp * 32 + lane;
+    const int row = warp * 32 + lane, m = m0 + row;
+    const uint32_t tm_row = tmem + ((uint32_t)(warp * 32) << 16);
+    if constexpr (SPLIT == 1) {
+        if (ready) {
 #pragma unroll 1
-        for (int c0 = 0; c0 < kBN; c0 += 16) {
-            // spectral scale of these 16 columns, loaded before the stores
-            // so the loads do not queue behind them
-            float ks[16];
-            if (p.epi == kTcSpectral) {
+            for (int c0 = 0; c0 < kBN; c0 += 16) {
+                // spectral scale of these 16 columns, loaded before the
+                // stores so the loads do not queue behind them
+                float ks[16];
+                if (p.epi == kTcSpectral) {
 #pragma unroll
-                for (int c = 0; c < 16; c++) ks[c] = __ldg(&p.kscale[(size_t)(n0 + c0 + c) * p.ldo + m]);
-            }
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-#pragma unroll
-            for (int c = 0; c < 16; c++) {
-                const size_t o = (size_t)(n0 + c0 + c) * p.ldo + m;
-                float v = __uint_as_float(r[c]);
-                if (p.epi == kTcField) {
-                    if (bz == 0)
-                        p.field[o].x = v;
-                    else if (bz == 1)
-                        p.field[o].y = v;
-                    else
-                        p.phi[o] = v;
-                } else {
-                    if (p.epi == kTcSpectral) v *= ks[c];
-                    uint16_t hi, lo;
-                    bf16_split(v, hi, lo);
-                    p.out_hi[o] = hi;
-                    p.out_lo[o] = lo;
+                    for (int c = 0; c < 16; c++) ks[c] = __ldg(&p.kscale[(size_t)(n0 + c0 + c) * p.ldo + m]);
                 }
+                uint32_t r[16];
+                tmem_ld16(tm_row + (uint32_t)c0, r);
+#pragma unroll
+                for (int c = 0; c < 16; c++) {
+                    float v = __uint_as_float(r[c]);
+                    if (p.epi == kTcSpectral) v *= ks[c];
+                    store_out(p, bz, n0 + c0 + c, m, v);
+                }
+            }
+        }
+    } else {
+        // Split-K reduction.  CTA q of the cluster owns columns
+        // [q * kCols, (q + 1) * kCols) of the tile.  Every CTA pushes each
+        // 16-column chunk of its FP32 partial straight into the owner's slot
+        // for this CTA (remote stores through distributed shared memory, no
+        // round trip), one cluster barrier makes them visible, and each CTA
+        // then sums its SPLIT slots in rank order (deterministic) from its own
+        // shared memory and stores the result.  The slots have their own
+        // region, so a peer that finishes early never writes into a stage
+        // ring that is still being filled.  The barrier is reached on every
+        // path.
+        namespace cg = cooperative_groups;
+        cg::cluster_group cl = cg::this_cluster();
+        constexpr int kCols = kBN / (SPLIT > 1 ? SPLIT : 1), kRedLd = kCols + 4;
+        if (ready) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < kBN; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tm_row + (uint32_t)c0, r);
+                const int q = c0 / kCols;  // owner of these 16 columns
+                float *dst = cl.map_shared_rank(red, q) + (part * kBM + row) * kRedLd + (c0 - q * kCols);
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    *(float4 *)(dst + 4 * i) =
+                        make_float4(__uint_as_float(r[4 * i]), __uint_as_float(r[4 * i + 1]),
+                                    __uint_as_float(r[4 * i + 2]), __uint_as_float(r[4 * i + 3]));
+            }
+        }
+        cl.sync();
+        const int cbeg = part * kCols;
+        float ks[kCols];
+        if (p.epi == kTcSpectral) {
+#pragma unroll
+            for (int j = 0; j < kCols; j++) ks[j] = __ldg(&p.kscale[(size_t)(n0 + cbeg + j) * p.ldo + m]);
+        }
+#pragma unroll
+        for (int q4 = 0; q4 < kCols / 4; q4++) {
+            float4 v = *(const float4 *)&red[row * kRedLd + 4 * q4];
+#pragma unroll
+            for (int r = 1; r < SPLIT; r++) {
+                const float4 w = *(const float4 *)&red[(r * kBM + row) * kRedLd + 4 * q4];
+                v.x += w.x;
+                v.y += w.y;
+                v.z += w.z;
+                v.w += w.w;
+            }
+            const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int j = 4 * q4 + i;
+                if (ready) store_out(p, bz, n0 + cbeg + j, m, p.epi == kTcSpectral ? vv[i] * ks[j] : vv[i]);
             }
         }
     }
@@ -292,7 +364,40 @@ struct TcPlan {
     uint16_t *rho = nullptr, *Cy = nullptr, *Cx = nullptr, *Tt = nullptr, *P = nullptr;
     uint16_t *B3 = nullptr, *A4 = nullptr, *T3 = nullptr;
     TcGemmParams g[4];
+    int sms = 148;       // SMs of the device
+    int max_split = 1;   // largest cluster the GEMM can be launched with
 };
+
+// Split-K factor: double it while the grid still fits in one wave and every
+// CTA keeps at least one K block.
+int pick_split(const TcPlan &t, const TcGemmParams &g, int batch) {
+    const int tiles = (g.M / kBM) * (g.N / kBN) * batch, nk = g.K / kBK;
+    int s = 1;
+    while (s * 2 <= t.max_split && tiles * s * 2 <= t.sms && nk % (s * 2) == 0) s *= 2;
+    return s;
+}
+
+void launch_tc(const TcGemmParams &g, dim3 grid, DevScalars *S, cudaStream_t st) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = kSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = (unsigned)g.split;
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    switch (g.split) {
+        case 4: cudaLaunchKernelEx(&cfg, k_umma_nt<4>, g, S); break;
+        case 2: cudaLaunchKernelEx(&cfg, k_umma_nt<2>, g, S); break;
+        default: cudaLaunchKernelEx(&cfg, k_umma_nt<1>, g, S); break;
+    }
+}
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
@@ -418,10 +523,37 @@ int dct_tc_init(DctPlan &p, std::string &err) {
         ok = make_map(&g4.a_hi[b], As[b], ny, nx, kBM, err) && make_map(&g4.a_lo[b], As[b] + t3, ny, nx, kBM, err) &&
              make_map(&g4.b_hi[b], Bs[b], nx, nx, kBN, err) && make_map(&g4.b_lo[b], Bs[b] + a4, nx, nx, kBN, err);
     if (!ok) return EP_ERR_UNSUPPORTED;
-    if (cudaFuncSetAttribute(k_umma_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_umma_nt<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess ||
+        cudaFuncSetAttribute(k_umma_nt<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess ||
+        cudaFuncSetAttribute(k_umma_nt<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) != cudaSuccess) {
         err = "cannot raise the dynamic shared memory limit of the tcgen05 GEMM";
         return EP_ERR_CUDA;
     }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, dev);
+    // largest cluster (<= 4) of which at least one fits on the device
+    for (int c = 4; c >= 2; c /= 2) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = kSmemBytes;
+        cudaLaunchAttribute a[1];
+        a[0].id = cudaLaunchAttributeClusterDimension;
+        a[0].val.clusterDim.x = (unsigned)c;
+        a[0].val.clusterDim.y = 1;
+        a[0].val.clusterDim.z = 1;
+        cfg.attrs = a;
+        cfg.numAttrs = 1;
+        int n = 0;
+        cudaError_t q = c == 4 ? cudaOccupancyMaxActiveClusters(&n, k_umma_nt<4>, &cfg)
+                               : cudaOccupancyMaxActiveClusters(&n, k_umma_nt<2>, &cfg);
+        if (q == cudaSuccess && n > 0) {
+            t->max_split = c;
+            break;
+        }
+    }
+    cudaGetLastError();  // clear a refused query
     return EP_OK;
 }
 
@@ -447,8 +579,9 @@ int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaS
             g.phi = phi;
             batch = phi ? 3 : 2;
         }
-        dim3 grid(g.N / kBN, g.M / kBM, batch);
-        launch_k(k_umma_nt, grid, kThreads, kSmemBytes, st, g, s);
+        g.split = pick_split(*t, g, batch);
+        dim3 grid(g.N / kBN * g.split, g.M / kBM, batch);
+        launch_tc(g, grid, s, st);
     }
     return EP_OK;
 }
