@@ -52,6 +52,7 @@ struct TcGemmParams {
     CUtensorMap a_hi[3], a_lo[3], b_hi[3], b_lo[3];
     int M, N, K;
     int split;                  // CTAs per cluster sharing one tile (split-K), 1 = none
+    int b_const;                // B does not depend on the previous grid (loaded before its end)
     int epi;
     uint16_t *out_hi, *out_lo;  // bf16 planes (kTcTransposed / kTcSpectral)
     int ldo;
@@ -177,8 +178,14 @@ template <int SPLIT>
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    pdl_begin();
-    if (S && S->done) return;  // uniform over the grid: no cluster member is left waiting
+    // S->done is final before this grid starts: only the update kernel writes
+    // it, and that grid completed before the previous grid passed its own
+    // wait.  The check is uniform over the grid, so no cluster member is left
+    // waiting; the early exit still waits for the previous grid first.
+    if (S && S->done) {
+        pdl_begin();
+        return;
+    }
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     float *red = (float *)(smem + kStages * kStageBytes);  // split-K reduction slots
     uint64_t *full = (uint64_t *)(smem + kStages * kStageBytes + kRedBytes);
@@ -216,10 +223,33 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
+    // Everything above and the B tiles of the first ring stages (B is a
+    // constant DCT table in all four GEMMs) overlap the previous grid; the A
+    // tiles are its output, so they are loaded after the wait.
+    const int pre = p.b_const ? (nk < kStages ? nk : kStages) : 0;
+    if (threadIdx.x == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.a_hi[bz]) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&p.a_lo[bz]) : "memory");
+        for (int kb = 0; kb < pre; kb++) {
+            uint8_t *st = smem + kb * kStageBytes;
+            const int kc = (kb0 + kb) * kBK;
+            mbar_expect_tx(&full[kb], kStageBytes);
+            tma_load_2d(st + 2 * kATile, &p.b_hi[bz], &full[kb], kc, n0);
+            tma_load_2d(st + 2 * kATile + kBTile, &p.b_lo[bz], &full[kb], kc, n0);
+        }
+    }
+    pdl_begin();
+
     if (threadIdx.x == 0) {
         // ---- TMA producer ----
-        int issued = 0;
-        for (int kb = 0; kb < nk; kb++) {
+        for (int kb = 0; kb < pre; kb++) {
+            uint8_t *st = smem + kb * kStageBytes;
+            const int kc = (kb0 + kb) * kBK;
+            tma_load_2d(st, &p.a_hi[bz], &full[kb], kc, m0);
+            tma_load_2d(st + kATile, &p.a_lo[bz], &full[kb], kc, m0);
+        }
+        int issued = pre;
+        for (int kb = pre; kb < nk; kb++) {
             int s = kb % kStages, use = kb / kStages;
             if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, abort)) break;
             uint8_t *st = smem + s * kStageBytes;
@@ -489,7 +519,7 @@ int dct_tc_init(DctPlan &p, std::string &err) {
     // G1: Tt[v][x] = sum_y rho[x][y] Cy[v][y]
     TcGemmParams &g1 = t->g[0];
     std::memset(&g1, 0, sizeof(g1));
-    g1.M = nx; g1.N = ny; g1.K = ny; g1.epi = kTcTransposed;
+    g1.M = nx; g1.N = ny; g1.K = ny; g1.epi = kTcTransposed; g1.b_const = 1;
     g1.out_hi = t->Tt; g1.out_lo = lo(t->Tt, nb); g1.ldo = nx;
     bool ok = make_map(&g1.a_hi[0], t->rho, nx, ny, kBM, err) && make_map(&g1.a_lo[0], lo(t->rho, nb), nx, ny, kBM, err) &&
               make_map(&g1.b_hi[0], t->Cy, ny, ny, kBN, err) && make_map(&g1.b_lo[0], lo(t->Cy, (size_t)ny * ny), ny, ny, kBN, err);
@@ -497,14 +527,14 @@ int dct_tc_init(DctPlan &p, std::string &err) {
     // B = Cx) so the transposed store writes P[u][v]; K has P's layout
     TcGemmParams &g2 = t->g[1];
     std::memset(&g2, 0, sizeof(g2));
-    g2.M = ny; g2.N = nx; g2.K = nx; g2.epi = kTcSpectral;
+    g2.M = ny; g2.N = nx; g2.K = nx; g2.epi = kTcSpectral; g2.b_const = 1;
     g2.out_hi = t->P; g2.out_lo = lo(t->P, nb); g2.ldo = ny; g2.kscale = p.K;
     ok = ok && make_map(&g2.a_hi[0], t->Tt, ny, nx, kBM, err) && make_map(&g2.a_lo[0], lo(t->Tt, nb), ny, nx, kBM, err) &&
          make_map(&g2.b_hi[0], t->Cx, nx, nx, kBN, err) && make_map(&g2.b_lo[0], lo(t->Cx, (size_t)nx * nx), nx, nx, kBN, err);
     // G3: T3[n][u] = sum_v P[u][v] B3[n][v]
     TcGemmParams &g3 = t->g[2];
     std::memset(&g3, 0, sizeof(g3));
-    g3.M = nx; g3.N = 2 * ny; g3.K = ny; g3.epi = kTcTransposed;
+    g3.M = nx; g3.N = 2 * ny; g3.K = ny; g3.epi = kTcTransposed; g3.b_const = 1;
     g3.out_hi = t->T3; g3.out_lo = lo(t->T3, 2 * nb); g3.ldo = nx;
     ok = ok && make_map(&g3.a_hi[0], t->P, nx, ny, kBM, err) && make_map(&g3.a_lo[0], lo(t->P, nb), nx, ny, kBM, err) &&
          make_map(&g3.b_hi[0], t->B3, 2 * ny, ny, kBN, err) && make_map(&g3.b_lo[0], lo(t->B3, (size_t)2 * ny * ny), 2 * ny, ny, kBN, err);
@@ -513,7 +543,7 @@ int dct_tc_init(DctPlan &p, std::string &err) {
     // batch 2 = phi (Ut with A4y)
     TcGemmParams &g4 = t->g[3];
     std::memset(&g4, 0, sizeof(g4));
-    g4.M = ny; g4.N = nx; g4.K = nx; g4.epi = kTcField; g4.ldo = ny;
+    g4.M = ny; g4.N = nx; g4.K = nx; g4.epi = kTcField; g4.ldo = ny; g4.b_const = 1;
     const size_t a4 = (size_t)2 * nx * nx;  // lo plane offset of A4
     const size_t t3 = (size_t)2 * nb;       // lo plane offset of T3
     uint16_t *A4x = t->A4, *A4y = t->A4 + (size_t)nx * nx;
