@@ -209,11 +209,10 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sh) {
 
 // "Last block done": returns true in thread 0 of the block that finishes
 // last among `total` blocks (counted on *cnt, which it resets).
+__device__ __forceinline__ unsigned int arrive_acq_rel(unsigned int *cnt);
+
 __device__ __forceinline__ bool last_block(unsigned int *cnt, unsigned int total) {
-    __threadfence();
-    unsigned int prev = atomicAdd(cnt, 1u);
-    if (prev == total - 1) {
-        __threadfence();
+    if (arrive_acq_rel(cnt) == total - 1) {
         *cnt = 0;
         return true;
     }
@@ -226,6 +225,15 @@ __device__ __forceinline__ bool last_block(unsigned int *cnt, unsigned int total
 // result does not depend on block scheduling.  Must be called by all threads
 // of every participating block.  Returns true in all threads of the last
 // block; its thread 0 then holds the totals in v.
+// Arrival count with acquire-release semantics at GPU scope: the partials this
+// thread stored before are visible to whoever observes the increment, and the
+// partials of every block counted before are visible to this thread after.
+__device__ __forceinline__ unsigned int arrive_acq_rel(unsigned int *cnt) {
+    unsigned int prev;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(cnt) : "memory");
+    return prev;
+}
+
 template <int NV>
 __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *sh, double *partials,
                                          unsigned int *cnt, unsigned int total,
@@ -235,13 +243,13 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *sh, double *pa
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < NV; k++) partials[(size_t)k * total + block_id] = v[k];
-        __threadfence();
-        unsigned int prev = atomicAdd(cnt, 1u);
+        const unsigned int prev = arrive_acq_rel(cnt);
         is_last = (prev == total - 1);
     }
     __syncthreads();
     if (!is_last) return false;
-    __threadfence();
+    // thread 0's acquire covers the block through the barrier above
+    __threadfence_block();
     double s[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) {

@@ -30,6 +30,7 @@ namespace ep {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kPinChunk = 128;  // pin gradients a warp of the combine kernel stages per round
 
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 
@@ -562,6 +563,43 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
     float lam = S->lambda0_mode ? 0.0f : (float)S->lambda;
     int iter = S->iter;
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // dg2, dy2, s.y, |gwl|, |gd|
+
+    // Wirelength gradient of the object: its pins' gradients added in pin
+    // order (EPlace/eplace.cpp:539-547).  The objects of a warp own one
+    // contiguous run of pin slots, so the warp stages that run's gradients
+    // in shared memory with all its loads in flight at once (kPinChunk per
+    // round), then every lane adds its own pins from there in order.
+    // Fillers own no pins.
+    __shared__ float2 pin_sm[kThreads / 32][kPinChunk];
+    float wx = 0.f, wy = 0.f;
+    {
+        const int lane = threadIdx.x & 31;
+        float2 *sm = pin_sm[threadIdx.x >> 5];
+        const bool valid = o < d.n_obj;
+        const int ps = valid ? d.obj_pin_start[o] : 0, pe = valid ? d.obj_pin_start[o + 1] : 0;
+        const int wbeg = __shfl_sync(0xffffffffu, ps, 0);
+        const int wend = __reduce_max_sync(0xffffffffu, (unsigned)pe);
+        for (int base = wbeg; base < wend; base += kPinChunk) {  // warp-uniform
+            const int n = min(kPinChunk, wend - base);
+            int idx[kPinChunk / 32];
+#pragma unroll
+            for (int u = 0; u < kPinChunk / 32; u++) {
+                const int t = lane + 32 * u;
+                idx[u] = t < n ? d.obj_pin_dev[base + t] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < kPinChunk / 32; u++)
+                if (idx[u] >= 0) sm[lane + 32 * u] = pin_grad[idx[u]];
+            __syncwarp();
+            const int k1 = min(pe, base + n);
+            for (int k = max(ps, base); k < k1; k++) {
+                const float2 v = sm[k - base];
+                wx = __fadd_rn(wx, v.x);
+                wy = __fadd_rn(wy, v.y);
+            }
+            __syncwarp();
+        }
+    }
     if (o < d.n_obj) {
         uint8_t f = d.flags[o];
         float2 p = d.pos[o];
@@ -581,15 +619,6 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
                     gdx += v.x;
                     gdy += v.y;
                 }
-        }
-        // wirelength gradient: the module's pins in pin order (eplace.cpp:539-547)
-        float wx = 0.f, wy = 0.f;
-        if (!(f & kFiller)) {
-            for (int k = d.obj_pin_start[o]; k < d.obj_pin_start[o + 1]; k++) {
-                float2 v = pin_grad[d.obj_pin_dev[k]];
-                wx = __fadd_rn(wx, v.x);
-                wy = __fadd_rn(wy, v.y);
-            }
         }
         // preconditioner 1/max(1, #pins + lambda*area) and direction
         float den = fmaxf(1.0f, __fadd_rn(d.npins[o], __fmul_rn(lam, d.area[o])));
