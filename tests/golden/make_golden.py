@@ -10,9 +10,11 @@ computes on the same netlist and starting positions:
     wirelength / total gradients, tau, 1/gamma, HPWL and lambda_0;
   * a second totalGradientUpdate with lambda_0 (the preconditioned direction);
   * the first optimizer steps (positions, tau, lambda after each);
-  * the whole mGP run (iterations, final tau, HPWL).
+  * the whole mGP run (iterations, final tau, HPWL);
+  * variants.npz: the LSE and BB options and the mixed-size stage sequence
+    (record_variants).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--variants-only] [--bench]
 """
 import os
 import sys
@@ -118,6 +120,64 @@ def check_reader():
     assert np.array_equal(a.gradients()[2], b.gradients()[2])
 
 
+def run_stage(ref):
+    """One EplaceNesterovOpt::opt of the current stage; returns its summary."""
+    ref.opt_run()
+    i = ref.info()
+    x, y = ref.positions()
+    return dict(iterations=np.int64(i["iter_count"]), overflow=np.float64(i["overflow"]),
+                hpwl=np.float64(ref.hpwl()), lam=np.float64(i["lambda"]), cx=x, cy=y)
+
+
+def record_variants():
+    """Reference runs under the non-default options and the later stages:
+      * gArg "LSE": the wirelength gradient at the initial positions and the
+        whole mGP run with the log-sum-exp model (EPlace/eplace.cpp:512-549);
+      * gArg "bb": the whole mGP run with the Barzilai-Borwein step
+        (Optimization/nesterov.hpp:231-302);
+      * mixed-size stages: mGP, switch2FillerOnly (the reference re-draws the
+        fillers with rand(); their new centres are recorded), 20 FILLERONLY
+        steps, switch2cGP and the cGP run (EPlace/eplace.cpp:887-904).
+    Written to variants.npz."""
+    out = {}
+    nl = synth.blob_start(synth.standard_cell(2000, seed=3))
+    for flag in ("LSE", "bb"):
+        R.set_flag(flag)
+        try:
+            ref = R.RefPlacer(nl)
+            ref.initialization(nl.target_density)
+            if flag == "LSE":
+                out["lse_init_grad_wl"] = ref.gradients()[0]
+            s = run_stage(ref)
+            for k in ("iterations", "overflow", "hpwl", "lam"):
+                out[f"{flag.lower()}_run_{k}"] = s[k]
+            ref.close()
+        finally:
+            R.clear_flag(flag)
+    mx = synth.blob_start(synth.mixed_size(5000, 6, 3, seed=5))
+    ref = R.RefPlacer(mx)
+    ref.initialization(mx.target_density)
+    cx, cy = ref.positions()
+    out["stage_init_cx"], out["stage_init_cy"] = cx, cy
+    mgp = run_stage(ref)
+    out["stage_mgp_iterations"], out["stage_mgp_lambda"] = mgp["iterations"], mgp["lam"]
+    ref.switch_filler_only()
+    x, y = ref.positions()
+    out["stage_fo_start_cx"], out["stage_fo_start_cy"] = x, y
+    fo = run_stage(ref)
+    for k in ("iterations", "overflow", "hpwl", "lam", "cx", "cy"):
+        out["stage_fo_" + k] = fo[k]
+    ref.switch_cgp()
+    out["stage_cgp_start_lambda"] = np.float64(ref.info()["lambda"])
+    cg = run_stage(ref)
+    for k in ("iterations", "overflow", "hpwl", "lam", "cx", "cy"):
+        out["stage_cgp_" + k] = cg[k]
+    ref.close()
+    path = os.path.join(HERE, "variants.npz")
+    np.savez_compressed(path, **out)
+    print("variants:", {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
+
+
 def record_bench_reference():
     """The reference's whole mGP run on bench.py's 200k-cell design (about a
     minute of CPU): iterations to overflow < 0.1, final overflow and HPWL.
@@ -145,8 +205,10 @@ def record_bench_reference():
 
 
 if __name__ == "__main__":
-    check_reader()
-    for name, nl, qp in designs():
-        record(name, nl, qp)
+    if "--variants-only" not in sys.argv:
+        check_reader()
+        for name, nl, qp in designs():
+            record(name, nl, qp)
+    record_variants()
     if "--bench" in sys.argv:
         record_bench_reference()
