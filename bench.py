@@ -163,6 +163,17 @@ def roofline(times, iterations):
     return r
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of `values` over all ranks (each rank's device
+    times; the job takes as long as its slowest replica).  `dist` is None for
+    a single process."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -280,10 +291,7 @@ def main():
     e2e_ms = statistics.mean(e2e_times)
 
     kt = eng.time_kernels(reps=20)
-    vals = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = vals.tolist()
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], "cuda")
     last = runs[-1]
     if rank == 0:
         out = {"metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": args.steps,
