@@ -51,6 +51,7 @@ struct DevScalars {
     int step_rule;
     int mgp_iterations;
     int step_cap;      // > 0: also stop after this many steps (bounded runs)
+    int bk_accept;     // backtracking: the last trial was accepted
 };
 
 // ----- geometry (reference float semantics) -------------------------------

@@ -44,6 +44,7 @@ struct ep_engine {
     float2 *size = nullptr, *pin_off = nullptr, *pin_grad = nullptr, *gd_big = nullptr;
     float2 *dump_gd = nullptr, *dump_gwl = nullptr, *field = nullptr, *static_map = nullptr;
     float2 *staging = nullptr;
+    float2 *bk_ysave = nullptr, *bk_gtrial = nullptr, *bk_xtrial = nullptr;  // backtracking trials
     uint8_t *flags = nullptr;
     float *npins = nullptr, *area = nullptr, *rho = nullptr, *node_f = nullptr, *filler_f = nullptr;
     float *sxy = nullptr;
@@ -260,8 +261,11 @@ int kernels_per_eval(const ep_engine *e) {
 
 int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
 
-// totalGradientUpdate: enqueue one gradient evaluation at the current positions.
-void enqueue_eval(ep_engine *e, int stepping) {
+// totalGradientUpdate: enqueue one gradient evaluation at the current
+// positions.  The direction goes to gout; the Lipschitz sums compare with
+// (g_ref, y_ref).
+void enqueue_eval_to(ep_engine *e, int stepping, float2 *gout, const float2 *g_ref,
+                     const float2 *y_ref) {
     e->launches += kernels_per_eval(e);
     cudaStream_t st = e->st;
     bool keep = e->prm.keep_maps != 0;
@@ -276,9 +280,11 @@ void enqueue_eval(ep_engine *e, int stepping) {
     dct_run(e->dct, e->rho, e->field, keep ? e->phi : nullptr, e->S, st);
     launch_wirelength(e->kc, e->dn, e->pin_grad, e->S, st);
     launch_gather_big(e->kc, e->dn, e->field, e->gd_big, e->S, st);
-    launch_combine(e->kc, e->dn, e->field, e->gd_big, e->pin_grad, e->g, e->g_prev, e->y_prev,
+    launch_combine(e->kc, e->dn, e->field, e->gd_big, e->pin_grad, gout, g_ref, y_ref,
                    keep ? e->dump_gd : nullptr, keep ? e->dump_gwl : nullptr, stepping, e->S, st);
 }
+
+void enqueue_eval(ep_engine *e, int stepping) { enqueue_eval_to(e, stepping, e->g, e->g_prev, e->y_prev); }
 
 void enqueue_step(ep_engine *e) {
     enqueue_eval(e, 1);
@@ -289,6 +295,49 @@ void enqueue_step(ep_engine *e) {
 void enqueue_hpwl(ep_engine *e, int mode) {
     launch_hpwl(e->kc, e->dn, mode, e->S, e->st);
     e->launches += kernels_per_hpwl(e);
+}
+
+// The reference retries forever when no trial is accepted; the engine stops
+// after this many trials of one step and reports EP_ERR_TIMEOUT.
+constexpr int kBktrkMaxTrials = 64;
+
+// One step of EplaceNesterovOpt::opt_step_bktrk (Optimization/nesterov.hpp:
+// 310-369) plus updatePenaltyFactor: evaluate at y_k (1/L step, a_{k+1}),
+// then move from y_k along g_k and re-evaluate at the trial point until the
+// new 1/L is at least 0.95 of the step tried (combine, stepping mode 2),
+// then make the trial the new iterate.  Returns with the step committed.
+ep_status bktrk_step(ep_engine *e) {
+    const size_t bytes = sizeof(float2) * e->n_obj;
+    cudaStream_t st = e->st;
+    enqueue_eval(e, 1);
+    CK(cudaMemcpyAsync(e->bk_ysave, e->pos, bytes, cudaMemcpyDeviceToDevice, st));
+    for (int t = 0;; t++) {
+        launch_bktrk_move(e->kc, e->dn, e->bk_ysave, e->g, e->x, e->pos, e->bk_xtrial, e->S, st);
+        enqueue_eval_to(e, 2, e->bk_gtrial, e->g, e->bk_ysave);
+        e->launches += 1;
+        CK(cudaGetLastError());
+        ep_status s = fetch_scalars(e);
+        if (s) return s;
+        if (e->hS->bk_accept || e->hS->status) break;
+        if (t + 1 >= kBktrkMaxTrials) {
+            s = update_scalars(e, [](DevScalars &h) {
+                h.status |= 1 << EP_ERR_TIMEOUT;
+                h.stop_pending = 1;
+            });
+            if (s) return s;
+            break;
+        }
+    }
+    // last_iter = cur_iter; cur_iter = new_iter (nesterov.hpp:365-367)
+    CK(cudaMemcpyAsync(e->y_prev, e->bk_ysave, bytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(e->g_prev, e->g, bytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(e->g, e->bk_gtrial, bytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(e->x, e->bk_xtrial, bytes, cudaMemcpyDeviceToDevice, st));
+    launch_bktrk_commit(e->S, st);
+    e->launches += 1;
+    enqueue_hpwl(e, 2);  // updatePenaltyFactor at the new positions
+    CK(cudaGetLastError());
+    return fetch_scalars(e);
 }
 
 ep_status build_graph(ep_engine *e, int iters) {
@@ -717,6 +766,9 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         return s;
     for (int v = 0; v < 3; v++)
         if ((s = dupload(e, e->view_idx[v], e->h_view[v]))) return s;
+    if (P.step_rule == EP_STEP_BKTRK &&
+        ((s = dalloc(e, e->bk_ysave, no)) || (s = dalloc(e, e->bk_gtrial, no)) || (s = dalloc(e, e->bk_xtrial, no))))
+        return s;
     if (P.keep_maps) {
         if ((s = dalloc(e, e->node_f, nb)) || (s = dalloc(e, e->filler_f, nb)) ||
             (s = dalloc(e, e->phi, nb)) || (s = dalloc(e, e->dump_gd, no)) ||
@@ -1088,8 +1140,9 @@ ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
     }
     if (stopped) *stopped = 0;
     if (e->prm.step_rule == EP_STEP_BKTRK) {
-        e->err = "backtracking step runs through ep_nesterov_run only";
-        return EP_ERR_UNSUPPORTED;
+        s = bktrk_step(e);
+        if (s) return s;
+        return device_status(e);
     }
     enqueue_step(e);
     enqueue_hpwl(e, 2);  // updatePenaltyFactor
@@ -1118,7 +1171,8 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
     s = update_scalars(e, [max_steps](DevScalars &h) { h.step_cap = max_steps > 0 ? max_steps : 0; });
     if (s) return s;
     const int K = 8;
-    if (!e->graph || e->graph_iters != K) {
+    const bool bktrk = e->prm.step_rule == EP_STEP_BKTRK;
+    if (!bktrk && (!e->graph || e->graph_iters != K)) {
         s = build_graph(e, K);
         if (s) return s;
     }
@@ -1126,7 +1180,17 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
     CK(cudaEventRecord(e->ev0, e->st));
     const int cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + K;
     int launched = 0;
-    while (true) {
+    if (bktrk) {
+        // host-driven steps: the number of trials per step is data-dependent
+        s = fetch_scalars(e);
+        if (s) return s;
+        while (!e->hS->done && launched <= cap) {
+            s = bktrk_step(e);
+            if (s) return s;
+            launched++;
+        }
+    }
+    while (!bktrk) {
         CK(cudaGraphLaunch(e->graph, e->st));
         e->launches += e->graph_kernels;
         launched += K;

@@ -114,6 +114,12 @@ void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *fi
                     DevScalars *S, cudaStream_t st);
 void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
                    const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S, cudaStream_t st);
+// Backtracking step rule: one trial move from y_k (ysave) along g_k, and the
+// scalar commit of an accepted trial (combine in stepping mode 2 decides).
+void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const float2 *ysave, const float2 *g,
+                       const float2 *x, float2 *pos, float2 *xtrial, const DevScalars *S,
+                       cudaStream_t st);
+void launch_bktrk_commit(DevScalars *S, cudaStream_t st);
 void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
                         cudaStream_t st);
 void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, const float2 *x,

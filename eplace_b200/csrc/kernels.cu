@@ -549,6 +549,21 @@ k_gather_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ 
 }
 
 // --------------------------------------------------------------- combine --
+// stop_condition after a step (Optimization/nesterov.hpp:86-122): `it` steps
+// taken in this stage, tau of the last gradient evaluation.
+__device__ int stop_after_step(const DevScalars *S, double tau, int it) {
+    int stop;
+    if (S->stage == EP_STAGE_MGP)
+        stop = tau < (double)S->target_overflow || it > S->max_iter;
+    else if (S->stage == EP_STAGE_FILLERONLY)
+        stop = it >= 20;
+    else
+        stop = tau < (double)0.07f || it > S->max_iter;
+    if (S->step_cap > 0 && it >= S->step_cap) stop = 1;
+    if (S->status) stop = 1;
+    return stop;
+}
+
 __global__ void __launch_bounds__(kThreads)
 k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
           const float2 *__restrict__ gd_big, const float2 *__restrict__ pin_grad,
@@ -636,7 +651,9 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
             dump_gd[o] = make_float2(gdx, gdy);
             dump_gwl[o] = make_float2(wx, wy);
         }
-        if (stepping && iter > 0 && (f & kInView)) {
+        // Lipschitz sums against the previous reference point: from the
+        // second step on, and for every backtracking trial (stepping == 2)
+        if ((stepping == 2 || (stepping && iter > 0)) && (f & kInView)) {
             float2 gp = g_prev[o], yp = y_prev[o];
             double dgx = __fsub_rn(gg.x, gp.x), dgy = __fsub_rn(gg.y, gp.y);
             double dyx = __fsub_rn(p.x, yp.x), dyy = __fsub_rn(p.y, yp.y);
@@ -659,7 +676,19 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
                 S->lambda0_mode = 0;
                 if (!isfinite(S->lambda)) S->status |= 1 << EP_ERR_NAN;
             }
-            if (stepping) {
+            if (stepping == 2) {
+                // backtracking trial (opt_step_bktrk, Optimization/nesterov.hpp:351-364):
+                // 1/L between the trial point and y_k; accepted when it is at
+                // least BKTRK_EPS (0.95, nesterov.hpp:37) of the step tried
+                double ns = sqrt(dy2) / sqrt(dg2);
+                if (!isfinite(ns)) {
+                    S->status |= 1 << EP_ERR_NAN;
+                    ns = 0.0;
+                }
+                S->bk_accept = 0.95 * S->step <= ns;
+                S->step = ns;
+                S->stop_pending = stop_after_step(S, S->tau, S->iter + 1);
+            } else if (stepping) {
                 double step = 1.0;
                 if (S->iter > 0) {
                     double lip = sqrt(dy2) / sqrt(dg2);  // 1/L
@@ -680,19 +709,7 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
                 S->step = step;
                 S->coef = (a - 1.0) / an;
                 S->a = an;
-                // stop_condition after this step (nesterov.hpp:86-122)
-                int it = S->iter + 1;
-                double tau = S->tau;
-                int stop;
-                if (S->stage == EP_STAGE_MGP)
-                    stop = tau < (double)S->target_overflow || it > S->max_iter;
-                else if (S->stage == EP_STAGE_FILLERONLY)
-                    stop = it >= 20;
-                else
-                    stop = tau < (double)0.07f || it > S->max_iter;
-                if (S->step_cap > 0 && it >= S->step_cap) stop = 1;
-                if (S->status) stop = 1;
-                S->stop_pending = stop;
+                S->stop_pending = stop_after_step(S, S->tau, S->iter + 1);
             }
         }
     }
@@ -736,6 +753,43 @@ k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restr
             S->done = 1;
             if (S->stage == EP_STAGE_MGP) S->mgp_iterations = S->iter;
         }
+    }
+}
+
+// Backtracking trial move (opt_step_bktrk, Optimization/nesterov.hpp:337-349):
+// from y_k (kept in ysave) x_t = y_k + step g_k, y_t = x_t + coef (x_t - x_k);
+// the positions become clamp(y_t) and x_t is kept in xtrial until accepted.
+__global__ void __launch_bounds__(kThreads)
+k_bktrk_move(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
+             const float2 *__restrict__ ysave, const float2 *__restrict__ gin,
+             const float2 *__restrict__ x, float2 *__restrict__ pos, float2 *__restrict__ xtrial,
+             const DevScalars *__restrict__ S) {
+    pdl_begin();
+    if (S->done) return;
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    if (!(flags[o] & kInView)) {
+        xtrial[o] = x[o];
+        return;
+    }
+    float s = (float)S->step, c = (float)S->coef;
+    float2 y = ysave[o], gg = gin[o], xo = x[o];
+    float2 xn = make_float2(__fadd_rn(y.x, __fmul_rn(gg.x, s)), __fadd_rn(y.y, __fmul_rn(gg.y, s)));
+    float2 yn = make_float2(__fadd_rn(xn.x, __fmul_rn(__fsub_rn(xn.x, xo.x), c)),
+                            __fadd_rn(xn.y, __fmul_rn(__fsub_rn(xn.y, xo.y), c)));
+    xtrial[o] = xn;
+    pos[o] = clamp_center(g, yn, size[o]);
+}
+
+// The accepted trial ends the step: the scalar side of k_update.
+__global__ void k_bktrk_commit(DevScalars *__restrict__ S) {
+    pdl_begin();
+    if (S->done) return;
+    S->iter += 1;
+    S->lambda_pending = 1;
+    if (S->stop_pending) {
+        S->done = 1;
+        if (S->stage == EP_STAGE_MGP) S->mgp_iterations = S->iter;
     }
 }
 
@@ -846,6 +900,15 @@ void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, floa
     launch_k(k_update, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
              pos, x, g, y_prev, g_prev, S);
 }
+
+void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const float2 *ysave, const float2 *g,
+                       const float2 *x, float2 *pos, float2 *xtrial, const DevScalars *S,
+                       cudaStream_t st) {
+    launch_k(k_bktrk_move, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags,
+             d.size, ysave, g, x, pos, xtrial, S);
+}
+
+void launch_bktrk_commit(DevScalars *S, cudaStream_t st) { launch_k(k_bktrk_commit, 1, 1, 0, st, S); }
 
 void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
                         cudaStream_t st) {

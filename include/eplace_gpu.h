@@ -206,7 +206,11 @@ ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy);
  * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:
  * init, steps until the stage's stop condition (or max_steps > 0 steps),
  * wrap_up.  The loop runs on the device (captured CUDA graphs, step size,
- * lambda and the stop test decided on the GPU). */
+ * lambda and the stop test decided on the GPU).  With EP_STEP_BKTRK
+ * (opt_step_bktrk, nesterov.hpp:310-369) each step is driven from the host,
+ * since the number of trial evaluations is data-dependent; a step that finds
+ * no acceptable trial within 64 tries ends the run with EP_ERR_TIMEOUT (the
+ * reference retries without limit). */
 ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats);
 /* The same loop one call at a time: begin = init(), step = "if
  * (!stop_condition()) opt_step(); updatePenaltyFactor()", end = wrap_up().

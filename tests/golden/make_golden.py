@@ -135,13 +135,15 @@ def record_variants():
         whole mGP run with the log-sum-exp model (EPlace/eplace.cpp:512-549);
       * gArg "bb": the whole mGP run with the Barzilai-Borwein step
         (Optimization/nesterov.hpp:231-302);
+      * gArg "bktrk": the whole mGP run with the backtracking step
+        (Optimization/nesterov.hpp:310-369);
       * mixed-size stages: mGP, switch2FillerOnly (the reference re-draws the
         fillers with rand(); their new centres are recorded), 20 FILLERONLY
         steps, switch2cGP and the cGP run (EPlace/eplace.cpp:887-904).
     Written to variants.npz."""
     out = {}
     nl = synth.blob_start(synth.standard_cell(2000, seed=3))
-    for flag in ("LSE", "bb"):
+    for flag in ("LSE", "bb", "bktrk"):
         R.set_flag(flag)
         try:
             ref = R.RefPlacer(nl)

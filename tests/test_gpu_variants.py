@@ -6,8 +6,10 @@ reference) and the FP64 oracle:
     PlaceCommon/objects.cpp:161-241,423-437): gradient at the initial
     positions within 1e-4 of the reference; whole mGP run within 10%
     iterations and 1% HPWL;
-  * Barzilai-Borwein step (gArg "bb", Optimization/nesterov.hpp:231-302):
-    whole run within 10% iterations and 1% HPWL;
+  * Barzilai-Borwein step (gArg "bb", Optimization/nesterov.hpp:231-302) and
+    backtracking step (gArg "bktrk", :310-369): whole run within 10%
+    iterations and 1% HPWL; backtracking one step at a time gives bitwise the
+    run's positions;
   * exact exp instead of fastExp: wirelength gradient within 1e-4 of the FP64
     oracle evaluated with exp;
   * mixed-size stages (EPlace/eplace.cpp:887-904): FILLERONLY runs exactly 20
@@ -70,6 +72,34 @@ def test_bb_run_matches_reference(variants):
     assert abs(st["iterations"] - it) <= max(2, 0.1 * it), (st["iterations"], it)
     assert st["overflow"] < 0.1
     assert abs(st["hpwl"] / float(variants["bb_run_hpwl"]) - 1) < 0.01
+
+
+def test_bktrk_run_matches_reference(variants):
+    g = load_golden("stdcell_2k")
+    e = engine_at_reference_start(g, step_rule=placer.STEP_BKTRK)
+    e.initialize()
+    st = e.nesterov_run()
+    it = int(variants["bktrk_run_iterations"])
+    assert abs(st["iterations"] - it) <= max(2, 0.1 * it), (st["iterations"], it)
+    assert st["overflow"] < 0.1
+    assert abs(st["hpwl"] / float(variants["bktrk_run_hpwl"]) - 1) < 0.01
+
+
+def test_bktrk_steps_one_at_a_time_match_the_run():
+    g = load_golden("stdcell_2k")
+    runs = []
+    for stepwise in (False, True):
+        e = engine_at_reference_start(g, step_rule=placer.STEP_BKTRK)
+        e.initialize()
+        if stepwise:
+            e.nesterov_begin()
+            for _ in range(6):
+                assert not e.nesterov_step()
+            e.nesterov_end()
+        else:
+            e.nesterov_run(max_steps=6)
+        runs.append(e.get_positions())
+    assert np.array_equal(runs[0], runs[1])
 
 
 def test_exact_exp_gradient_matches_oracle():
