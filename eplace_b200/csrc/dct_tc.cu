@@ -413,15 +413,17 @@ void launch_tc(const TcGemmParams &g, dim3 grid, DevScalars *S, cudaStream_t st)
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = kSmemBytes;
     cfg.stream = st;
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[3];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     attr[1].id = cudaLaunchAttributeClusterDimension;
     attr[1].val.clusterDim.x = (unsigned)g.split;
     attr[1].val.clusterDim.y = 1;
     attr[1].val.clusterDim.z = 1;
+    attr[2].id = cudaLaunchAttributePriority;
+    attr[2].val.priority = launch_priority(true);
     cfg.attrs = attr;
-    cfg.numAttrs = 2;
+    cfg.numAttrs = 3;
     switch (g.split) {
         case 4: cudaLaunchKernelEx(&cfg, k_umma_nt<4>, g, S); break;
         case 2: cudaLaunchKernelEx(&cfg, k_umma_nt<2>, g, S); break;

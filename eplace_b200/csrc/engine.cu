@@ -27,6 +27,10 @@ struct ep_engine {
     int device = 0;
     cudaStream_t st = nullptr;
     bool own_stream = false;
+    // the per-net pass runs on its own stream, forked after prep and joined
+    // before the gather / combine, beside the Poisson GEMMs
+    cudaStream_t st_wl = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     int n_nodes = 0, n_fillers = 0, n_obj = 0, n_terms = 0, n_nets = 0, n_pins = 0;
     int n_macros = 0, n_cgp = 0;
@@ -277,8 +281,14 @@ void enqueue_eval_to(ep_engine *e, int stepping, float2 *gout, const float2 *g_r
     void *bf = e->dct.mode == EP_DCT_BF16X3 ? dct_tc_rho_planes(e->dct) : nullptr;
     launch_prep(e->kc, e->node_q, e->filler_q, e->static_map, bf ? nullptr : e->rho, bf,
                 keep ? e->node_f : nullptr, keep ? e->filler_f : nullptr, keep ? 0 : 1, e->S, st);
+    // fork: the per-net pass needs the positions and 1/gamma (from prep), not
+    // the field, so it runs beside the Poisson solve
+    cudaEventRecord(e->ev_fork, st);
+    cudaStreamWaitEvent(e->st_wl, e->ev_fork, 0);
+    launch_wirelength(e->kc, e->dn, e->pin_grad, e->S, e->st_wl);
+    cudaEventRecord(e->ev_join, e->st_wl);
     dct_run(e->dct, e->rho, e->field, keep ? e->phi : nullptr, e->S, st);
-    launch_wirelength(e->kc, e->dn, e->pin_grad, e->S, st);
+    cudaStreamWaitEvent(st, e->ev_join, 0);
     launch_gather_big(e->kc, e->dn, e->field, e->gd_big, e->S, st);
     launch_combine(e->kc, e->dn, e->field, e->gd_big, e->pin_grad, gout, g_ref, y_ref,
                    keep ? e->dump_gd : nullptr, keep ? e->dump_gwl : nullptr, stepping, e->S, st);
@@ -445,6 +455,13 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     e->own_stream = true;
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
+    {
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CK(cudaStreamCreateWithPriority(&e->st_wl, cudaStreamNonBlocking, lo));
+        CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+    }
     e->rng.seed(P.filler_seed);
 
     const int nn = nl->num_nodes, nt = nl->num_terminals, nnet = nl->num_nets, nr = nl->num_rows;
@@ -835,6 +852,9 @@ void ep_destroy(ep_engine *e) {
     if (e->hS) cudaFreeHost(e->hS);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
+    if (e->st_wl) cudaStreamDestroy(e->st_wl);
     if (e->own_stream && e->st) cudaStreamDestroy(e->st);
     delete e;
 }

@@ -30,11 +30,36 @@ inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sme
     cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
+// Stream priorities of the loop's two branches: the Poisson GEMMs (critical
+// path) launch at the device's highest priority, the per-net pass that runs
+// beside them at the lowest, so blocks of the GEMM chain are placed first
+// whenever SM resources free up.
+int launch_priority(bool high);
+
+// launch_k with a scheduling priority attribute as well.
+template <typename... KArgs, typename... Args>
+inline void launch_kp(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                      int priority, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Per-net pass: one warp per task.  Nets of up to kWarpPins pins share a warp
 // (floor(kWarpPins / degree) nets of one degree, a pin per lane); larger nets
 // take a warp each, their first kStagedPins pins staged in shared memory.
 constexpr int kWarpPins = 32;
-constexpr int kStagedPins = 256;
+constexpr int kStagedPins = 128;
 constexpr int kNetWarps = 8;  // warps per block of the per-net pass
 // Objects whose bin footprint may exceed this many bins take the
 // block-per-object scatter / gather path.

@@ -283,7 +283,8 @@ __device__ __forceinline__ double lambda_multiplier(double cur, double last) {
 __device__ void finish_wirelength(DevScalars *S, double hp, double wl) {
     S->wirelength = wl;
     S->hpwl = hp;
-    if (!isfinite(hp)) S->status |= 1 << EP_ERR_NAN;
+    // atomic: the Poisson GEMMs, running beside this pass, may raise a bit too
+    if (!isfinite(hp)) atomicOr(&S->status, 1 << EP_ERR_NAN);
     if (S->lambda_pending) {
         S->lambda *= lambda_multiplier(hp, S->last_hpwl);
         S->last_hpwl = hp;
@@ -831,6 +832,17 @@ __global__ void k_wrap_up(Grid g, int n, const uint8_t *__restrict__ flags,
 }  // namespace
 
 // ------------------------------------------------------------- launchers --
+int launch_priority(bool high) {
+    static int lo = 1, hi = 1;
+    if (lo > 0) {
+        int l = 0, h = 0;
+        cudaDeviceGetStreamPriorityRange(&l, &h);
+        hi = h;
+        lo = l;
+    }
+    return high ? hi : lo;
+}
+
 int prep_blocks(const Grid &g) { return std::min(blocks_for(g.nx * g.ny, kThreads), 148 * 8); }
 
 int reduction_blocks(const DeviceNetlist &d, int which) {
@@ -865,8 +877,8 @@ void launch_nets(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad, d
                  int mode, DevScalars *S, cudaStream_t st) {
     PinCtx pc{d.pin_owner, d.pin_off, d.pos};
     if (d.n_net_tasks == 0) return;
-    launch_k(k_wl<WL, EXACT, LSE>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, d.net_tasks,
-             d.n_net_tasks, pc, pin_grad, c.want_wl_value, partials, mode, S);
+    launch_kp(k_wl<WL, EXACT, LSE>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, launch_priority(false),
+              d.net_tasks, d.n_net_tasks, pc, pin_grad, c.want_wl_value, partials, mode, S);
 }
 
 void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad,
