@@ -147,6 +147,16 @@ def ncu_traffic():
     return {}
 
 
+def group_rate(t, hbm, tf):
+    """(achieved, fraction of peak) of one kernel group: FLOP/s against the
+    bf16 tensor peak when it has flops, else bytes/s against HBM."""
+    if t["flops"] > 0:
+        a = t["flops"] / (t["ms"] * 1e-3) / 1e12
+        return a, a / tf
+    a = t["bytes"] / (t["ms"] * 1e-3) / 1e9
+    return a, a / hbm
+
+
 def roofline(times, iterations):
     """Dominant kernel group by time per iteration; its achieved rate vs peak."""
     hbm, tf, src = peaks()
@@ -159,7 +169,8 @@ def roofline(times, iterations):
         ach = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
         r = dict(bound="hbm", achieved=ach, peak=hbm, unit="GB/s", frac=ach / hbm)
     r.update(kernel=dom["name"], ms_per_launch=dom["ms"], traffic=traffic, peak_source=src,
-             groups={t["name"]: round(t["ms"] * 1e3, 2) for t in times})
+             groups={t["name"]: round(t["ms"] * 1e3, 2) for t in times},
+             group_frac={t["name"]: round(group_rate(t, hbm, tf)[1], 4) for t in times if t["bytes"] or t["flops"]})
     return r
 
 
