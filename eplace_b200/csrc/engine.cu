@@ -260,7 +260,7 @@ ep_status device_status(ep_engine *e) {
 // Kernels one enqueue_eval launches (the DCT is four GEMMs).
 int kernels_per_eval(const ep_engine *e) {
     const DeviceNetlist &d = e->dn;
-    return 1 + (d.n_big_objs > 0) + 1 + 4 + (d.n_net_tasks > 0) + (d.n_big_objs > 0) + 1;
+    return 1 + 1 + 4 + (d.n_net_tasks > 0) + (d.n_big_objs > 0) + 1;
 }
 
 int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
@@ -269,15 +269,15 @@ int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
 // positions.  The direction goes to gout; the Lipschitz sums compare with
 // (g_ref, y_ref).
 void enqueue_eval_to(ep_engine *e, int stepping, float2 *gout, const float2 *g_ref,
-                     const float2 *y_ref) {
-    e->launches += kernels_per_eval(e);
+                     const float2 *y_ref, bool scatter = true) {
+    e->launches += kernels_per_eval(e) - (scatter ? 0 : 1);
     cudaStream_t st = e->st;
     bool keep = e->prm.keep_maps != 0;
     if (keep) {
         cudaMemsetAsync(e->node_q, 0, sizeof(unsigned long long) * e->grid.nx * e->grid.ny, st);
         cudaMemsetAsync(e->filler_q, 0, sizeof(unsigned long long) * e->grid.nx * e->grid.ny, st);
     }
-    launch_scatter(e->kc, e->dn, e->node_q, e->filler_q, e->S, st);
+    if (scatter) launch_scatter(e->kc, e->dn, e->node_q, e->filler_q, e->S, st);
     void *bf = e->dct.mode == EP_DCT_BF16X3 ? dct_tc_rho_planes(e->dct) : nullptr;
     launch_prep(e->kc, e->node_q, e->filler_q, e->static_map, bf ? nullptr : e->rho, bf,
                 keep ? e->node_f : nullptr, keep ? e->filler_f : nullptr, keep ? 0 : 1, e->S, st);
@@ -295,6 +295,24 @@ void enqueue_eval_to(ep_engine *e, int stepping, float2 *gout, const float2 *g_r
 }
 
 void enqueue_eval(ep_engine *e, int stepping) { enqueue_eval_to(e, stepping, e->g, e->g_prev, e->y_prev); }
+
+// A step of the captured loop when the maps are not kept: the evaluation
+// finds the maps already filled by the previous step's update (or by the
+// scatter the run issues first), and the update fills them for the next one.
+bool fused_loop(const ep_engine *e) { return e->prm.keep_maps == 0; }
+
+void enqueue_step(ep_engine *e);
+
+void enqueue_loop_step(ep_engine *e) {
+    if (!fused_loop(e)) {
+        enqueue_step(e);
+        return;
+    }
+    enqueue_eval_to(e, 1, e->g, e->g_prev, e->y_prev, false);
+    launch_update_scatter(e->kc, e->dn, e->pos, e->x, e->g, e->y_prev, e->g_prev, e->node_q, e->filler_q,
+                          e->S, e->st);
+    e->launches += 1;
+}
 
 void enqueue_step(ep_engine *e) {
     enqueue_eval(e, 1);
@@ -358,7 +376,7 @@ ep_status build_graph(ep_engine *e, int iters) {
     cudaGraph_t g = nullptr;
     int64_t before = e->launches;
     CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < iters; i++) enqueue_step(e);
+    for (int i = 0; i < iters; i++) enqueue_loop_step(e);
     CK(cudaStreamEndCapture(e->st, &g));
     e->graph_kernels = e->launches - before;  // counted per replay, not at capture
     e->launches = before;
@@ -1210,6 +1228,11 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
             launched++;
         }
     }
+    if (!bktrk && fused_loop(e)) {
+        // the first step's maps (the graph's steps start at prep)
+        launch_scatter(e->kc, e->dn, e->node_q, e->filler_q, e->S, e->st);
+        e->launches += 1;
+    }
     while (!bktrk) {
         CK(cudaGraphLaunch(e->graph, e->st));
         e->launches += e->graph_kernels;
@@ -1217,6 +1240,14 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
         CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
         CK(cudaStreamSynchronize(e->st));
         if (e->hS->done || launched > cap + K) break;
+    }
+    if (!bktrk && fused_loop(e)) {
+        // clear in any case: the maps must be empty when the next evaluation
+        // scatters (the stopping step scatters nothing, so this is a no-op
+        // unless the loop was cut off)
+        const size_t nb = (size_t)e->grid.nx * e->grid.ny;
+        CK(cudaMemsetAsync(e->node_q, 0, sizeof(unsigned long long) * nb, e->st));
+        CK(cudaMemsetAsync(e->filler_q, 0, sizeof(unsigned long long) * nb, e->st));
     }
     enqueue_hpwl(e, 2);  // the lambda update owed by the last step
     launch_wrap_up(e->kc, e->dn, e->pos, e->x, e->st);

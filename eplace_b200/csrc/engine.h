@@ -139,6 +139,11 @@ void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *fi
                     DevScalars *S, cudaStream_t st);
 void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
                    const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S, cudaStream_t st);
+// The update of the captured loop: also scatters the new positions into the
+// (clear) density maps for the next evaluation, unless the step ends the stage.
+void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
+                           const float2 *g, float2 *y_prev, float2 *g_prev, unsigned long long *node_q,
+                           unsigned long long *filler_q, DevScalars *S, cudaStream_t st);
 // Backtracking step rule: one trial move from y_k (ysave) along g_k, and the
 // scalar commit of an accepted trial (combine in stepping mode 2 decides).
 void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const float2 *ysave, const float2 *g,

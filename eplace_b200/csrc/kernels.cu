@@ -52,18 +52,10 @@ __device__ __forceinline__ float contrib_scale(const Rect &r, uint8_t f, float t
     return (f & kMacro) ? __fmul_rn(s, td) : s;
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_scatter_small(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
-                const uint8_t *__restrict__ flags, int n, double qscale,
-                unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
-                const DevScalars *__restrict__ S) {
-    pdl_begin();
-    if (S->done) return;
-    int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n) return;
-    uint8_t f = flags[o];
-    if (f & kBig) return;
-    float2 p = pos[o], s = size[o];
+// One object of the thread-per-object path (kBig objects excluded).
+__device__ __forceinline__ void scatter_small_object(const Grid &g, float2 p, float2 s, uint8_t f, double qscale,
+                                                     unsigned long long *__restrict__ node_q,
+                                                     unsigned long long *__restrict__ filler_q) {
     Rect r = object_rect(g, p.x, p.y, s.x, s.y);
     int i0, i1, j0, j1;
     bin_range(g, r, i0, i1, j0, j1);
@@ -73,26 +65,40 @@ k_scatter_small(Grid g, const float2 *__restrict__ pos, const float2 *__restrict
         for (int j = j0; j <= j1; j++) scatter_one(g, r, scale, i, j, qscale, map);
 }
 
-__global__ void __launch_bounds__(128)
-k_scatter_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
-              const uint8_t *__restrict__ flags, const int32_t *__restrict__ big, double qscale,
-              unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
-              const DevScalars *__restrict__ S) {
-    pdl_begin();
-    if (S->done) return;
-    int o = big[blockIdx.x];
-    uint8_t f = flags[o];
-    float2 p = pos[o], s = size[o];
+// One kBig object by a whole block, its bins strided over the threads.
+__device__ __forceinline__ void scatter_big_object(const Grid &g, float2 p, float2 s, uint8_t f, double qscale,
+                                                   unsigned long long *__restrict__ node_q,
+                                                   unsigned long long *__restrict__ filler_q) {
     Rect r = object_rect(g, p.x, p.y, s.x, s.y);
     int i0, i1, j0, j1;
     bin_range(g, r, i0, i1, j0, j1);
+    if (i1 < i0 || j1 < j0) return;
     float scale = contrib_scale(r, f, g.td);
     unsigned long long *map = (f & kFiller) ? filler_q : node_q;
-    int wy = j1 - j0 + 1;
-    int nb = (i1 - i0 + 1) * wy;
-    if (i1 < i0 || j1 < j0) return;
+    const int wy = j1 - j0 + 1, nb = (i1 - i0 + 1) * wy;
     for (int t = threadIdx.x; t < nb; t += blockDim.x)
         scatter_one(g, r, scale, i0 + t / wy, j0 + t % wy, qscale, map);
+}
+
+// Blocks [0, small_blocks): thread per object; the blocks after them: one
+// kBig object each.
+__global__ void __launch_bounds__(kThreads)
+k_scatter(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
+          const uint8_t *__restrict__ flags, int n, int small_blocks, const int32_t *__restrict__ big,
+          double qscale, unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
+          const DevScalars *__restrict__ S) {
+    pdl_begin();
+    if (S->done) return;
+    if ((int)blockIdx.x >= small_blocks) {
+        const int o = big[blockIdx.x - small_blocks];
+        scatter_big_object(g, pos[o], size[o], flags[o], qscale, node_q, filler_q);
+        return;
+    }
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const uint8_t f = flags[o];
+    if (f & kBig) return;
+    scatter_small_object(g, pos[o], size[o], f, qscale, node_q, filler_q);
 }
 
 // ------------------------------------------------------------------- prep --
@@ -729,6 +735,35 @@ __device__ __forceinline__ float2 clamp_center(const Grid &g, float2 c, float2 s
     return make_float2(x, y);
 }
 
+// x_{k+1} = y_k + s g_k, y_{k+1} = x_{k+1} + c (x_{k+1} - x_k)
+// (opt_step_vanilla, Optimization/nesterov.hpp:391-404); returns the clamped
+// new position, which becomes the object's position.
+__device__ __forceinline__ float2 nesterov_move(const Grid &g, int o, float s, float c,
+                                                const float2 *__restrict__ size, float2 *__restrict__ pos,
+                                                float2 *__restrict__ x, const float2 *__restrict__ gin,
+                                                float2 *__restrict__ y_prev, float2 *__restrict__ g_prev) {
+    float2 y = pos[o], gg = gin[o], xo = x[o];
+    float2 xn = make_float2(__fadd_rn(y.x, __fmul_rn(gg.x, s)), __fadd_rn(y.y, __fmul_rn(gg.y, s)));
+    float2 yn = make_float2(__fadd_rn(xn.x, __fmul_rn(__fsub_rn(xn.x, xo.x), c)),
+                            __fadd_rn(xn.y, __fmul_rn(__fsub_rn(xn.y, xo.y), c)));
+    y_prev[o] = y;
+    g_prev[o] = gg;
+    x[o] = xn;
+    const float2 p = clamp_center(g, yn, size[o]);
+    pos[o] = p;
+    return p;
+}
+
+// The scalar side of the end of a step (last block of the update).
+__device__ __forceinline__ void end_step(DevScalars *S) {
+    S->iter += 1;
+    S->lambda_pending = 1;
+    if (S->stop_pending) {
+        S->done = 1;
+        if (S->stage == EP_STAGE_MGP) S->mgp_iterations = S->iter;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
 k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
          float2 *__restrict__ pos, float2 *__restrict__ x, const float2 *__restrict__ gin,
@@ -736,25 +771,47 @@ k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restr
     pdl_begin();
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o < n && (flags[o] & kInView)) {
-        float s = (float)S->step, c = (float)S->coef;
-        float2 y = pos[o], gg = gin[o], xo = x[o];
-        float2 xn = make_float2(__fadd_rn(y.x, __fmul_rn(gg.x, s)), __fadd_rn(y.y, __fmul_rn(gg.y, s)));
-        float2 yn = make_float2(__fadd_rn(xn.x, __fmul_rn(__fsub_rn(xn.x, xo.x), c)),
-                                __fadd_rn(xn.y, __fmul_rn(__fsub_rn(xn.y, xo.y), c)));
-        y_prev[o] = y;
-        g_prev[o] = gg;
-        x[o] = xn;
-        pos[o] = clamp_center(g, yn, size[o]);
-    }
-    if (threadIdx.x == 0 && last_block(&S->cnt_upd, gridDim.x)) {
-        S->iter += 1;
-        S->lambda_pending = 1;
-        if (S->stop_pending) {
-            S->done = 1;
-            if (S->stage == EP_STAGE_MGP) S->mgp_iterations = S->iter;
+    if (o < n && (flags[o] & kInView))
+        nesterov_move(g, o, (float)S->step, (float)S->coef, size, pos, x, gin, y_prev, g_prev);
+    if (threadIdx.x == 0 && last_block(&S->cnt_upd, gridDim.x)) end_step(S);
+}
+
+// The update of the captured loop, with the next evaluation's scatter fused
+// in: every object is scattered at its new position right after its move
+// (objects outside the stage view at their unchanged one).  kBig objects are
+// moved and scattered by a block of their own (the blocks after
+// small_blocks).  The step that ends the stage scatters nothing, so the maps
+// stay clear (prep clears them after each read).
+__global__ void __launch_bounds__(kThreads)
+k_update_scatter(Grid g, int n, int small_blocks, const int32_t *__restrict__ big,
+                 const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
+                 float2 *__restrict__ pos, float2 *__restrict__ x, const float2 *__restrict__ gin,
+                 float2 *__restrict__ y_prev, float2 *__restrict__ g_prev, double qscale,
+                 unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
+                 DevScalars *__restrict__ S) {
+    pdl_begin();
+    __shared__ float2 big_pos;
+    if (S->done) return;
+    const float s = (float)S->step, c = (float)S->coef;
+    const bool scatter = !S->stop_pending;
+    if ((int)blockIdx.x >= small_blocks) {
+        const int o = big[blockIdx.x - small_blocks];
+        const uint8_t f = flags[o];
+        if (threadIdx.x == 0)
+            big_pos = (f & kInView) ? nesterov_move(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
+        __syncthreads();
+        if (scatter) scatter_big_object(g, big_pos, size[o], f, qscale, node_q, filler_q);
+    } else {
+        const int o = blockIdx.x * blockDim.x + threadIdx.x;
+        if (o < n) {
+            const uint8_t f = flags[o];
+            if (!(f & kBig)) {
+                const float2 p = (f & kInView) ? nesterov_move(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
+                if (scatter) scatter_small_object(g, p, size[o], f, qscale, node_q, filler_q);
+            }
         }
     }
+    if (threadIdx.x == 0 && last_block(&S->cnt_upd, gridDim.x)) end_step(S);
 }
 
 // Backtracking trial move (opt_step_bktrk, Optimization/nesterov.hpp:337-349):
@@ -854,11 +911,17 @@ int reduction_blocks(const DeviceNetlist &d, int which) {
 
 void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, unsigned long long *node_q,
                     unsigned long long *filler_q, const DevScalars *S, cudaStream_t st) {
-    launch_k(k_scatter_small, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.pos, d.size,
-             d.flags, d.n_obj, c.qscale, node_q, filler_q, S);
-    if (d.n_big_objs > 0)
-        launch_k(k_scatter_big, d.n_big_objs, 128, 0, st, c.grid, d.pos, d.size, d.flags, d.big_objs,
-                 c.qscale, node_q, filler_q, S);
+    const int sb = blocks_for(d.n_obj, kThreads);
+    launch_k(k_scatter, sb + d.n_big_objs, kThreads, 0, st, c.grid, d.pos, d.size, d.flags, d.n_obj, sb,
+             d.big_objs, c.qscale, node_q, filler_q, S);
+}
+
+void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
+                           const float2 *g, float2 *y_prev, float2 *g_prev, unsigned long long *node_q,
+                           unsigned long long *filler_q, DevScalars *S, cudaStream_t st) {
+    const int sb = blocks_for(d.n_obj, kThreads);
+    launch_k(k_update_scatter, sb + d.n_big_objs, kThreads, 0, st, c.grid, d.n_obj, sb, d.big_objs,
+             d.flags, d.size, pos, x, g, y_prev, g_prev, c.qscale, node_q, filler_q, S);
 }
 
 void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long long *filler_q,

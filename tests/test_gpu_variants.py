@@ -161,6 +161,29 @@ def test_mixed_size_stage_sequence(variants):
     assert abs(cg["hpwl"] / float(variants["stage_cgp_hpwl"]) - 1) < 0.02
 
 
+@pytest.mark.parametrize("design", ["stdcell_2k", "mixed_5k"])
+def test_fused_update_scatter_loop_matches_separate_scatter(design):
+    """Without kept maps the captured loop scatters inside the update kernel;
+    with them it scatters at the start of each evaluation.  Same integer maps,
+    so the runs agree bit for bit (mixed_5k has block-per-object objects).  A
+    capped run must leave the maps clear: the next evaluation sees the same
+    overflow either way."""
+    g = load_golden(design)
+    res = []
+    for keep in (1, 0):
+        e = engine_at_reference_start(g, keep_maps=keep)
+        e.initialize()
+        capped = e.nesterov_run(max_steps=7)
+        e.eval_gradient()
+        tau_after = e.query()["overflow"]
+        st = e.nesterov_run()
+        res.append((capped["iterations"], tau_after, st["iterations"], e.get_positions()))
+    assert res[0][0] == res[1][0] == 7
+    assert res[0][1] == res[1][1]
+    assert res[0][2] == res[1][2]
+    assert np.array_equal(res[0][3], res[1][3])
+
+
 def test_nan_position_reported_and_engine_recovers():
     g = load_golden("stdcell_2k")
     e = engine_at_reference_start(g)
