@@ -143,6 +143,18 @@ __device__ __forceinline__ double rect_bin_overlap(const Grid &g, const Rect &r,
     return overlap_area(l, b, rr, t, r.llx, r.lly, r.urx, r.ury);
 }
 
+// PlaceDB::setModuleCenter_2D clamp (PlaceDB/placedb.cpp:257-281), double
+// compares and double sums stored to float, as the reference evaluates them.
+__device__ __forceinline__ float2 clamp_center(const Grid &g, float2 c, float2 s) {
+    double hw = 0.5 * (double)s.x, hh = 0.5 * (double)s.y;
+    float x = c.x, y = c.y;
+    if ((double)x - hw < (double)g.llx) x = (float)((double)g.llx + hw + kEps);
+    if ((double)x + hw > (double)g.urx) x = (float)((double)g.urx - hw - kEps);
+    if ((double)y - hh < (double)g.lly) y = (float)((double)g.lly + hh + kEps);
+    if ((double)y + hh > (double)g.ury) y = (float)((double)g.ury - hh - kEps);
+    return make_float2(x, y);
+}
+
 // fastExp, PlaceCommon/global.h:457-471 (float, ten squarings).  a / 1024 is
 // an exact power-of-two scaling, so the multiply rounds identically to the
 // reference's division.

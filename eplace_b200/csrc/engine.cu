@@ -75,6 +75,12 @@ struct ep_engine {
     std::mt19937_64 rng;
     float2 *snap = nullptr;   // ep_save_positions
     bool has_snap = false;
+    // quadratic placement (qp.cu): net -> first device pin / pins, pin -> net
+    std::vector<int32_t> h_net_first, h_net_deg, h_pin_net;
+    QpDev qp{};
+    bool qp_ready = false;
+    size_t qp_cap_x = 0, qp_cap_y = 0;
+    double *qp_out_h = nullptr;  // pinned mirror of qp.out
     int64_t launches = 0;     // engine kernels launched so far
     int64_t graph_kernels = 0;  // kernels in one replay of the step graph
 };
@@ -755,6 +761,16 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
             }
         }
     }
+    // quadratic placement: nets in device order
+    e->h_net_first.assign(nnet, 0);
+    e->h_net_deg.assign(nnet, 0);
+    e->h_pin_net.assign(np, 0);
+    for (int n = 0; n < nnet; n++) {
+        const int a = net_start[n], d = net_start[n + 1] - a;
+        e->h_net_deg[n] = d;
+        if (d > 0) e->h_net_first[n] = dev_of_pin[a];
+        for (int k = 0; k < d; k++) e->h_pin_net[dev_of_pin[a + k]] = n;
+    }
     // each object's pins (reference order) -> their device positions
     std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0);
     for (int p = 0; p < np; p++)
@@ -868,6 +884,7 @@ void ep_destroy(ep_engine *e) {
     dct_plan_free(e->dct);
     for (void *p : e->allocs) cudaFree(p);
     if (e->hS) cudaFreeHost(e->hS);
+    if (e->qp_out_h) cudaFreeHost(e->qp_out_h);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -1399,6 +1416,214 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
     CK(cudaMemcpyAsync(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice, e->st));
     if (!keep_maps) zero_maps();
     CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+}  // extern "C"
+
+// ---- quadratic placement ---------------------------------------------------------
+namespace {
+
+ep_status qp_setup(ep_engine *e) {
+    if (e->qp_ready) return EP_OK;
+    QpDev &q = e->qp;
+    const int nn = e->n_nodes, nnet = e->n_nets, np = e->n_pins;
+    q.nn = nn;
+    q.nnet = nnet;
+    q.obj_pin_start = e->obj_pin_start;
+    q.obj_pin_dev = e->obj_pin_dev;
+    q.owner = e->pin_owner;
+    q.off = e->pin_off;
+    int32_t *pin_net = nullptr, *net_first = nullptr, *net_deg = nullptr;
+    // at most 4 entries per pin and axis: every counted pair of a net involves
+    // one of its two bound pins (< 2 d pairs, two entries each)
+    const size_t cap = 4 * (size_t)np + 16;
+    const int pb = qp_partial_blocks(nn, nnet);
+    ep_status s;
+    if ((s = dupload(e, pin_net, e->h_pin_net)) || (s = dupload(e, net_first, e->h_net_first)) ||
+        (s = dupload(e, net_deg, e->h_net_deg)) || (s = dalloc(e, q.bound, std::max(nnet, 1))) ||
+        (s = dalloc(e, q.count, 2 * (size_t)nn)) || (s = dalloc(e, q.row_x, (size_t)nn + 1)) ||
+        (s = dalloc(e, q.row_y, (size_t)nn + 1)) || (s = dalloc(e, q.col_x, cap)) || (s = dalloc(e, q.col_y, cap)) ||
+        (s = dalloc(e, q.val_x, cap)) || (s = dalloc(e, q.val_y, cap)) || (s = dalloc(e, q.diag, nn)) ||
+        (s = dalloc(e, q.rhs, nn)) || (s = dalloc(e, q.x, nn)) || (s = dalloc(e, q.r, nn)) ||
+        (s = dalloc(e, q.r0, nn)) || (s = dalloc(e, q.p, nn)) || (s = dalloc(e, q.v, nn)) ||
+        (s = dalloc(e, q.s, nn)) || (s = dalloc(e, q.t, nn)) || (s = dalloc(e, q.partials, 4 * (size_t)pb)) ||
+        (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)))
+        return s;
+    q.pin_net = pin_net;
+    q.net_first = net_first;
+    q.net_deg = net_deg;
+    CK(cudaMemset(q.cnt, 0, sizeof(unsigned)));
+    CK(cudaMallocHost((void **)&e->qp_out_h, 4 * sizeof(double)));
+    e->qp_cap_x = e->qp_cap_y = cap;
+    e->qp_ready = true;
+    return EP_OK;
+}
+
+ep_status qp_read(ep_engine *e, int n) {
+    CK(cudaMemcpyAsync(e->qp_out_h, e->qp.out, n * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    CK(cudaGetLastError());
+    return EP_OK;
+}
+
+// Build both systems at the current centres: count, prefix sum, fill.
+ep_status qp_build(ep_engine *e) {
+    QpDev &q = e->qp;
+    const int nn = q.nn;
+    qp_rows(q, 0, e->pos, e->st);
+    std::vector<int32_t> cnt(2 * (size_t)nn), rx(nn + 1), ry(nn + 1);
+    CK(cudaMemcpyAsync(cnt.data(), q.count, cnt.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    rx[0] = ry[0] = 0;
+    for (int i = 0; i < nn; i++) {
+        rx[i + 1] = rx[i] + cnt[i];
+        ry[i + 1] = ry[i] + cnt[nn + i];
+    }
+    if ((size_t)rx[nn] > e->qp_cap_x || (size_t)ry[nn] > e->qp_cap_y) {
+        e->err = "quadratic placement: more matrix entries than the bound allows";
+        return EP_ERR_STATE;
+    }
+    CK(cudaMemcpyAsync(q.row_x, rx.data(), rx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(q.row_y, ry.data(), ry.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
+    qp_rows(q, 1, e->pos, e->st);
+    CK(cudaStreamSynchronize(e->st));  // the host vectors above go out of scope
+    CK(cudaGetLastError());
+    return EP_OK;
+}
+
+// BiCGSTAB as Eigen implements it (van der Vorst's method with a restart
+// when r0.r vanishes; identity preconditioner), both axes at once: stop when
+// |r|^2 <= (eps |b|)^2 with eps the float epsilon, or after max_it
+// iterations; the current centres are the initial guess.  err[c] = |r|/|b|
+// at the end, the value QPPlacer reads as solver.error().
+ep_status qp_solve(ep_engine *e, int max_it, double err[2], int &iters) {
+    QpDev &q = e->qp;
+    cudaStream_t st = e->st;
+    const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
+    qp_to_x(q, e->pos, st);
+    qp_init(q, st);
+    ep_status s = qp_read(e, 4);
+    if (s) return s;
+    double rr[2] = {e->qp_out_h[0], e->qp_out_h[1]}, bb[2] = {e->qp_out_h[2], e->qp_out_h[3]};
+    double r0sq[2] = {rr[0], rr[1]};
+    double rho[2] = {1, 1}, alpha[2] = {1, 1}, w[2] = {1, 1};
+    double r0r[2] = {rr[0], rr[1]};  // r0.r of the current residual (r0 = r at the start)
+    double tol2[2];
+    int it[2] = {0, 0}, restarts[2] = {0, 0};
+    bool active[2];
+    for (int c = 0; c < 2; c++) {
+        tol2[c] = eps2 * bb[c];
+        if (bb[c] == 0.0) {  // x = 0 (Eigen returns at once)
+            qp_zero_axis(q, c, st);
+            rr[c] = 0.0;
+            active[c] = false;
+        } else {
+            active[c] = rr[c] > tol2[c] && max_it > 0;
+        }
+    }
+    iters = 0;
+    while (active[0] || active[1]) {
+        double rho_old[2] = {rho[0], rho[1]};
+        int restart = 0;
+        for (int c = 0; c < 2; c++) {
+            if (!active[c]) continue;
+            rho[c] = r0r[c];
+            if (std::fabs(rho[c]) < eps2 * r0sq[c]) restart |= 1 << c;
+        }
+        if (restart) {
+            // r = b - A x, r0 = r, rho = r0sq = |r|^2
+            qp_restart(q, restart, st);
+            if ((s = qp_read(e, 2))) return s;
+            for (int c = 0; c < 2; c++)
+                if (restart & (1 << c)) {
+                    rho[c] = r0sq[c] = e->qp_out_h[c];
+                    if (restarts[c]++ == 0) it[c] = 0;
+                }
+        }
+        float2 fb = make_float2(0.f, 0.f), fw = make_float2(0.f, 0.f), fa = make_float2(0.f, 0.f);
+        double beta[2] = {0, 0};
+        for (int c = 0; c < 2; c++)
+            if (active[c]) beta[c] = (rho[c] / rho_old[c]) * (alpha[c] / w[c]);
+        fb = make_float2((float)beta[0], (float)beta[1]);
+        fw = make_float2(active[0] ? (float)w[0] : 0.f, active[1] ? (float)w[1] : 0.f);
+        qp_dir(q, fb, fw, st);  // p = r + beta (p - w v)
+        qp_av(q, st);           // v = A p, r0.v
+        if ((s = qp_read(e, 2))) return s;
+        for (int c = 0; c < 2; c++) alpha[c] = active[c] ? rho[c] / e->qp_out_h[c] : 0.0;
+        fa = make_float2((float)alpha[0], (float)alpha[1]);
+        qp_s(q, fa, st);  // s = r - alpha v
+        qp_at(q, st);     // t = A s, t.t, t.s
+        if ((s = qp_read(e, 4))) return s;
+        for (int c = 0; c < 2; c++) {
+            if (!active[c]) continue;
+            const double tt = e->qp_out_h[c], ts = e->qp_out_h[2 + c];
+            w[c] = tt > 0.0 ? ts / tt : 0.0;
+        }
+        fw = make_float2(active[0] ? (float)w[0] : 0.f, active[1] ? (float)w[1] : 0.f);
+        qp_step(q, fa, fw, st);  // x += alpha p + w s, r = s - w t, |r|^2, r0.r
+        if ((s = qp_read(e, 4))) return s;
+        iters++;
+        for (int c = 0; c < 2; c++) {
+            if (!active[c]) continue;
+            rr[c] = e->qp_out_h[c];
+            r0r[c] = e->qp_out_h[2 + c];
+            it[c]++;
+            active[c] = rr[c] > tol2[c] && it[c] < max_it;
+        }
+    }
+    for (int c = 0; c < 2; c++) err[c] = bb[c] > 0.0 ? std::sqrt(rr[c] / bb[c]) : 0.0;
+    return EP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
+    if (!e) return EP_ERR_ARG;
+    if (e->in_run) {
+        e->err = "ep_quadratic_placement cannot run inside an optimizer run";
+        return EP_ERR_STATE;
+    }
+    ep_status s = qp_setup(e);
+    if (s) return s;
+    QpDev &q = e->qp;
+    cudaStream_t st = e->st;
+    const int max_outer = max_iterations > 0 ? max_iterations : 20;  // IPiteCount, default 20
+    const double target_error = 0.000001;                           // qplace.cpp:47
+    CK(cudaEventRecord(e->ev0, st));
+    qp_center(q, e->grid, e->size, e->pos, st);  // moveNodesCenterToCenter
+    qp_bounds(q, e->pos, q.out, st);
+    if ((s = qp_read(e, 1))) return s;
+    double hpwl = e->qp_out_h[0], err[2] = {0, 0};
+    int outer = 0, solver_iters = 0;
+    for (int i = 0;; i++) {
+        if ((s = qp_build(e))) return s;
+        int it = 0;
+        if ((s = qp_solve(e, 100, err, it))) return s;  // solver.setMaxIterations(100)
+        solver_iters += it;
+        qp_from_x(q, e->grid, e->size, e->pos, st);  // updateModuleLocation
+        qp_bounds(q, e->pos, q.out, st);             // calcNetBoundPins
+        if ((s = qp_read(e, 1))) return s;
+        hpwl = e->qp_out_h[0];
+        outer = i + 1;
+        if (std::fabs(err[0]) < target_error && std::fabs(err[1]) < target_error && i > 4) break;
+        if (i >= max_outer) break;
+    }
+    CK(cudaEventRecord(e->ev1, st));
+    CK(cudaEventSynchronize(e->ev1));
+    e->initialized = false;  // the gradient state belongs to the old positions
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+        stats->rounds = outer;
+        stats->solver_iterations = solver_iters;
+        stats->hpwl = hpwl;
+        stats->error_x = err[0];
+        stats->error_y = err[1];
+        stats->seconds = ms * 1e-3;
+    }
     return EP_OK;
 }
 

@@ -159,4 +159,41 @@ void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, con
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
                  cudaStream_t st);
 
+// ---- quadratic placement (qp.cu) ---------------------------------------------
+// Device view of one engine's quadratic placement: the netlist in device pin
+// order (nets contiguous) plus the per-round systems and BiCGSTAB vectors,
+// both axes side by side in float2 (x for the X system, y for the Y system).
+struct QpDev {
+    int nn, nnet;
+    const int32_t *obj_pin_start, *obj_pin_dev;  // movable node -> its pins (modulePins order)
+    const int32_t *pin_net;                      // device pin -> net
+    const int32_t *net_first, *net_deg;          // net -> first device pin, pins
+    const int32_t *owner;
+    const float2 *off;
+    int4 *bound;                                 // per net: x-min, x-max, y-min, y-max pin (in net)
+    int32_t *count;                              // [2 nn] entries per row (X then Y)
+    int32_t *row_x, *row_y;                      // [nn + 1] CSR offsets
+    int32_t *col_x, *col_y;
+    float *val_x, *val_y;
+    float2 *diag, *rhs;
+    float2 *x, *r, *r0, *p, *v, *s, *t;
+    double *partials;
+    unsigned *cnt;
+    double *out;  // [4] sums of the last reduction
+};
+void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st);
+void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st);
+void qp_init(const QpDev &q, cudaStream_t st);
+void qp_dir(const QpDev &q, float2 beta, float2 w, cudaStream_t st);
+void qp_av(const QpDev &q, cudaStream_t st);
+void qp_s(const QpDev &q, float2 alpha, cudaStream_t st);
+void qp_at(const QpDev &q, cudaStream_t st);
+void qp_step(const QpDev &q, float2 alpha, float2 w, cudaStream_t st);
+void qp_restart(const QpDev &q, int mask, cudaStream_t st);
+void qp_zero_axis(const QpDev &q, int axis, cudaStream_t st);
+void qp_to_x(const QpDev &q, const float2 *pos, cudaStream_t st);
+void qp_from_x(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);
+void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);
+int qp_partial_blocks(int nn, int nnet);
+
 }  // namespace ep

@@ -723,17 +723,6 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
 }
 
 // ---------------------------------------------------------------- update --
-// PlaceDB::setModuleCenter_2D clamp (PlaceDB/placedb.cpp:257-281), double
-// compares and double sums stored to float, as the reference evaluates them.
-__device__ __forceinline__ float2 clamp_center(const Grid &g, float2 c, float2 s) {
-    double hw = 0.5 * (double)s.x, hh = 0.5 * (double)s.y;
-    float x = c.x, y = c.y;
-    if ((double)x - hw < (double)g.llx) x = (float)((double)g.llx + hw + kEps);
-    if ((double)x + hw > (double)g.urx) x = (float)((double)g.urx - hw - kEps);
-    if ((double)y - hh < (double)g.lly) y = (float)((double)g.lly + hh + kEps);
-    if ((double)y + hh > (double)g.ury) y = (float)((double)g.ury - hh - kEps);
-    return make_float2(x, y);
-}
 
 // x_{k+1} = y_k + s g_k, y_{k+1} = x_{k+1} + c (x_{k+1} - x_k)
 // (opt_step_vanilla, Optimization/nesterov.hpp:391-404); returns the clamped

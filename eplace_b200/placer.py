@@ -84,6 +84,11 @@ class RunStats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_int64)]
 
 
+class QpStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int32), ("solver_iterations", ctypes.c_int32), ("hpwl", ctypes.c_double),
+                ("error_x", ctypes.c_double), ("error_y", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
 MAX_TIMED = 12
 
 
@@ -100,7 +105,7 @@ EXPORTS = (
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
-    "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels",
+    "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement",
     "ep_density_scatter_noalloc",
 )
 
@@ -150,6 +155,7 @@ def load():
               "ep_nesterov_begin", "ep_nesterov_end", "ep_save_positions", "ep_load_positions"):
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
+    L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
         [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
@@ -305,6 +311,12 @@ class Engine:
         v = ctypes.c_double()
         self._check(self._L.ep_hpwl(self.h, ctypes.byref(v)))
         return v.value
+
+    def quadratic_placement(self, max_iterations=0):
+        """QPPlacer::quadraticPlacement on the device; returns its stats."""
+        st = QpStats()
+        self._check(self._L.ep_quadratic_placement(self.h, int(max_iterations), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
     def switch_stage(self, stage, filler_ll=None):
         a = None if filler_ll is None else np.ascontiguousarray(filler_ll, np.float32)

@@ -130,6 +130,15 @@ typedef struct ep_run_stats {
     int64_t kernel_launches; /* engine kernels launched by this run */
 } ep_run_stats;
 
+/* Result of ep_quadratic_placement. */
+typedef struct ep_qp_stats {
+    int32_t rounds;            /* outer rounds (matrix rebuilds) */
+    int32_t solver_iterations; /* BiCGSTAB iterations over all rounds */
+    double hpwl;               /* HPWL after the last round (calcNetBoundPins) */
+    double error_x, error_y;   /* |r| / |b| of the last solves (solver.error()) */
+    double seconds;            /* device time, CUDA events */
+} ep_qp_stats;
+
 /* Per-kernel device times of one evaluation + step (ep_time_kernels). */
 #define EP_MAX_TIMED_KERNELS 12
 typedef struct ep_kernel_times {
@@ -201,6 +210,18 @@ ep_status ep_hpwl(ep_engine *e, double *hpwl);
  * setModuleLocation_2D_random writes them) may be NULL: the engine then draws
  * its own seeded positions. */
 ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy);
+
+/* QPPlacer::quadraticPlacement (QPlace/qplace.cpp:20-106), the initial
+ * placement of the reference's flow, on the device: the movable nodes start
+ * at the core centre; each round builds the bound-pin quadratic model of
+ * QPPlacer::createSparseMatrix (qplace.cpp:125-272, weights
+ * 1/((p-1) max(d, 25)), the reference's Y pair test included) at the current
+ * centres and solves X and Y with BiCGSTAB (identity preconditioner, at most
+ * 100 iterations, warm start), then moves the nodes to the solution clamped
+ * into the core.  Rounds stop when both solver errors are below 1e-6 after
+ * the fifth, or after max_iterations + 1 rounds (0 = the reference's 20).
+ * Fillers are not moved.  ep_initialize must run again afterwards. */
+ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats);
 
 /* FirstOrderOptimizer::opt (Optimization/opt.hpp:30-36) with
  * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:

@@ -139,7 +139,9 @@ def record_variants():
         (Optimization/nesterov.hpp:310-369);
       * mixed-size stages: mGP, switch2FillerOnly (the reference re-draws the
         fillers with rand(); their new centres are recorded), 20 FILLERONLY
-        steps, switch2cGP and the cGP run (EPlace/eplace.cpp:887-904).
+        steps, switch2cGP and the cGP run (EPlace/eplace.cpp:887-904);
+      * quadratic placement (QPPlacer::quadraticPlacement,
+        QPlace/qplace.cpp:20-106): the node centres it produces.
     Written to variants.npz."""
     out = {}
     nl = synth.blob_start(synth.standard_cell(2000, seed=3))
@@ -175,6 +177,15 @@ def record_variants():
     for k in ("iterations", "overflow", "hpwl", "lam", "cx", "cy"):
         out["stage_cgp_" + k] = cg[k]
     ref.close()
+    # quadratic placement (QPPlacer::quadraticPlacement) from the netlist alone
+    for name, d in (("stdcell_2k", nl), ("mixed_5k", mx)):
+        ref = R.RefPlacer(d)
+        t = ref.qp()
+        cx, cy = ref.node_centers()
+        out[f"qp_{name}_cx"], out[f"qp_{name}_cy"] = cx, cy
+        out[f"qp_{name}_hpwl"] = np.float64(ref.hpwl())
+        out[f"qp_{name}_seconds"] = np.float64(t)
+        ref.close()
     path = os.path.join(HERE, "variants.npz")
     np.savez_compressed(path, **out)
     print("variants:", {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
