@@ -72,6 +72,7 @@ struct ep_engine {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_poll = nullptr;  // the run's read-back of `done` has landed
     std::mt19937_64 rng;
     float2 *snap = nullptr;   // ep_save_positions
     bool has_snap = false;
@@ -484,6 +485,7 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         CK(cudaStreamCreateWithPriority(&e->st_wl, cudaStreamNonBlocking, lo));
         CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_poll, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
     }
     e->rng.seed(P.filler_seed);
@@ -888,6 +890,7 @@ void ep_destroy(ep_engine *e) {
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_poll) cudaEventDestroy(e->ev_poll);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
     if (e->st_wl) cudaStreamDestroy(e->st_wl);
     if (e->own_stream && e->st) cudaStreamDestroy(e->st);
@@ -1219,46 +1222,71 @@ ep_status ep_nesterov_end(ep_engine *e) {
     return EP_OK;
 }
 
-ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) {
-    if (!e) return EP_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// One optimizer run split into phases, so that several engines' runs can be
+// interleaved (ep_run_batch): start, then launch / check until the stop,
+// then finish.
+struct RunState {
+    int K = 8;
+    bool bktrk = false;
+    int64_t launches0 = 0;
+    int cap = 0, launched = 0;
+};
+
+ep_status run_start(ep_engine *e, int32_t max_steps, RunState &r) {
     ep_status s = ep_nesterov_begin(e);
     if (s) return s;
     s = update_scalars(e, [max_steps](DevScalars &h) { h.step_cap = max_steps > 0 ? max_steps : 0; });
     if (s) return s;
-    const int K = 8;
-    const bool bktrk = e->prm.step_rule == EP_STEP_BKTRK;
-    if (!bktrk && (!e->graph || e->graph_iters != K)) {
-        s = build_graph(e, K);
+    r.bktrk = e->prm.step_rule == EP_STEP_BKTRK;
+    if (!r.bktrk && (!e->graph || e->graph_iters != r.K)) {
+        s = build_graph(e, r.K);
         if (s) return s;
     }
-    const int64_t launches0 = e->launches - 1;  // include the stage-begin kernel
+    r.launches0 = e->launches - 1;  // include the stage-begin kernel
     CK(cudaEventRecord(e->ev0, e->st));
-    const int cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + K;
-    int launched = 0;
-    if (bktrk) {
-        // host-driven steps: the number of trials per step is data-dependent
-        s = fetch_scalars(e);
-        if (s) return s;
-        while (!e->hS->done && launched <= cap) {
-            s = bktrk_step(e);
-            if (s) return s;
-            launched++;
-        }
-    }
-    if (!bktrk && fused_loop(e)) {
+    r.cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + r.K;
+    r.launched = 0;
+    if (!r.bktrk && fused_loop(e)) {
         // the first step's maps (the graph's steps start at prep)
         launch_scatter(e->kc, e->dn, e->node_q, e->filler_q, e->S, e->st);
         e->launches += 1;
     }
-    while (!bktrk) {
-        CK(cudaGraphLaunch(e->graph, e->st));
-        e->launches += e->graph_kernels;
-        launched += K;
-        CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
-        CK(cudaStreamSynchronize(e->st));
-        if (e->hS->done || launched > cap + K) break;
+    return EP_OK;
+}
+
+// Enqueue the next K steps (one graph replay) and the read-back of `done`;
+// backtracking steps run one at a time from the host.
+ep_status run_launch(ep_engine *e, RunState &r) {
+    if (r.bktrk) {
+        ep_status s = fetch_scalars(e);
+        if (s || e->hS->done) return s;
+        r.launched++;
+        return bktrk_step(e);
     }
-    if (!bktrk && fused_loop(e)) {
+    CK(cudaGraphLaunch(e->graph, e->st));
+    e->launches += e->graph_kernels;
+    r.launched += r.K;
+    CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
+    CK(cudaEventRecord(e->ev_poll, e->st));
+    return EP_OK;
+}
+
+ep_status run_check(ep_engine *e, RunState &r, bool &more) {
+    if (r.bktrk) {
+        more = !e->hS->done && r.launched <= r.cap;
+        return EP_OK;
+    }
+    CK(cudaEventSynchronize(e->ev_poll));
+    more = !(e->hS->done || r.launched > r.cap + r.K);
+    return EP_OK;
+}
+
+ep_status run_finish(ep_engine *e, RunState &r, ep_run_stats *stats) {
+    if (!r.bktrk && fused_loop(e)) {
         // clear in any case: the maps must be empty when the next evaluation
         // scatters (the stopping step scatters nothing, so this is a no-op
         // unless the loop was cut off)
@@ -1272,7 +1300,7 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
     CK(cudaEventRecord(e->ev1, e->st));
     enqueue_hpwl(e, 0);
     CK(cudaGetLastError());
-    s = fetch_scalars(e);
+    ep_status s = fetch_scalars(e);
     e->in_run = false;
     if (s) return s;
     if (stats) {
@@ -1283,9 +1311,73 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
         stats->hpwl = e->hS->hpwl_query;
         stats->lambda = e->hS->lambda;
         stats->seconds = ms * 1e-3;
-        stats->kernel_launches = e->launches - launches0;
+        stats->kernel_launches = e->launches - r.launches0;
     }
     return device_status(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) {
+    if (!e) return EP_ERR_ARG;
+    RunState r;
+    ep_status s = run_start(e, max_steps, r);
+    if (s) return s;
+    for (bool more = true; more;) {
+        if ((s = run_launch(e, r)) || (s = run_check(e, r, more))) {
+            e->in_run = false;
+            return s;
+        }
+    }
+    return run_finish(e, r, stats);
+}
+
+ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep_run_stats *stats) {
+    if (!engines || count < 0) return EP_ERR_ARG;
+    for (int i = 0; i < count; i++)
+        if (!engines[i]) return EP_ERR_ARG;
+    std::vector<RunState> rs(count);
+    std::vector<char> active(count, 0);
+    ep_status first_error = EP_OK;
+    auto stop_all = [&]() {
+        for (int i = 0; i < count; i++) engines[i]->in_run = false;
+    };
+    for (int i = 0; i < count; i++) {
+        ep_status s = run_start(engines[i], max_steps, rs[i]);
+        if (s) {
+            stop_all();
+            return s;
+        }
+        active[i] = 1;
+    }
+    for (int left = count; left > 0;) {
+        for (int i = 0; i < count; i++)
+            if (active[i]) {
+                ep_status s = run_launch(engines[i], rs[i]);
+                if (s) {
+                    stop_all();
+                    return s;
+                }
+            }
+        for (int i = 0; i < count; i++) {
+            if (!active[i]) continue;
+            bool more = true;
+            ep_status s = run_check(engines[i], rs[i], more);
+            if (s) {
+                stop_all();
+                return s;
+            }
+            if (!more) {
+                s = run_finish(engines[i], rs[i], stats ? &stats[i] : nullptr);
+                if (s && !first_error) first_error = s;
+                active[i] = 0;
+                left--;
+            }
+        }
+    }
+    return first_error;
 }
 
 ep_status ep_save_positions(ep_engine *e) {

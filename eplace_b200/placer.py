@@ -105,7 +105,7 @@ EXPORTS = (
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
-    "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement",
+    "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
     "ep_density_scatter_noalloc",
 )
 
@@ -156,6 +156,7 @@ def load():
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
+    L.ep_run_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(RunStats)]
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
         [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
@@ -169,6 +170,19 @@ def load():
     L.ep_nesterov_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     _lib = L
     return L
+
+
+def run_batch(engines, max_steps=0):
+    """ep_run_batch: the optimizer loops of several engines at once (each
+    engine initialized first); returns one run-stats dict per engine."""
+    L = load()
+    n = len(engines)
+    arr = (ctypes.c_void_p * n)(*[e.h.value for e in engines])
+    st = (RunStats * n)()
+    rc = L.ep_run_batch(arr, n, int(max_steps), st)
+    if rc:
+        raise EPError(rc, f"ep_run_batch: {STATUS_NAMES[rc]}")
+    return [{k: getattr(s, k) for k, _ in RunStats._fields_} for s in st]
 
 
 def default_params(**kw):

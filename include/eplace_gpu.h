@@ -233,6 +233,14 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
  * no acceptable trial within 64 tries ends the run with EP_ERR_TIMEOUT (the
  * reference retries without limit). */
 ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats);
+/* ep_nesterov_run for several independent engines (designs) at once, no
+ * counterpart in the reference (which places one design per process): each
+ * engine's loop runs on its own stream and the host interleaves their graph
+ * replays, so small designs fill the GPU together.  Each engine ends as
+ * ep_nesterov_run would leave it; stats (may be NULL) gets one entry per
+ * engine.  Returns the first error met (the others still finish). */
+ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep_run_stats *stats);
+
 /* The same loop one call at a time: begin = init(), step = "if
  * (!stop_condition()) opt_step(); updatePenaltyFactor()", end = wrap_up().
  * *stopped is set when the stop condition held and no step was taken. */

@@ -200,3 +200,26 @@ def test_nan_position_reported_and_engine_recovers():
     e.initialize()
     st = e.nesterov_run()
     assert st["overflow"] < 0.1
+
+
+def test_run_batch_matches_single_runs():
+    """ep_run_batch interleaves several engines' loops on their own streams;
+    each ends exactly as its own ep_nesterov_run would (different designs,
+    options and stop conditions in one batch)."""
+    cases = [("stdcell_2k", {}), ("mixed_5k", {}), ("stdcell_2k", {"step_rule": placer.STEP_BB}),
+             ("ref_smoke", {})]
+    solo, batch = [], []
+    for target in (solo, batch):
+        for name, kw in cases:
+            g = load_golden(name)
+            p = placer.default_params(target_density=float(g["target_density"]), **kw)
+            e = placer.Engine(golden_netlist(g), p)
+            e.set_positions(np.stack([g["init_cx"], g["init_cy"]], 1))
+            e.initialize()
+            target.append(e)
+    single = [e.nesterov_run() for e in solo]
+    many = placer.run_batch(batch)
+    for a, b, ea, eb in zip(single, many, solo, batch):
+        assert a["iterations"] == b["iterations"]
+        assert a["hpwl"] == b["hpwl"]
+        assert np.array_equal(ea.get_positions(), eb.get_positions())
