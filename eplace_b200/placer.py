@@ -106,6 +106,7 @@ EXPORTS = (
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
+    "ep_netbin_write", "ep_netbin_open", "ep_netbin_close",
     "ep_density_scatter_noalloc",
 )
 
@@ -157,6 +158,11 @@ def load():
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_run_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(RunStats)]
+    L.ep_netbin_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.c_float, ctypes.c_int32]
+    L.ep_netbin_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_float),
+                                 ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(vp)]
+    L.ep_netbin_close.argtypes = [vp]
+    L.ep_netbin_close.restype = None
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
         [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
@@ -170,6 +176,65 @@ def load():
     L.ep_nesterov_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     _lib = L
     return L
+
+
+def netlist_struct(nl):
+    """ep_netlist view of a synth.Netlist; returns (struct, arrays it points
+    into), the arrays kept alive by the caller."""
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    k = dict(
+        node_w=f(nl.node_w), node_h=f(nl.node_h), node_cx=f(nl.node_cx), node_cy=f(nl.node_cy),
+        term_llx=f(nl.term_llx), term_lly=f(nl.term_lly), term_w=f(nl.term_w), term_h=f(nl.term_h),
+        term_ni=np.ascontiguousarray(nl.term_is_ni, dtype=np.uint8),
+        net_start=np.ascontiguousarray(nl.net_start, dtype=np.int32),
+        pin_owner=np.ascontiguousarray(nl.pin_owner, dtype=np.int32),
+        pin_dx=f(nl.pin_dx), pin_dy=f(nl.pin_dy), row_llx=f(nl.row_llx), row_lly=f(nl.row_lly),
+        row_urx=f(nl.row_urx), row_h=f(nl.row_h))
+    c = Netlist(nl.num_nodes, nl.num_terminals, nl.num_nets, nl.num_rows,
+                _p(k["node_w"], _f32p), _p(k["node_h"], _f32p), _p(k["node_cx"], _f32p),
+                _p(k["node_cy"], _f32p), _p(k["term_llx"], _f32p), _p(k["term_lly"], _f32p),
+                _p(k["term_w"], _f32p), _p(k["term_h"], _f32p), _p(k["term_ni"], _u8p),
+                _p(k["net_start"], _i32p), _p(k["pin_owner"], _i32p), _p(k["pin_dx"], _f32p),
+                _p(k["pin_dy"], _f32p), _p(k["row_llx"], _f32p), _p(k["row_lly"], _f32p),
+                _p(k["row_urx"], _f32p), _p(k["row_h"], _f32p), 0.0)
+    return c, k
+
+
+def netbin_write(nl, path):
+    """ep_netbin_write: the netlist as the engine's binary netlist file."""
+    c, keep = netlist_struct(nl)
+    rc = load().ep_netbin_write(str(path).encode(), ctypes.byref(c), float(nl.target_density), int(nl.bins))
+    if rc:
+        raise EPError(rc, f"ep_netbin_write({path}): {STATUS_NAMES[rc]}")
+    return path
+
+
+def netbin_read(path):
+    """ep_netbin_open: map a binary netlist file; returns a synth.Netlist
+    holding copies of its arrays (row site widths are not part of
+    ep_netlist and come back as 1)."""
+    from .synth import Netlist as SynthNetlist
+    L = load()
+    c, td, bins, h = Netlist(), ctypes.c_float(), ctypes.c_int32(), ctypes.c_void_p()
+    rc = L.ep_netbin_open(str(path).encode(), ctypes.byref(c), ctypes.byref(td), ctypes.byref(bins),
+                          ctypes.byref(h))
+    if rc:
+        raise EPError(rc, f"ep_netbin_open({path}): {STATUS_NAMES[rc]}")
+    try:
+        nn, nt, nnet, nr = c.num_nodes, c.num_terminals, c.num_nets, c.num_rows
+        a = lambda ptr, n: np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.float32)
+        np_ = int(np.ctypeslib.as_array(c.net_start, shape=(nnet + 1,))[nnet])
+        return SynthNetlist(
+            name=str(path).rsplit("/", 1)[-1].split(".")[0],
+            node_w=a(c.node_w, nn), node_h=a(c.node_h, nn), node_cx=a(c.node_cx, nn), node_cy=a(c.node_cy, nn),
+            term_llx=a(c.term_llx, nt), term_lly=a(c.term_lly, nt), term_w=a(c.term_w, nt),
+            term_h=a(c.term_h, nt), term_is_ni=a(c.term_is_ni, nt).astype(np.uint8),
+            net_start=a(c.net_start, nnet + 1), pin_owner=a(c.pin_owner, np_), pin_dx=a(c.pin_dx, np_),
+            pin_dy=a(c.pin_dy, np_), row_llx=a(c.row_llx, nr), row_lly=a(c.row_lly, nr),
+            row_urx=a(c.row_urx, nr), row_h=a(c.row_h, nr), row_site_w=np.ones(nr, np.float32),
+            target_density=td.value, bins=bins.value)
+    finally:
+        L.ep_netbin_close(h)
 
 
 def run_batch(engines, max_steps=0):
@@ -209,22 +274,7 @@ class Engine:
         for k, v in kw.items():
             setattr(params, k, v)
         self.params = params
-        f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
-        self._keep = k = dict(
-            node_w=f(nl.node_w), node_h=f(nl.node_h), node_cx=f(nl.node_cx), node_cy=f(nl.node_cy),
-            term_llx=f(nl.term_llx), term_lly=f(nl.term_lly), term_w=f(nl.term_w), term_h=f(nl.term_h),
-            term_ni=np.ascontiguousarray(nl.term_is_ni, dtype=np.uint8),
-            net_start=np.ascontiguousarray(nl.net_start, dtype=np.int32),
-            pin_owner=np.ascontiguousarray(nl.pin_owner, dtype=np.int32),
-            pin_dx=f(nl.pin_dx), pin_dy=f(nl.pin_dy), row_llx=f(nl.row_llx), row_lly=f(nl.row_lly),
-            row_urx=f(nl.row_urx), row_h=f(nl.row_h))
-        c = Netlist(nl.num_nodes, nl.num_terminals, nl.num_nets, nl.num_rows,
-                    _p(k["node_w"], _f32p), _p(k["node_h"], _f32p), _p(k["node_cx"], _f32p),
-                    _p(k["node_cy"], _f32p), _p(k["term_llx"], _f32p), _p(k["term_lly"], _f32p),
-                    _p(k["term_w"], _f32p), _p(k["term_h"], _f32p), _p(k["term_ni"], _u8p),
-                    _p(k["net_start"], _i32p), _p(k["pin_owner"], _i32p), _p(k["pin_dx"], _f32p),
-                    _p(k["pin_dy"], _f32p), _p(k["row_llx"], _f32p), _p(k["row_lly"], _f32p),
-                    _p(k["row_urx"], _f32p), _p(k["row_h"], _f32p), 0.0)
+        c, self._keep = netlist_struct(nl)
         h = ctypes.c_void_p()
         rc = L.ep_create(ctypes.byref(c), ctypes.byref(params), ctypes.byref(h))
         self.h = h

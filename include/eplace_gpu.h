@@ -233,6 +233,17 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
  * no acceptable trial within 64 tries ends the run with EP_ERR_TIMEOUT (the
  * reference retries without limit). */
 ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats);
+/* Binary netlist file, no counterpart in the reference (whose Bookshelf
+ * parser, Parser/parser.cpp:44-819, is its slow I/O step): the arrays of
+ * ep_netlist as they lie in memory (layout in eplace_b200/csrc/netbin.cu).
+ * ep_netbin_write stores a netlist; ep_netbin_open maps a file and points
+ * *nl at its arrays without copying (valid until ep_netbin_close(handle));
+ * target_density and bins (may be NULL) receive the stored values. */
+ep_status ep_netbin_write(const char *path, const ep_netlist *nl, float target_density, int32_t bins);
+ep_status ep_netbin_open(const char *path, ep_netlist *nl, float *target_density, int32_t *bins,
+                         void **handle);
+void ep_netbin_close(void *handle);
+
 /* ep_nesterov_run for several independent engines (designs) at once, no
  * counterpart in the reference (which places one design per process): each
  * engine's loop runs on its own stream and the host interleaves their graph
