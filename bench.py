@@ -234,16 +234,9 @@ def main():
 
     from eplace_b200 import placer
     nl = design()
-    dct_mode = {"fp32": placer.DCT_FP32, "bf16x3": placer.DCT_BF16X3}.get(args.dct)
-    if dct_mode is None:
-        dct_mode = placer.DCT_BF16X3
-    try:
-        eng = placer.Engine(nl, placer.default_params(target_density=1.0, dct_mode=dct_mode, device=local))
-    except placer.EPError as ex:
-        if args.dct != "auto" or ex.status != placer.EP_ERR_UNSUPPORTED:
-            raise
-        dct_mode = placer.DCT_FP32
-        eng = placer.Engine(nl, placer.default_params(target_density=1.0, dct_mode=dct_mode, device=local))
+    dct_mode = {"fp32": placer.DCT_FP32, "bf16x3": placer.DCT_BF16X3}.get(args.dct, placer.DCT_AUTO)
+    eng = placer.Engine(nl, placer.default_params(target_density=1.0, dct_mode=dct_mode, device=local))
+    dct_mode = eng.info.dct_mode
     stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
     eng.save_positions()

@@ -446,7 +446,7 @@ void ep_default_params(ep_params *p) {
     p->wl_model = EP_WL_WA;
     p->exp_mode = EP_EXP_FAST;
     p->step_rule = EP_STEP_LIPSCHITZ;
-    p->dct_mode = EP_DCT_FP32;
+    p->dct_mode = EP_DCT_AUTO;
     p->filler_seed = 1;
 }
 
@@ -465,7 +465,7 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         e->err = "target_density must be in (0, 1]";
         return EP_ERR_ARG;
     }
-    if (P.dct_mode != EP_DCT_FP32 && P.dct_mode != EP_DCT_BF16X3) {
+    if (P.dct_mode != EP_DCT_FP32 && P.dct_mode != EP_DCT_BF16X3 && P.dct_mode != EP_DCT_AUTO) {
         e->err = "unknown dct_mode";
         return EP_ERR_ARG;
     }
@@ -871,7 +871,14 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         (s = dalloc(e, kc.part_hp, (size_t)2 * std::max(1, reduction_blocks(d, 0)))))
         return s;
 
-    int rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, P.dct_mode, e->err);
+    int rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy,
+                           P.dct_mode == EP_DCT_AUTO ? EP_DCT_BF16X3 : P.dct_mode, e->err);
+    if (rc == EP_ERR_UNSUPPORTED && P.dct_mode == EP_DCT_AUTO) {
+        // the tensor-core solve does not take this grid: the FP32 one does
+        dct_plan_free(e->dct);
+        e->err.clear();
+        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, EP_DCT_FP32, e->err);
+    }
     if (rc) return (ep_status)rc;
     e->stage = EP_STAGE_MGP;
     s = upload_view(e, EP_STAGE_MGP);
@@ -921,6 +928,7 @@ ep_status ep_get_info(const ep_engine *e, ep_info *info) {
     info->macro_area = e->macro_area;
     info->total_row_area = e->total_row_area;
     info->density_scale = e->kc.qscale;
+    info->dct_mode = e->dct.mode;
     return EP_OK;
 }
 

@@ -22,7 +22,7 @@ MGP, FILLERONLY, CGP = 0, 1, 2
 WL_WA, WL_LSE = 0, 1
 EXP_FAST, EXP_EXACT = 0, 1
 STEP_LIPSCHITZ, STEP_BB, STEP_BKTRK = 0, 1, 2
-DCT_FP32, DCT_BF16X3 = 0, 1
+DCT_FP32, DCT_BF16X3, DCT_AUTO = 0, 1, 2
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -75,7 +75,8 @@ class Info(ctypes.Structure):
                 ("core_urx", ctypes.c_float), ("core_ury", ctypes.c_float),
                 ("filler_w", ctypes.c_float), ("filler_h", ctypes.c_float),
                 ("std_area", ctypes.c_double), ("macro_area", ctypes.c_double),
-                ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double)]
+                ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double),
+                ("dct_mode", ctypes.c_int32)]
 
 
 class RunStats(ctypes.Structure):

@@ -51,8 +51,11 @@ typedef enum ep_step_rule { EP_STEP_LIPSCHITZ = 0, EP_STEP_BB = 1, EP_STEP_BKTRK
 
 /* Arithmetic of the DCT/IDCT Poisson solve (replaces FFT_2D::doFFT,
  * FFT/fft.cpp:191-284): dense GEMMs in FP32 on the CUDA cores, or on the
- * tcgen05 tensor cores with 3xBF16 split products (FP32 accumulate). */
-typedef enum ep_dct_mode { EP_DCT_FP32 = 0, EP_DCT_BF16X3 = 1 } ep_dct_mode;
+ * tcgen05 tensor cores with 3xBF16 split products (FP32 accumulate; bin
+ * counts must be multiples of 128).  EP_DCT_AUTO (the default) takes the
+ * tensor cores when the bin grid allows, else FP32; ep_info.dct_mode tells
+ * which. */
+typedef enum ep_dct_mode { EP_DCT_FP32 = 0, EP_DCT_BF16X3 = 1, EP_DCT_AUTO = 2 } ep_dct_mode;
 
 /* Netlist in plain arrays (what Parser/parser.cpp:44-97 builds into PlaceDB).
  * Nodes are movable; a node is a macro iff its height exceeds
@@ -119,6 +122,7 @@ typedef struct ep_info {
     double std_area, macro_area;  /* ePlaceStdCellArea / ePlaceMacroArea */
     double total_row_area;
     double density_scale;         /* fixed-point units per unit area of the bin maps */
+    int32_t dct_mode;             /* ep_dct_mode in use (never EP_DCT_AUTO) */
 } ep_info;
 
 typedef struct ep_run_stats {

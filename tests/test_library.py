@@ -33,7 +33,7 @@ def test_abi_version_and_defaults():
     assert p.target_density == pytest.approx(1.0)
     assert p.target_overflow == pytest.approx(0.10)
     assert p.max_iterations == 1000
-    assert p.dct_mode == placer.DCT_FP32 and p.exp_mode == placer.EXP_FAST
+    assert p.dct_mode == placer.DCT_AUTO and p.exp_mode == placer.EXP_FAST
 
 
 def _bad_netlist(mutate):
