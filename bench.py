@@ -215,7 +215,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--dct", default="auto", choices=["auto", "fp32", "bf16x3"])
+    ap.add_argument("--dct", default="auto", choices=["auto", "fp32", "bf16x3", "fft"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -234,7 +234,7 @@ def main():
 
     from eplace_b200 import placer
     nl = design()
-    dct_mode = {"fp32": placer.DCT_FP32, "bf16x3": placer.DCT_BF16X3}.get(args.dct, placer.DCT_AUTO)
+    dct_mode = {"fp32": placer.DCT_FP32, "bf16x3": placer.DCT_BF16X3, "fft": placer.DCT_FFT}.get(args.dct, placer.DCT_AUTO)
     eng = placer.Engine(nl, placer.default_params(target_density=1.0, dct_mode=dct_mode, device=local))
     dct_mode = eng.info.dct_mode
     stream = torch.cuda.current_stream()
@@ -303,7 +303,8 @@ def main():
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": workload_config(nl, dict(
                    fillers=eng.info.num_fillers, parallelism=f"replicas x{world}" if world > 1 else "1 GPU",
-                   dct="3xBF16 tcgen05 GEMMs, FP32 accumulate" if dct_mode == placer.DCT_BF16X3 else "FP32 CUDA-core GEMMs",
+                   dct={placer.DCT_BF16X3: "3xBF16 tcgen05 GEMMs, FP32 accumulate",
+                        placer.DCT_FFT: "FP32 fast transforms (shared-memory FFTs)"}.get(dct_mode, "FP32 CUDA-core GEMMs"),
                    density="int64 fixed-point scatter", reductions="FP64")),
                "iterations": last["iterations"], "overflow": last["overflow"], "hpwl": last["hpwl"],
                "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": 8 * n_obj,

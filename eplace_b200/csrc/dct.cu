@@ -19,7 +19,8 @@
 //       E_y[x][y] = sum_u A4y[x][u] Vt[y][u],  A4y[x][u] = C_nx[u][x]
 //       (phi, when asked: A4y against Ut)          (interleaved float2 field)
 // This file holds the tables and the FP32 CUDA-core GEMM; dct_tc.cu runs the
-// same four GEMMs on the tcgen05 tensor cores.
+// same four GEMMs on the tcgen05 tensor cores, dct_fft.cu evaluates the same
+// sums by fast transforms.
 #include <cmath>
 #include <vector>
 
@@ -30,6 +31,9 @@ namespace ep {
 int dct_tc_init(DctPlan &p, std::string &err);
 void dct_tc_free(DctPlan &p);
 int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaStream_t st);
+int dct_fft_init(DctPlan &p, const std::vector<double> &wx, const std::vector<double> &wy, std::string &err);
+void dct_fft_free(DctPlan &p);
+int dct_fft_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S, cudaStream_t st);
 
 namespace {
 
@@ -117,6 +121,16 @@ void sgemm(int M, int N, int K, int batch, const GemmArgs &a, const DevScalars *
     launch_k(k_sgemm_nt<EPI>, grid, 256, 0, st, M, N, K, a, S);
 }
 
+}  // namespace
+
+void set_sgemm_carveout(int carveout) {
+    for (const void *f : {(const void *)k_sgemm_nt<kEpiT>, (const void *)k_sgemm_nt<kEpiSpectral>,
+                          (const void *)k_sgemm_nt<kEpiField>})
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
+}
+
+namespace {
+
 template <typename T>
 int upload(T *&dst, const std::vector<T> &src, std::string &err) {
     if (cudaMalloc(&dst, src.size() * sizeof(T)) != cudaSuccess) {
@@ -135,11 +149,12 @@ int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mo
     p.ny = ny;
     p.mode = mode;
     const double pi = 3.14159265358979323846;
-    std::vector<float> Cy((size_t)ny * ny), Cx((size_t)nx * nx), K((size_t)nx * ny),
-        B3((size_t)2 * ny * ny), A4((size_t)2 * nx * nx);
     std::vector<double> wx(nx), wy(ny);
     for (int u = 0; u < nx; u++) wx[u] = pi * u / nx;
     for (int v = 0; v < ny; v++) wy[v] = pi * v / ny * ((double)step_y / (double)step_x);
+    if (mode == EP_DCT_FFT) return dct_fft_init(p, wx, wy, err);
+    std::vector<float> Cy((size_t)ny * ny), Cx((size_t)nx * nx), K((size_t)nx * ny),
+        B3((size_t)2 * ny * ny), A4((size_t)2 * nx * nx);
     for (int v = 0; v < ny; v++)
         for (int y = 0; y < ny; y++) {
             double ang = pi * v * (y + 0.5) / ny;
@@ -176,6 +191,7 @@ int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mo
 
 void dct_plan_free(DctPlan &p) {
     if (p.tc) dct_tc_free(p);
+    if (p.fft) dct_fft_free(p);
     for (float *q : {p.Cy, p.Cx, p.K, p.B3, p.A4, p.Tt, p.P, p.T3})
         if (q) cudaFree(q);
     p = DctPlan();
@@ -184,6 +200,7 @@ void dct_plan_free(DctPlan &p) {
 int dct_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S,
             cudaStream_t st) {
     if (p.mode == EP_DCT_BF16X3) return dct_tc_run(p, field, phi, S, st);
+    if (p.mode == EP_DCT_FFT) return dct_fft_run(p, rho, field, phi, S, st);
     const int nx = p.nx, ny = p.ny;
     GemmArgs a{};
     // G1: Tt = (rho Cy^T)^T

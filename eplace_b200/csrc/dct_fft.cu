@@ -1,0 +1,529 @@
+// dct_fft.cu -- the electrostatic Poisson solve of FFT_2D::doFFT
+// (FFT/fft.cpp:191-284) by fast transforms: the same sums as dct.cu,
+//   a   = C_nx rho C_ny^T,   P = a .* K,
+//   E_x = S_nx^T diag(wx) P C_ny,   E_y = C_nx^T P diag(wy) S_ny,   phi = C_nx^T P C_ny,
+// evaluated as 1-D transforms along one axis at a time, each a length-n
+// complex FFT in shared memory (n a power of two), O(n^2 log n) per map
+// instead of the GEMMs' O(n^3).
+//
+// The 1-D transforms (C_n[k][j] = cos(pi k (j+1/2) / n)):
+//   DCT-II  X = C_n x     by Makhoul's permutation v = (x0, x2, .., x3, x1),
+//                         V = FFT(v), X[k] = Re(V[k] e^{-i pi k / 2n});
+//   DCT-III y = C_n^T X   by the inverse of that: Z[k] = (X~[k] - i X[n-k])
+//                         e^{i pi k / 2n} / 2 (X~[0] = 2 X[0], X[n] = 0),
+//                         z = IFFT(Z) (unnormalised), y[2j] = z[j],
+//                         y[2j+1] = z[n-1-j] (z is real: Z is Hermitian);
+//   sine    y = S_n^T X   = (-1)^j C_n^T b with b[0] = 0, b[k] = X[n-k]
+//                         (sin(pi (n-k)(j+1/2)/n) = (-1)^j cos(pi k (j+1/2)/n)).
+// Two real sequences share one complex FFT (one in the real, one in the
+// imaginary part) wherever the inputs or outputs are real.
+//
+// Three kernels, maps x-major [nx][ny] as everywhere in the engine:
+//   k_fft_rows_fwd  T[x][v]  = DCT-II of rho[x][:] along y          (2 rows per FFT)
+//   k_fft_cols      per column v of T: DCT-II along x, times K, then
+//                   X1[:][v] = S^T diag(wx) P[:][v] and X2[:][v] = C^T P[:][v]
+//                   (4 columns per block; X1 of two columns share one complex
+//                   IFFT and X2 of two columns another: P is dominated by its
+//                   low frequencies, so an FFT carrying P beside wx P would
+//                   round the small E inputs relative to |P|)
+//   k_fft_rows_inv  per row x: E_x = C^T X1[x][:], E_y = S^T diag(wy) X2[x][:]
+//                   (one complex IFFT), phi = C^T X2[x][:] when asked
+// Twiddles, the e^{i pi k / 2n} factors and the frequency weights come from
+// tables computed in double on the host, staged in shared memory by every
+// block before it waits on the previous grid.  The kernels are instantiated
+// per log2 n so that every loop has a fixed trip count and a thread issues
+// all its loads before it uses any.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <utility>
+#include <vector>
+
+#include "engine.h"
+
+namespace ep {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCols = 4;  // columns per block of k_fft_cols
+
+struct FftPlan {
+    int lognx = 0, logny = 0;
+    // twiddles, stage-major: stage s (half-size h = 2^s) holds e^{-i pi j / h},
+    // j < h, at [h - 1 + j]; n - 1 entries per axis
+    float2 *twx = nullptr, *twy = nullptr;
+    // (cos, sin)(pi k / 2n), k <= n/2
+    float2 *qx = nullptr, *qy = nullptr;
+    float *wx = nullptr, *wy = nullptr;
+    float kscale = 0.f;  // 4 / (nx ny)
+    float *T = nullptr;  // [nx][ny] after the first pass
+    float *X = nullptr;  // X1, X2: [2][nx][ny]
+    size_t smem_rows_fwd = 0, smem_cols = 0, smem_rows_inv = 0;
+    int pairs_fwd = 1, rows_inv = 1;
+};
+
+__device__ __forceinline__ int makhoul(int j, int n) { return (j & 1) ? n - 1 - (j >> 1) : (j >> 1); }
+
+__device__ __forceinline__ int brev(int i, int logn) { return (int)(__brev((unsigned)i) >> (32 - logn)); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// In-place radix-2 decimation-in-time FFT of nseq (<= NSEQ) length-2^LOGN
+// sequences stored back to back in shared memory, input in bit-reversed
+// order, output in natural order.  tw: the stage-major twiddles, in shared
+// memory.  INV uses e^{+...} (unnormalised inverse).  Ends with a block
+// barrier.
+template <bool INV, int LOGN, int NSEQ>
+__device__ __forceinline__ void block_fft(float2 *buf, int nseq, const float2 *tw) {
+    constexpr int half = 1 << (LOGN - 1);
+    constexpr int iters = (NSEQ * half + kThreads - 1) / kThreads;
+    const int total = nseq * half;
+#pragma unroll
+    for (int s = 0; s < LOGN; s++) {
+        const int h = 1 << s;
+#pragma unroll
+        for (int it = 0; it < iters; it++) {
+            const int j = threadIdx.x + it * kThreads;
+            if (j >= total) break;
+            const int q = j >> (LOGN - 1), b = j & (half - 1);
+            const int pos = b & (h - 1);
+            const int i0 = (q << LOGN) + ((b >> s) << (s + 1)) + pos;
+            float2 w = tw[h - 1 + pos];
+            if (INV) w.y = -w.y;
+            const float2 a = buf[i0];
+            const float2 t = cmul(buf[i0 + h], w);
+            buf[i0] = make_float2(a.x + t.x, a.y + t.y);
+            buf[i0 + h] = make_float2(a.x - t.x, a.y - t.y);
+        }
+        __syncthreads();
+    }
+}
+
+// The twiddles (n - 1) and the (cos, sin)(pi k / 2n) factors (n/2 + 1) of
+// one axis, and its frequency weights (n, when w is given), into shared
+// memory, every load of a thread issued before its first store (one memory
+// round trip).  These are constant tables, so blocks stage them before
+// waiting on the previous grid; the caller's barrier publishes them.
+template <int LOGN>
+__device__ __forceinline__ void stage_tables(float2 *tw_s, float2 *q_s, float *w_s, const float2 *__restrict__ tw,
+                                             const float2 *__restrict__ q, const float *__restrict__ w) {
+    constexpr int n = 1 << LOGN;
+    constexpr int it_t = (n - 1 + kThreads - 1) / kThreads, it_q = (n / 2 + 1 + kThreads - 1) / kThreads,
+                  it_w = (n + kThreads - 1) / kThreads;
+    float2 vt[it_t], vq[it_q];
+    float vw[it_w];
+#pragma unroll
+    for (int it = 0; it < it_t; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (i < n - 1) vt[it] = tw[i];
+    }
+#pragma unroll
+    for (int it = 0; it < it_q; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (i <= n / 2) vq[it] = q[i];
+    }
+#pragma unroll
+    for (int it = 0; it < it_w; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (w && i < n) vw[it] = w[i];
+    }
+#pragma unroll
+    for (int it = 0; it < it_t; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (i < n - 1) tw_s[i] = vt[it];
+    }
+#pragma unroll
+    for (int it = 0; it < it_q; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (i <= n / 2) q_s[i] = vq[it];
+    }
+#pragma unroll
+    for (int it = 0; it < it_w; it++) {
+        const int i = threadIdx.x + it * kThreads;
+        if (w && i < n) w_s[i] = vw[it];
+    }
+}
+
+// Spectrum entry k (1 <= k <= n/2) of the DCT-III input X (entry n-k is its
+// conjugate): (X[k] c + X[n-k] s, X[k] s - X[n-k] c) / 2.
+__device__ __forceinline__ float2 dct3_spec(float xk, float xm, float2 cs) {
+    return make_float2(0.5f * (xk * cs.x + xm * cs.y), 0.5f * (xk * cs.y - xm * cs.x));
+}
+
+// Entries k and n-k (bit-reversed positions) of the complex spectrum that
+// carries DCT-III input a in its real part and b in its imaginary part.
+__device__ __forceinline__ void pack_spec(float2 *o, int k, int m, int logn, float2 sa, float2 sb, bool self) {
+    o[brev(k, logn)] = make_float2(sa.x - sb.y, sa.y + sb.x);
+    if (!self) o[brev(m, logn)] = make_float2(sa.x + sb.y, sb.x - sa.y);
+}
+
+// Shared-memory bytes of the per-axis tables (twiddles, factors, weights).
+__host__ __device__ constexpr size_t table_bytes(int n) {
+    return sizeof(float2) * ((size_t)n - 1 + n / 2 + 1) + sizeof(float) * n;
+}
+
+// Row pairs (pass 1) and rows (pass 3) per block: enough sequences that a
+// butterfly stage has a thread each.
+template <int LOGN>
+__host__ __device__ constexpr int seqs_per_block() {
+    return (2 * kThreads) >> LOGN > 1 ? (2 * kThreads) >> LOGN : 1;
+}
+
+// ---- pass 1: rows along y --------------------------------------------------
+template <int LOGN>
+__global__ void __launch_bounds__(kThreads)
+k_fft_rows_fwd(const float *__restrict__ rho, float *__restrict__ T, int pairs, const float2 *__restrict__ tw,
+               const float2 *__restrict__ q, const DevScalars *__restrict__ S) {
+    constexpr int n = 1 << LOGN, NS = seqs_per_block<LOGN>();
+    extern __shared__ float2 sm[];
+    float2 *tw_s = sm + NS * n, *q_s = tw_s + n - 1;
+    stage_tables<LOGN>(tw_s, q_s, nullptr, tw, q, nullptr);
+    pdl_begin();
+    if (S && S->done) return;
+    const int x0 = blockIdx.x * pairs * 2;
+    constexpr int li = (NS * n + kThreads - 1) / kThreads;
+    float2 v[li];
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e < (pairs << LOGN)) {
+            const int p = e >> LOGN, y = e & (n - 1);
+            const size_t ra = (size_t)(x0 + 2 * p) * n;
+            v[it] = make_float2(rho[ra + y], rho[ra + n + y]);
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e < (pairs << LOGN)) sm[(e & ~(n - 1)) + brev(makhoul(e & (n - 1), n), LOGN)] = v[it];
+    }
+    __syncthreads();
+    block_fft<false, LOGN, NS>(sm, pairs, tw_s);
+    constexpr int hk = n / 2 + 1;
+    constexpr int pi_ = (NS * hk + kThreads - 1) / kThreads;
+#pragma unroll
+    for (int it = 0; it < pi_; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e >= pairs * hk) break;
+        const int p = e / hk, k = e - p * hk;
+        const float2 *z = sm + (p << LOGN);
+        const float2 Z = z[k], M = z[(n - k) & (n - 1)];
+        // V_a = (Z + conj M) / 2, V_b = (Z - conj M) / 2i
+        const float ar = 0.5f * (Z.x + M.x), ai = 0.5f * (Z.y - M.y);
+        const float br = 0.5f * (Z.y + M.y), bi = -0.5f * (Z.x - M.x);
+        const float2 cs = q_s[k];
+        float *ta = T + (size_t)(x0 + 2 * p) * n, *tb = ta + n;
+        ta[k] = ar * cs.x + ai * cs.y;
+        tb[k] = br * cs.x + bi * cs.y;
+        if (k != 0 && k != n / 2) {
+            ta[n - k] = ar * cs.y - ai * cs.x;
+            tb[n - k] = br * cs.y - bi * cs.x;
+        }
+    }
+}
+
+// ---- pass 2: columns along x -----------------------------------------------
+// The spectral scale K[u][v] = kscale h_u h_v / (wx_u^2 + wy_v^2) (h_0 = 1/2,
+// K[0][0] = 0) is formed here in FP32 from the weight tables.
+template <int LOGN>
+__global__ void __launch_bounds__(kThreads)
+k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const float *__restrict__ wy, float kscale,
+           float *__restrict__ X1, float *__restrict__ X2, int ny, const float2 *__restrict__ tw,
+           const float2 *__restrict__ q, const DevScalars *__restrict__ S) {
+    constexpr int n = 1 << LOGN;
+    extern __shared__ float2 sm[];
+    float2 *fw = sm;  // 2 packed forward sequences (columns v0, v0+1 | v0+2, v0+3)
+    float2 *iv = sm;  // then 4 inverse sequences: E branch of pairs 0, 1; cosine branch of pairs 0, 1
+    float2 *tw_s = sm + 4 * n, *q_s = tw_s + n - 1;
+    float *wx_s = (float *)(q_s + n / 2 + 1);
+    stage_tables<LOGN>(tw_s, q_s, wx_s, tw, q, wx);
+    const int v0 = blockIdx.x * kCols;
+    const float4 wv4 = *reinterpret_cast<const float4 *>(wy + v0);
+    pdl_begin();
+    if (S && S->done) return;
+    constexpr int li = (n + kThreads - 1) / kThreads;
+    float4 t[li];
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int x = threadIdx.x + it * kThreads;
+        if (x < n) t[it] = *reinterpret_cast<const float4 *>(T + (size_t)x * ny + v0);
+    }
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int x = threadIdx.x + it * kThreads;
+        if (x < n) {
+            const int pos = brev(makhoul(x, n), LOGN);
+            fw[pos] = make_float2(t[it].x, t[it].y);
+            fw[n + pos] = make_float2(t[it].z, t[it].w);
+        }
+    }
+    __syncthreads();
+    block_fft<false, LOGN, 2>(fw, 2, tw_s);
+    constexpr int hk = n / 2 + 1;
+    constexpr int pi_ = (2 * hk + kThreads - 1) / kThreads;
+    // the forward spectra into registers: the inverse sequences overwrite them
+    float2 zk[pi_], zm[pi_];
+#pragma unroll
+    for (int it = 0; it < pi_; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e < 2 * hk) {
+            const int p = e / hk, k = e - p * hk;
+            zk[it] = fw[p * n + k];
+            zm[it] = fw[p * n + ((n - k) & (n - 1))];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < pi_; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e >= 2 * hk) break;
+        const int p = e / hk, k = e - p * hk;
+        const int m = (n - k) & (n - 1);
+        const bool self = (k == n / 2);
+        const float2 Z = zk[it], M = zm[it];
+        const float2 cs = q_s[k];
+        const float re[2] = {0.5f * (Z.x + M.x), 0.5f * (Z.y + M.y)};
+        const float im[2] = {0.5f * (Z.y - M.y), -0.5f * (Z.x - M.x)};
+        const float wk = wx_s[k], wm = wx_s[m];
+        float pk[2], pm[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int v = v0 + 2 * p + h;
+            const float wv = p == 0 ? (h == 0 ? wv4.x : wv4.y) : (h == 0 ? wv4.z : wv4.w);
+            const float cv = (v == 0 ? 0.5f : 1.f) * kscale;
+            // DCT-II outputs k and n-k, times K
+            const float kk = (k == 0) ? (v == 0 ? 0.f : 0.5f * cv / (wv * wv)) : cv / fmaf(wk, wk, wv * wv);
+            pk[h] = (re[h] * cs.x + im[h] * cs.y) * kk;
+            pm[h] = (self || k == 0) ? pk[h] : (re[h] * cs.y - im[h] * cs.x) * (cv / fmaf(wm, wm, wv * wv));
+        }
+        float2 *oe = iv + p * n, *oc = iv + (2 + p) * n;
+        if (k == 0) {
+            oe[0] = make_float2(0.f, 0.f);  // sine branch: b[0] = 0
+            oc[0] = make_float2(pk[0], pk[1]);
+            continue;
+        }
+        // sine branch: b[k] = wx[n-k] P[n-k], b[n-k] = wx[k] P[k]
+        pack_spec(oe, k, m, LOGN, dct3_spec(wm * pm[0], wk * pk[0], cs), dct3_spec(wm * pm[1], wk * pk[1], cs),
+                  self);
+        pack_spec(oc, k, m, LOGN, dct3_spec(pk[0], pm[0], cs), dct3_spec(pk[1], pm[1], cs), self);
+    }
+    __syncthreads();
+    block_fft<true, LOGN, 4>(iv, 4, tw_s);
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int x = threadIdx.x + it * kThreads;
+        if (x >= n) break;
+        const int m = makhoul(x, n);
+        const float sg = (x & 1) ? -1.f : 1.f;
+        const float2 e0 = iv[m], e1 = iv[n + m], c0 = iv[2 * n + m], c1 = iv[3 * n + m];
+        *reinterpret_cast<float4 *>(X1 + (size_t)x * ny + v0) = make_float4(sg * e0.x, sg * e0.y, sg * e1.x, sg * e1.y);
+        *reinterpret_cast<float4 *>(X2 + (size_t)x * ny + v0) = make_float4(c0.x, c0.y, c1.x, c1.y);
+    }
+}
+
+// ---- pass 3: rows along y, to the field -------------------------------------
+template <int LOGN, bool PHI>
+__global__ void __launch_bounds__(kThreads)
+k_fft_rows_inv(const float *__restrict__ X1, const float *__restrict__ X2, const float *__restrict__ wy,
+               float2 *__restrict__ field, float *__restrict__ phi, int rows, const float2 *__restrict__ tw,
+               const float2 *__restrict__ q, const DevScalars *__restrict__ S) {
+    constexpr int n = 1 << LOGN, NS = seqs_per_block<LOGN>();
+    constexpr int nseq = PHI ? 2 : 1;  // per row: (E_x, E_y) packed, then phi
+    extern __shared__ float2 sm[];
+    float2 *tw_s = sm + NS * nseq * n, *q_s = tw_s + n - 1;
+    float *wy_s = (float *)(q_s + n / 2 + 1);
+    stage_tables<LOGN>(tw_s, q_s, wy_s, tw, q, wy);
+    pdl_begin();
+    if (S && S->done) return;
+    const int x0 = blockIdx.x * rows;
+    constexpr int hk = n / 2 + 1;
+    constexpr int li = (NS * hk + kThreads - 1) / kThreads;
+    float4 v[li];  // X1[k], X1[n-k], X2[k], X2[n-k]
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e < rows * hk) {
+            const int r = e / hk, k = e - r * hk;
+            const int m = (n - k) & (n - 1);
+            const size_t base = (size_t)(x0 + r) * n;
+            v[it] = make_float4(X1[base + k], X1[base + m], X2[base + k], X2[base + m]);
+        }
+    }
+    __syncthreads();  // the tables
+#pragma unroll
+    for (int it = 0; it < li; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e >= rows * hk) break;
+        const int r = e / hk, k = e - r * hk;
+        const int m = (n - k) & (n - 1);
+        float2 *o = sm + ((r * nseq) << LOGN);
+        const float a_k = v[it].x, a_m = v[it].y, b_k = v[it].z, b_m = v[it].w;
+        if (k == 0) {
+            o[0] = make_float2(a_k, 0.f);
+            if (PHI) o[n] = make_float2(b_k, 0.f);
+            continue;
+        }
+        const float2 cs = q_s[k];
+        const bool self = (k == n / 2);
+        // sine branch of wy X2: b[k] = wy[n-k] X2[n-k], b[n-k] = wy[k] X2[k]
+        pack_spec(o, k, m, LOGN, dct3_spec(a_k, a_m, cs), dct3_spec(wy_s[m] * b_m, wy_s[k] * b_k, cs), self);
+        if (PHI) pack_spec(o + n, k, m, LOGN, dct3_spec(b_k, b_m, cs), make_float2(0.f, 0.f), self);
+    }
+    __syncthreads();
+    block_fft<true, LOGN, NS * nseq>(sm, rows * nseq, tw_s);
+    constexpr int oi = (NS * n + kThreads - 1) / kThreads;
+#pragma unroll
+    for (int it = 0; it < oi; it++) {
+        const int e = threadIdx.x + it * kThreads;
+        if (e >= (rows << LOGN)) break;
+        const int r = e >> LOGN, y = e & (n - 1);
+        const int m = makhoul(y, n);
+        const float2 *z = sm + ((r * nseq) << LOGN);
+        const size_t at = (size_t)(x0 + r) * n + y;
+        field[at] = make_float2(z[m].x, (y & 1) ? -z[m].y : z[m].y);
+        if (PHI) phi[at] = z[n + m].x;
+    }
+}
+
+// Kernel instances for log2 n = kMinLog .. kMaxLog.
+constexpr int kMinLog = 3, kMaxLog = 11;
+constexpr int kLogs = kMaxLog - kMinLog + 1;
+using RowsFwdFn = void (*)(const float *, float *, int, const float2 *, const float2 *, const DevScalars *);
+using ColsFn = void (*)(const float *, const float *, const float *, float, float *, float *, int, const float2 *,
+                        const float2 *, const DevScalars *);
+using RowsInvFn = void (*)(const float *, const float *, const float *, float2 *, float *, int, const float2 *,
+                           const float2 *, const DevScalars *);
+template <int... L>
+constexpr std::array<RowsFwdFn, sizeof...(L)> rows_fwd_fns(std::integer_sequence<int, L...>) {
+    return {k_fft_rows_fwd<L + kMinLog>...};
+}
+template <int... L>
+constexpr std::array<ColsFn, sizeof...(L)> cols_fns(std::integer_sequence<int, L...>) {
+    return {k_fft_cols<L + kMinLog>...};
+}
+template <bool PHI, int... L>
+constexpr std::array<RowsInvFn, sizeof...(L)> rows_inv_fns(std::integer_sequence<int, L...>) {
+    return {k_fft_rows_inv<L + kMinLog, PHI>...};
+}
+using LogSeq = std::make_integer_sequence<int, kLogs>;
+const std::array<RowsFwdFn, kLogs> kRowsFwdFns = rows_fwd_fns(LogSeq{});
+const std::array<ColsFn, kLogs> kColsFns = cols_fns(LogSeq{});
+const std::array<RowsInvFn, kLogs> kRowsInvFns = rows_inv_fns<false>(LogSeq{});
+const std::array<RowsInvFn, kLogs> kRowsInvPhiFns = rows_inv_fns<true>(LogSeq{});
+
+int seqs_per_block_rt(int logn) { return std::max(1, (2 * kThreads) >> logn); }
+
+int ilog2_exact(int n) {
+    int l = 0;
+    while ((1 << l) < n) l++;
+    return (1 << l) == n ? l : -1;
+}
+
+template <typename T>
+int upload_vec(T *&dst, const std::vector<T> &src, std::string &err) {
+    if (cudaMalloc(&dst, src.size() * sizeof(T)) != cudaSuccess) {
+        err = "cudaMalloc failed for FFT tables";
+        return EP_ERR_NOMEM;
+    }
+    if (cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+        err = "copy of FFT tables failed";
+        return EP_ERR_CUDA;
+    }
+    return EP_OK;
+}
+
+void tables(int n, std::vector<float2> &tw, std::vector<float2> &q) {
+    const double pi = 3.14159265358979323846;
+    tw.assign(n - 1, make_float2(0.f, 0.f));
+    for (int h = 1; h < n; h <<= 1)
+        for (int j = 0; j < h; j++) tw[h - 1 + j] = make_float2((float)cos(pi * j / h), (float)-sin(pi * j / h));
+    q.assign(n / 2 + 1, make_float2(0.f, 0.f));
+    for (int k = 0; k <= n / 2; k++)
+        q[k] = make_float2((float)cos(pi * k / (2.0 * n)), (float)sin(pi * k / (2.0 * n)));
+}
+
+}  // namespace
+
+int dct_fft_init(DctPlan &p, const std::vector<double> &wx, const std::vector<double> &wy, std::string &err) {
+    const int nx = p.nx, ny = p.ny;
+    const int lx = ilog2_exact(nx), ly = ilog2_exact(ny);
+    if (lx < kMinLog || ly < kMinLog || lx > kMaxLog || ly > kMaxLog) {
+        err = "the FFT Poisson path needs power-of-two bin counts in [8, 2048]";
+        return EP_ERR_UNSUPPORTED;
+    }
+    FftPlan *f = new FftPlan;
+    p.fft = f;
+    f->lognx = lx;
+    f->logny = ly;
+    std::vector<float2> tw, q;
+    int rc;
+    tables(nx, tw, q);
+    if ((rc = upload_vec(f->twx, tw, err)) || (rc = upload_vec(f->qx, q, err))) return rc;
+    tables(ny, tw, q);
+    if ((rc = upload_vec(f->twy, tw, err)) || (rc = upload_vec(f->qy, q, err))) return rc;
+    std::vector<float> wxf(nx), wyf(ny);
+    for (int u = 0; u < nx; u++) wxf[u] = (float)wx[u];
+    for (int v = 0; v < ny; v++) wyf[v] = (float)wy[v];
+    if ((rc = upload_vec(f->wx, wxf, err)) || (rc = upload_vec(f->wy, wyf, err))) return rc;
+    f->kscale = (float)(4.0 / nx / ny);
+    if (cudaMalloc(&f->T, sizeof(float) * nx * ny) != cudaSuccess ||
+        cudaMalloc(&f->X, sizeof(float) * 2 * nx * ny) != cudaSuccess) {
+        err = "cudaMalloc failed for FFT intermediates";
+        return EP_ERR_NOMEM;
+    }
+    const int nsf = seqs_per_block_rt(ly);
+    f->pairs_fwd = std::min(nsf, nx / 2);
+    f->rows_inv = std::min(nsf, nx);
+    f->smem_rows_fwd = sizeof(float2) * (size_t)nsf * ny + table_bytes(ny);
+    f->smem_cols = sizeof(float2) * (size_t)kCols * nx + table_bytes(nx);
+    f->smem_rows_inv = sizeof(float2) * (size_t)nsf * 2 * ny + table_bytes(ny);
+    const std::pair<const void *, size_t> attr[4] = {
+        {(const void *)kRowsFwdFns[ly - kMinLog], f->smem_rows_fwd},
+        {(const void *)kColsFns[lx - kMinLog], f->smem_cols},
+        {(const void *)kRowsInvFns[ly - kMinLog], f->smem_rows_inv - sizeof(float2) * (size_t)nsf * ny},
+        {(const void *)kRowsInvPhiFns[ly - kMinLog], f->smem_rows_inv}};
+    for (auto &a : attr) {
+        if (a.second > 48 * 1024 &&
+            cudaFuncSetAttribute(a.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.second) != cudaSuccess) {
+            err = "shared memory of the FFT Poisson kernels refused";
+            return EP_ERR_UNSUPPORTED;
+        }
+        // the loop's split, unless this block needs more (1 KB per block is
+        // reserved by the hardware)
+        cudaFuncSetAttribute(a.first, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             carveout_percent(std::max(kLoopSmemBytes, a.second + 1024)));
+    }
+    return EP_OK;
+}
+
+void dct_fft_free(DctPlan &p) {
+    FftPlan *f = (FftPlan *)p.fft;
+    if (!f) return;
+    for (void *d : {(void *)f->twx, (void *)f->twy, (void *)f->qx, (void *)f->qy, (void *)f->wx, (void *)f->wy,
+                    (void *)f->T, (void *)f->X})
+        if (d) cudaFree(d);
+    delete f;
+    p.fft = nullptr;
+}
+
+int dct_fft_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S, cudaStream_t st) {
+    const FftPlan *f = (const FftPlan *)p.fft;
+    const int nx = p.nx, ny = p.ny;
+    float *X1 = f->X, *X2 = f->X + (size_t)nx * ny;
+    const int pr = launch_priority(true);
+    const int lx = f->lognx - kMinLog, ly = f->logny - kMinLog;
+    launch_kp(kRowsFwdFns[ly], nx / (2 * f->pairs_fwd), kThreads, f->smem_rows_fwd, st, pr, rho, f->T,
+              f->pairs_fwd, f->twy, f->qy, S);
+    launch_kp(kColsFns[lx], ny / kCols, kThreads, f->smem_cols, st, pr, f->T, f->wx, f->wy, f->kscale, X1, X2, ny,
+              f->twx, f->qx, S);
+    const size_t phi_seqs = sizeof(float2) * (size_t)seqs_per_block_rt(f->logny) * ny;
+    launch_kp(phi ? kRowsInvPhiFns[ly] : kRowsInvFns[ly], nx / f->rows_inv, kThreads,
+              phi ? f->smem_rows_inv : f->smem_rows_inv - phi_seqs, st, pr, X1, X2, f->wy, field, phi,
+              f->rows_inv, f->twy, f->qy, S);
+    return EP_OK;
+}
+
+}  // namespace ep

@@ -267,7 +267,7 @@ ep_status device_status(ep_engine *e) {
 // Kernels one enqueue_eval launches (the DCT is four GEMMs).
 int kernels_per_eval(const ep_engine *e) {
     const DeviceNetlist &d = e->dn;
-    return 1 + 1 + 4 + (d.n_net_tasks > 0) + (d.n_big_objs > 0) + 1;
+    return 1 + 1 + dct_launches(e->dct) + (d.n_net_tasks > 0) + (d.n_big_objs > 0) + 1;
 }
 
 int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
@@ -465,7 +465,8 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         e->err = "target_density must be in (0, 1]";
         return EP_ERR_ARG;
     }
-    if (P.dct_mode != EP_DCT_FP32 && P.dct_mode != EP_DCT_BF16X3 && P.dct_mode != EP_DCT_AUTO) {
+    if (P.dct_mode != EP_DCT_FP32 && P.dct_mode != EP_DCT_BF16X3 && P.dct_mode != EP_DCT_AUTO &&
+        P.dct_mode != EP_DCT_FFT) {
         e->err = "unknown dct_mode";
         return EP_ERR_ARG;
     }
@@ -871,15 +872,21 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         (s = dalloc(e, kc.part_hp, (size_t)2 * std::max(1, reduction_blocks(d, 0)))))
         return s;
 
-    int rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy,
-                           P.dct_mode == EP_DCT_AUTO ? EP_DCT_BF16X3 : P.dct_mode, e->err);
-    if (rc == EP_ERR_UNSUPPORTED && P.dct_mode == EP_DCT_AUTO) {
-        // the tensor-core solve does not take this grid: the FP32 one does
-        dct_plan_free(e->dct);
-        e->err.clear();
-        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, EP_DCT_FP32, e->err);
+    int rc = EP_ERR_UNSUPPORTED;
+    if (P.dct_mode == EP_DCT_AUTO) {
+        // fast transforms where the grid allows (fastest and most accurate),
+        // else the tensor-core GEMMs, else the FP32 GEMMs (any grid)
+        for (int mode : {EP_DCT_FFT, EP_DCT_BF16X3, EP_DCT_FP32}) {
+            rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, mode, e->err);
+            if (rc != EP_ERR_UNSUPPORTED) break;
+            dct_plan_free(e->dct);
+            e->err.clear();
+        }
+    } else {
+        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, P.dct_mode, e->err);
     }
     if (rc) return (ep_status)rc;
+    set_loop_carveout();
     e->stage = EP_STAGE_MGP;
     s = upload_view(e, EP_STAGE_MGP);
     if (s) return s;
@@ -1482,9 +1489,12 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
                               nullptr, nullptr, keep_maps ? 0 : 1, e->S, e->st);
               }, nothing);
     if (s) return s;
-    // G1 2nx*ny*ny + G2 2nx*nx*ny + G3 2nx*2ny*ny + G4 2*(2nx*ny*nx)
-    double dct_flops = 2 * nx * ny * ny + 2 * nx * nx * ny + 4 * nx * ny * ny + 4 * nx * ny * nx;
-    s = timed("poisson_dct", 4, 16.0 * nbin, dct_flops,
+    // dense: G1 2nx*ny*ny + G2 2nx*nx*ny + G3 2nx*2ny*ny + G4 2*(2nx*ny*nx) flops;
+    // fast transforms: bytes of the three passes (rho 4 -> T 4; T 4 -> X1, X2
+    // 8; X1, X2 8 -> field 8)
+    const bool fft = e->dct.mode == EP_DCT_FFT;
+    double dct_flops = fft ? 0.0 : 2 * nx * ny * ny + 2 * nx * nx * ny + 4 * nx * ny * ny + 4 * nx * ny * nx;
+    s = timed("poisson_dct", dct_launches(e->dct), (fft ? 36.0 : 16.0) * nbin, dct_flops,
               [&] { dct_run(e->dct, e->rho, e->field, nullptr, e->S, e->st); }, nothing);
     if (s) return s;
     s = timed("wirelength", d.n_net_tasks > 0, 28.0 * npin + 16.0 * d.n_net_tasks, 0.0,

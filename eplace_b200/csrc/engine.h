@@ -75,6 +75,8 @@ struct DctPlan {
     float *Tt = nullptr, *P = nullptr, *T3 = nullptr;
     // tensor-core path (bf16 hi/lo planes + TMA descriptors), dct_tc.cu
     void *tc = nullptr;
+    // fast-transform path (twiddle tables, intermediates), dct_fft.cu
+    void *fft = nullptr;
 };
 
 int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode,
@@ -83,6 +85,8 @@ void dct_plan_free(DctPlan &p);
 // rho (fp32 [nx][ny]) -> field (float2 [nx][ny]) and, when phi != nullptr, phi.
 int dct_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S,
             cudaStream_t st);
+// Kernel launches of one dct_run.
+inline int dct_launches(const DctPlan &p) { return p.mode == EP_DCT_FFT ? 3 : 4; }
 // The tensor-core path reads rho as bf16 hi/lo planes written by the prep kernel.
 void *dct_tc_rho_planes(DctPlan &p);
 
@@ -121,6 +125,13 @@ struct KernelCtx {
     double *part_prep, *part_wl, *part_comb, *part_hp;
 };
 int prep_blocks(const Grid &g);
+// The L1/shared split of the loop's kernels (kernels.cu): every kernel asks
+// for kLoopSmemBytes of shared memory, kernels that need more for the
+// smallest split that holds them.
+constexpr size_t kLoopSmemBytes = 64 * 1024;
+int carveout_percent(size_t smem_bytes);
+void set_loop_carveout();
+void set_sgemm_carveout(int carveout);
 // grid sizes of the reductions: 0 = per-net passes (both kernels), 1 = combine
 int reduction_blocks(const DeviceNetlist &d, int which);
 

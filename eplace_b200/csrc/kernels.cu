@@ -21,6 +21,7 @@
 // Every kernel of the loop returns at once when S->done is set, so a captured
 // multi-iteration graph stops doing work after the stop condition.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "engine.h"
@@ -989,6 +990,40 @@ void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, con
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
                  cudaStream_t st) {
     launch_nets<false, false, false>(c, d, nullptr, c.part_hp, mode, S, st);
+}
+
+int carveout_percent(size_t smem_bytes) {
+    // shared-memory capacities of an sm_100 SM, KB; the driver maps a
+    // preferred percentage of the largest to one of them, so ask for the
+    // middle of the interval that rounds to the capacity wanted
+    static const int kConfigs[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+    const double kb = (double)smem_bytes / 1024.0;
+    for (int i = 1; i < 10; i++)
+        if (kConfigs[i] >= kb) return (int)std::ceil(50.0 * (kConfigs[i - 1] + kConfigs[i]) / 228.0);
+    return 100;
+}
+
+// One L1/shared split, kLoopSmemBytes of shared memory, for every kernel of
+// the loop: an SM whose split has to change between consecutive kernels must
+// drain first, which costs the programmatic overlap of the launches (on the
+// 200k-cell solve with the FFT Poisson path: 14.5 ms per solve with one split
+// against 18.3 ms with the driver's choice per kernel).  64 KB holds the
+// per-net and combine kernels' staging at full occupancy and leaves 192 KB of
+// L1; smaller splits cost them occupancy, larger ones L1.
+void set_loop_carveout() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    const int carveout = carveout_percent(kLoopSmemBytes);
+    const void *fns[] = {(const void *)k_scatter, (const void *)k_prep, (const void *)k_wl<true, false, false>,
+                         (const void *)k_wl<true, true, false>, (const void *)k_wl<true, false, true>,
+                         (const void *)k_wl<true, true, true>, (const void *)k_wl<false, false, false>,
+                         (const void *)k_wl<false, true, false>, (const void *)k_wl<false, false, true>,
+                         (const void *)k_wl<false, true, true>, (const void *)k_gather_big, (const void *)k_combine,
+                         (const void *)k_update, (const void *)k_update_scatter, (const void *)k_bktrk_move,
+                         (const void *)k_bktrk_commit, (const void *)k_stage_begin, (const void *)k_wrap_up};
+    for (const void *f : fns) cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
+    set_sgemm_carveout(carveout);
 }
 
 }  // namespace ep

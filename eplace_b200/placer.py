@@ -22,7 +22,7 @@ MGP, FILLERONLY, CGP = 0, 1, 2
 WL_WA, WL_LSE = 0, 1
 EXP_FAST, EXP_EXACT = 0, 1
 STEP_LIPSCHITZ, STEP_BB, STEP_BKTRK = 0, 1, 2
-DCT_FP32, DCT_BF16X3, DCT_AUTO = 0, 1, 2
+DCT_FP32, DCT_BF16X3, DCT_AUTO, DCT_FFT = 0, 1, 2, 3
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)

@@ -50,12 +50,19 @@ typedef enum ep_exp_mode { EP_EXP_FAST = 0, EP_EXP_EXACT = 1 } ep_exp_mode;
 typedef enum ep_step_rule { EP_STEP_LIPSCHITZ = 0, EP_STEP_BB = 1, EP_STEP_BKTRK = 2 } ep_step_rule;
 
 /* Arithmetic of the DCT/IDCT Poisson solve (replaces FFT_2D::doFFT,
- * FFT/fft.cpp:191-284): dense GEMMs in FP32 on the CUDA cores, or on the
+ * FFT/fft.cpp:191-284): dense GEMMs in FP32 on the CUDA cores, on the
  * tcgen05 tensor cores with 3xBF16 split products (FP32 accumulate; bin
- * counts must be multiples of 128).  EP_DCT_AUTO (the default) takes the
- * tensor cores when the bin grid allows, else FP32; ep_info.dct_mode tells
- * which. */
-typedef enum ep_dct_mode { EP_DCT_FP32 = 0, EP_DCT_BF16X3 = 1, EP_DCT_AUTO = 2 } ep_dct_mode;
+ * counts must be multiples of 128), or FP32 fast transforms (length-n FFTs
+ * in shared memory; bin counts powers of two in [8, 2048]).  EP_DCT_AUTO
+ * (the default) takes the fast transforms when the bin grid allows, else
+ * the tensor cores when it allows, else the FP32 GEMMs; ep_info.dct_mode
+ * tells which. */
+typedef enum ep_dct_mode {
+    EP_DCT_FP32 = 0,
+    EP_DCT_BF16X3 = 1,
+    EP_DCT_AUTO = 2,
+    EP_DCT_FFT = 3
+} ep_dct_mode;
 
 /* Netlist in plain arrays (what Parser/parser.cpp:44-97 builds into PlaceDB).
  * Nodes are movable; a node is a macro iff its height exceeds
