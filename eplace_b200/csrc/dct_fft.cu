@@ -46,7 +46,8 @@ namespace ep {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kCols = 4;  // columns per block of k_fft_cols
+constexpr int kCols = 4;           // columns per block of k_fft_cols
+constexpr int kColThreads = 512;  // its threads: a butterfly each in the forward stages
 
 struct FftPlan {
     int lognx = 0, logny = 0;
@@ -71,32 +72,64 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// In-place radix-2 decimation-in-time FFT of nseq (<= NSEQ) length-2^LOGN
-// sequences stored back to back in shared memory, input in bit-reversed
-// order, output in natural order.  tw: the stage-major twiddles, in shared
-// memory.  INV uses e^{+...} (unnormalised inverse).  Ends with a block
-// barrier.
-template <bool INV, int LOGN, int NSEQ>
+// In-place decimation-in-time FFT of nseq (<= NSEQ) length-2^LOGN sequences
+// stored back to back in shared memory, input in bit-reversed order, output
+// in natural order, by NT threads.  tw: the stage-major twiddles, in shared
+// memory.  INV uses e^{+...} (unnormalised inverse).  The radix-2 stages run
+// in pairs: a thread loads the four elements that stages s and s+1 combine,
+// applies both stages in registers (the same operations as two radix-2
+// passes) and stores them, one barrier per pair; an odd stage count starts
+// with one radix-2 pass.  Ends with a block barrier.
+template <bool INV, int LOGN, int NSEQ, int NT>
 __device__ __forceinline__ void block_fft(float2 *buf, int nseq, const float2 *tw) {
-    constexpr int half = 1 << (LOGN - 1);
-    constexpr int iters = (NSEQ * half + kThreads - 1) / kThreads;
-    const int total = nseq * half;
+    constexpr int half = 1 << (LOGN - 1), quarter = 1 << (LOGN - 2);
+    constexpr int it2 = (NSEQ * half + NT - 1) / NT, it4 = (NSEQ * quarter + NT - 1) / NT;
+    auto twiddle = [&](int i) {
+        float2 w = tw[i];
+        if (INV) w.y = -w.y;
+        return w;
+    };
+    constexpr int first = LOGN & 1;  // stages done by the radix-2 pass
+    if (first) {
+        const int total = nseq * half;
 #pragma unroll
-    for (int s = 0; s < LOGN; s++) {
+        for (int it = 0; it < it2; it++) {
+            const int j = threadIdx.x + it * NT;
+            if (j >= total) break;
+            const int i0 = 2 * j;  // stage 0: h = 1, twiddle 1
+            const float2 a = buf[i0], c = buf[i0 + 1];
+            buf[i0] = make_float2(a.x + c.x, a.y + c.y);
+            buf[i0 + 1] = make_float2(a.x - c.x, a.y - c.y);
+        }
+        __syncthreads();
+    }
+    const int total = nseq * quarter;
+#pragma unroll
+    for (int s = first; s < LOGN; s += 2) {
         const int h = 1 << s;
 #pragma unroll
-        for (int it = 0; it < iters; it++) {
-            const int j = threadIdx.x + it * kThreads;
+        for (int it = 0; it < it4; it++) {
+            const int j = threadIdx.x + it * NT;
             if (j >= total) break;
-            const int q = j >> (LOGN - 1), b = j & (half - 1);
+            const int q = j >> (LOGN - 2), b = j & (quarter - 1);
             const int pos = b & (h - 1);
-            const int i0 = (q << LOGN) + ((b >> s) << (s + 1)) + pos;
-            float2 w = tw[h - 1 + pos];
-            if (INV) w.y = -w.y;
-            const float2 a = buf[i0];
-            const float2 t = cmul(buf[i0 + h], w);
-            buf[i0] = make_float2(a.x + t.x, a.y + t.y);
-            buf[i0 + h] = make_float2(a.x - t.x, a.y - t.y);
+            const int i0 = (q << LOGN) + ((b >> s) << (s + 2)) + pos;
+            float2 a0 = buf[i0], a1 = buf[i0 + h], a2 = buf[i0 + 2 * h], a3 = buf[i0 + 3 * h];
+            // stage s: pairs (i0, i0+h) and (i0+2h, i0+3h), one twiddle
+            const float2 w1 = twiddle(h - 1 + pos);
+            float2 t = cmul(a1, w1);
+            a1 = make_float2(a0.x - t.x, a0.y - t.y);
+            a0 = make_float2(a0.x + t.x, a0.y + t.y);
+            t = cmul(a3, w1);
+            a3 = make_float2(a2.x - t.x, a2.y - t.y);
+            a2 = make_float2(a2.x + t.x, a2.y + t.y);
+            // stage s+1: pairs (i0, i0+2h) at pos and (i0+h, i0+3h) at pos+h
+            t = cmul(a2, twiddle(2 * h - 1 + pos));
+            buf[i0] = make_float2(a0.x + t.x, a0.y + t.y);
+            buf[i0 + 2 * h] = make_float2(a0.x - t.x, a0.y - t.y);
+            t = cmul(a3, twiddle(2 * h - 1 + pos + h));
+            buf[i0 + h] = make_float2(a1.x + t.x, a1.y + t.y);
+            buf[i0 + 3 * h] = make_float2(a1.x - t.x, a1.y - t.y);
         }
         __syncthreads();
     }
@@ -107,10 +140,11 @@ __device__ __forceinline__ void block_fft(float2 *buf, int nseq, const float2 *t
 // memory, every load of a thread issued before its first store (one memory
 // round trip).  These are constant tables, so blocks stage them before
 // waiting on the previous grid; the caller's barrier publishes them.
-template <int LOGN>
+template <int LOGN, int NT = kThreads>
 __device__ __forceinline__ void stage_tables(float2 *tw_s, float2 *q_s, float *w_s, const float2 *__restrict__ tw,
                                              const float2 *__restrict__ q, const float *__restrict__ w) {
     constexpr int n = 1 << LOGN;
+    constexpr int kThreads = NT;
     constexpr int it_t = (n - 1 + kThreads - 1) / kThreads, it_q = (n / 2 + 1 + kThreads - 1) / kThreads,
                   it_w = (n + kThreads - 1) / kThreads;
     float2 vt[it_t], vq[it_q];
@@ -201,7 +235,7 @@ k_fft_rows_fwd(const float *__restrict__ rho, float *__restrict__ T, int pairs, 
         if (e < (pairs << LOGN)) sm[(e & ~(n - 1)) + brev(makhoul(e & (n - 1), n), LOGN)] = v[it];
     }
     __syncthreads();
-    block_fft<false, LOGN, NS>(sm, pairs, tw_s);
+    block_fft<false, LOGN, NS, kThreads>(sm, pairs, tw_s);
     constexpr int hk = n / 2 + 1;
     constexpr int pi_ = (NS * hk + kThreads - 1) / kThreads;
 #pragma unroll
@@ -229,17 +263,18 @@ k_fft_rows_fwd(const float *__restrict__ rho, float *__restrict__ T, int pairs, 
 // The spectral scale K[u][v] = kscale h_u h_v / (wx_u^2 + wy_v^2) (h_0 = 1/2,
 // K[0][0] = 0) is formed here in FP32 from the weight tables.
 template <int LOGN>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kColThreads)
 k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const float *__restrict__ wy, float kscale,
            float *__restrict__ X1, float *__restrict__ X2, int ny, const float2 *__restrict__ tw,
            const float2 *__restrict__ q, const DevScalars *__restrict__ S) {
     constexpr int n = 1 << LOGN;
+    constexpr int kThreads = kColThreads;
     extern __shared__ float2 sm[];
     float2 *fw = sm;  // 2 packed forward sequences (columns v0, v0+1 | v0+2, v0+3)
     float2 *iv = sm;  // then 4 inverse sequences: E branch of pairs 0, 1; cosine branch of pairs 0, 1
     float2 *tw_s = sm + 4 * n, *q_s = tw_s + n - 1;
     float *wx_s = (float *)(q_s + n / 2 + 1);
-    stage_tables<LOGN>(tw_s, q_s, wx_s, tw, q, wx);
+    stage_tables<LOGN, kColThreads>(tw_s, q_s, wx_s, tw, q, wx);
     const int v0 = blockIdx.x * kCols;
     const float4 wv4 = *reinterpret_cast<const float4 *>(wy + v0);
     pdl_begin();
@@ -261,7 +296,7 @@ k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const floa
         }
     }
     __syncthreads();
-    block_fft<false, LOGN, 2>(fw, 2, tw_s);
+    block_fft<false, LOGN, 2, kColThreads>(fw, 2, tw_s);
     constexpr int hk = n / 2 + 1;
     constexpr int pi_ = (2 * hk + kThreads - 1) / kThreads;
     // the forward spectra into registers: the inverse sequences overwrite them
@@ -311,7 +346,7 @@ k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const floa
         pack_spec(oc, k, m, LOGN, dct3_spec(pk[0], pm[0], cs), dct3_spec(pk[1], pm[1], cs), self);
     }
     __syncthreads();
-    block_fft<true, LOGN, 4>(iv, 4, tw_s);
+    block_fft<true, LOGN, 4, kColThreads>(iv, 4, tw_s);
 #pragma unroll
     for (int it = 0; it < li; it++) {
         const int x = threadIdx.x + it * kThreads;
@@ -373,7 +408,7 @@ k_fft_rows_inv(const float *__restrict__ X1, const float *__restrict__ X2, const
         if (PHI) pack_spec(o + n, k, m, LOGN, dct3_spec(b_k, b_m, cs), make_float2(0.f, 0.f), self);
     }
     __syncthreads();
-    block_fft<true, LOGN, NS * nseq>(sm, rows * nseq, tw_s);
+    block_fft<true, LOGN, NS * nseq, kThreads>(sm, rows * nseq, tw_s);
     constexpr int oi = (NS * n + kThreads - 1) / kThreads;
 #pragma unroll
     for (int it = 0; it < oi; it++) {
@@ -517,7 +552,7 @@ int dct_fft_run(DctPlan &p, const float *rho, float2 *field, float *phi, const D
     const int lx = f->lognx - kMinLog, ly = f->logny - kMinLog;
     launch_kp(kRowsFwdFns[ly], nx / (2 * f->pairs_fwd), kThreads, f->smem_rows_fwd, st, pr, rho, f->T,
               f->pairs_fwd, f->twy, f->qy, S);
-    launch_kp(kColsFns[lx], ny / kCols, kThreads, f->smem_cols, st, pr, f->T, f->wx, f->wy, f->kscale, X1, X2, ny,
+    launch_kp(kColsFns[lx], ny / kCols, kColThreads, f->smem_cols, st, pr, f->T, f->wx, f->wy, f->kscale, X1, X2, ny,
               f->twx, f->qx, S);
     const size_t phi_seqs = sizeof(float2) * (size_t)seqs_per_block_rt(f->logny) * ny;
     launch_kp(phi ? kRowsInvPhiFns[ly] : kRowsInvFns[ly], nx / f->rows_inv, kThreads,
