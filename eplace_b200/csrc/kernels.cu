@@ -23,6 +23,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <vector>
 
 #include "engine.h"
 
@@ -1010,10 +1012,17 @@ int carveout_percent(size_t smem_bytes) {
 // against 18.3 ms with the driver's choice per kernel).  64 KB holds the
 // per-net and combine kernels' staging at full occupancy and leaves 192 KB of
 // L1; smaller splits cost them occupancy, larger ones L1.
+// Function attributes belong to the current device: set once per device.
 void set_loop_carveout() {
-    static bool done = false;
-    if (done) return;
-    done = true;
+    static std::mutex mu;
+    static std::vector<int> done_devices;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (std::find(done_devices.begin(), done_devices.end(), dev) != done_devices.end()) return;
+        done_devices.push_back(dev);
+    }
     const int carveout = carveout_percent(kLoopSmemBytes);
     const void *fns[] = {(const void *)k_scatter, (const void *)k_prep, (const void *)k_wl<true, false, false>,
                          (const void *)k_wl<true, true, false>, (const void *)k_wl<true, false, true>,
