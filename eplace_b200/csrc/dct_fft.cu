@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <new>
 #include <utility>
 #include <vector>
 
@@ -489,7 +490,11 @@ int dct_fft_init(DctPlan &p, const std::vector<double> &wx, const std::vector<do
         err = "the FFT Poisson path needs power-of-two bin counts in [8, 2048]";
         return EP_ERR_UNSUPPORTED;
     }
-    FftPlan *f = new FftPlan;
+    FftPlan *f = new (std::nothrow) FftPlan;
+    if (!f) {
+        err = "out of host memory for the FFT plan";
+        return EP_ERR_NOMEM;
+    }
     p.fft = f;
     f->lognx = lx;
     f->logny = ly;
