@@ -22,7 +22,7 @@
 //   k_fft_rows_fwd  T[x][v]  = DCT-II of rho[x][:] along y          (2 rows per FFT)
 //   k_fft_cols      per column v of T: DCT-II along x, times K, then
 //                   X1[:][v] = S^T diag(wx) P[:][v] and X2[:][v] = C^T P[:][v]
-//                   (4 columns per block; X1 of two columns share one complex
+//                   (2 columns per block; X1 of two columns share one complex
 //                   IFFT and X2 of two columns another: P is dominated by its
 //                   low frequencies, so an FFT carrying P beside wx P would
 //                   round the small E inputs relative to |P|)
@@ -47,8 +47,10 @@ namespace ep {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kCols = 4;           // columns per block of k_fft_cols
-constexpr int kColThreads = 512;  // its threads: a butterfly each in the forward stages
+// Columns per block of the column pass (2 or 4; 128 threads per column).
+// Measured at 512^2: 2 columns (256 blocks) 18.5 us for the three passes and
+// 14.67 ms per solve, 4 columns (128 blocks, 512 threads) 19.0 us, 14.86 ms.
+constexpr int kCols = 2;
 
 struct FftPlan {
     int lognx = 0, logny = 0;
@@ -261,51 +263,68 @@ k_fft_rows_fwd(const float *__restrict__ rho, float *__restrict__ T, int pairs, 
 }
 
 // ---- pass 2: columns along x -----------------------------------------------
-// The spectral scale K[u][v] = kscale h_u h_v / (wx_u^2 + wy_v^2) (h_0 = 1/2,
-// K[0][0] = 0) is formed here in FP32 from the weight tables.
-template <int LOGN>
-__global__ void __launch_bounds__(kColThreads)
+// COLS (2 or 4) columns per block, 128 * COLS threads; column pairs
+// (v0 + 2p, v0 + 2p + 1) share the forward FFT, the E-branch IFFT and the
+// cosine-branch IFFT.  The spectral scale K[u][v] = kscale h_u h_v /
+// (wx_u^2 + wy_v^2) (h_0 = 1/2, K[0][0] = 0) is formed here in FP32 from the
+// weight tables.
+template <int COLS>
+struct ColVec;
+template <>
+struct ColVec<2> {
+    using T = float2;
+};
+template <>
+struct ColVec<4> {
+    using T = float4;
+};
+
+template <int LOGN, int COLS>
+__global__ void __launch_bounds__(128 * COLS)
 k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const float *__restrict__ wy, float kscale,
            float *__restrict__ X1, float *__restrict__ X2, int ny, const float2 *__restrict__ tw,
            const float2 *__restrict__ q, const DevScalars *__restrict__ S) {
     constexpr int n = 1 << LOGN;
-    constexpr int kThreads = kColThreads;
+    constexpr int kThreads = 128 * COLS, NP = COLS / 2;
+    using V = typename ColVec<COLS>::T;
     extern __shared__ float2 sm[];
-    float2 *fw = sm;  // 2 packed forward sequences (columns v0, v0+1 | v0+2, v0+3)
-    float2 *iv = sm;  // then 4 inverse sequences: E branch of pairs 0, 1; cosine branch of pairs 0, 1
-    float2 *tw_s = sm + 4 * n, *q_s = tw_s + n - 1;
+    float2 *fw = sm;  // NP packed forward sequences (columns v0 + 2p, v0 + 2p + 1)
+    float2 *iv = sm;  // then COLS inverse sequences: E branch of each pair, then cosine branch of each pair
+    float2 *tw_s = sm + COLS * n, *q_s = tw_s + n - 1;
     float *wx_s = (float *)(q_s + n / 2 + 1);
-    stage_tables<LOGN, kColThreads>(tw_s, q_s, wx_s, tw, q, wx);
-    const int v0 = blockIdx.x * kCols;
-    const float4 wv4 = *reinterpret_cast<const float4 *>(wy + v0);
+    stage_tables<LOGN, kThreads>(tw_s, q_s, wx_s, tw, q, wx);
+    const int v0 = blockIdx.x * COLS;
+    const V wvv = *reinterpret_cast<const V *>(wy + v0);
+    const float *wvc = reinterpret_cast<const float *>(&wvv);
     pdl_begin();
     if (S && S->done) return;
     constexpr int li = (n + kThreads - 1) / kThreads;
-    float4 t[li];
+    V t[li];
 #pragma unroll
     for (int it = 0; it < li; it++) {
         const int x = threadIdx.x + it * kThreads;
-        if (x < n) t[it] = *reinterpret_cast<const float4 *>(T + (size_t)x * ny + v0);
+        if (x < n) t[it] = *reinterpret_cast<const V *>(T + (size_t)x * ny + v0);
     }
 #pragma unroll
     for (int it = 0; it < li; it++) {
         const int x = threadIdx.x + it * kThreads;
         if (x < n) {
             const int pos = brev(makhoul(x, n), LOGN);
-            fw[pos] = make_float2(t[it].x, t[it].y);
-            fw[n + pos] = make_float2(t[it].z, t[it].w);
+            const float *tv = reinterpret_cast<const float *>(&t[it]);
+#pragma unroll
+            for (int p = 0; p < NP; p++) fw[p * n + pos] = make_float2(tv[2 * p], tv[2 * p + 1]);
         }
     }
     __syncthreads();
-    block_fft<false, LOGN, 2, kColThreads>(fw, 2, tw_s);
+    block_fft<false, LOGN, NP, kThreads>(fw, NP, tw_s);
     constexpr int hk = n / 2 + 1;
-    constexpr int pi_ = (2 * hk + kThreads - 1) / kThreads;
+    constexpr int pi_ = (NP * hk + kThreads - 1) / kThreads;
     // the forward spectra into registers: the inverse sequences overwrite them
     float2 zk[pi_], zm[pi_];
 #pragma unroll
     for (int it = 0; it < pi_; it++) {
         const int e = threadIdx.x + it * kThreads;
-        if (e < 2 * hk) {
+        if (e < NP * hk) {
             const int p = e / hk, k = e - p * hk;
             zk[it] = fw[p * n + k];
             zm[it] = fw[p * n + ((n - k) & (n - 1))];
@@ -315,7 +334,7 @@ k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const floa
 #pragma unroll
     for (int it = 0; it < pi_; it++) {
         const int e = threadIdx.x + it * kThreads;
-        if (e >= 2 * hk) break;
+        if (e >= NP * hk) break;
         const int p = e / hk, k = e - p * hk;
         const int m = (n - k) & (n - 1);
         const bool self = (k == n / 2);
@@ -328,14 +347,14 @@ k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const floa
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int v = v0 + 2 * p + h;
-            const float wv = p == 0 ? (h == 0 ? wv4.x : wv4.y) : (h == 0 ? wv4.z : wv4.w);
+            const float wv = wvc[2 * p + h];
             const float cv = (v == 0 ? 0.5f : 1.f) * kscale;
             // DCT-II outputs k and n-k, times K
             const float kk = (k == 0) ? (v == 0 ? 0.f : 0.5f * cv / (wv * wv)) : cv / fmaf(wk, wk, wv * wv);
             pk[h] = (re[h] * cs.x + im[h] * cs.y) * kk;
             pm[h] = (self || k == 0) ? pk[h] : (re[h] * cs.y - im[h] * cs.x) * (cv / fmaf(wm, wm, wv * wv));
         }
-        float2 *oe = iv + p * n, *oc = iv + (2 + p) * n;
+        float2 *oe = iv + p * n, *oc = iv + (NP + p) * n;
         if (k == 0) {
             oe[0] = make_float2(0.f, 0.f);  // sine branch: b[0] = 0
             oc[0] = make_float2(pk[0], pk[1]);
@@ -347,16 +366,25 @@ k_fft_cols(const float *__restrict__ T, const float *__restrict__ wx, const floa
         pack_spec(oc, k, m, LOGN, dct3_spec(pk[0], pm[0], cs), dct3_spec(pk[1], pm[1], cs), self);
     }
     __syncthreads();
-    block_fft<true, LOGN, 4, kColThreads>(iv, 4, tw_s);
+    block_fft<true, LOGN, COLS, kThreads>(iv, COLS, tw_s);
 #pragma unroll
     for (int it = 0; it < li; it++) {
         const int x = threadIdx.x + it * kThreads;
         if (x >= n) break;
         const int m = makhoul(x, n);
         const float sg = (x & 1) ? -1.f : 1.f;
-        const float2 e0 = iv[m], e1 = iv[n + m], c0 = iv[2 * n + m], c1 = iv[3 * n + m];
-        *reinterpret_cast<float4 *>(X1 + (size_t)x * ny + v0) = make_float4(sg * e0.x, sg * e0.y, sg * e1.x, sg * e1.y);
-        *reinterpret_cast<float4 *>(X2 + (size_t)x * ny + v0) = make_float4(c0.x, c0.y, c1.x, c1.y);
+        V o1, o2;
+        float *f1 = reinterpret_cast<float *>(&o1), *f2 = reinterpret_cast<float *>(&o2);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            const float2 e = iv[p * n + m], c = iv[(NP + p) * n + m];
+            f1[2 * p] = sg * e.x;
+            f1[2 * p + 1] = sg * e.y;
+            f2[2 * p] = c.x;
+            f2[2 * p + 1] = c.y;
+        }
+        *reinterpret_cast<V *>(X1 + (size_t)x * ny + v0) = o1;
+        *reinterpret_cast<V *>(X2 + (size_t)x * ny + v0) = o2;
     }
 }
 
@@ -438,7 +466,7 @@ constexpr std::array<RowsFwdFn, sizeof...(L)> rows_fwd_fns(std::integer_sequence
 }
 template <int... L>
 constexpr std::array<ColsFn, sizeof...(L)> cols_fns(std::integer_sequence<int, L...>) {
-    return {k_fft_cols<L + kMinLog>...};
+    return {k_fft_cols<L + kMinLog, kCols>...};
 }
 template <bool PHI, int... L>
 constexpr std::array<RowsInvFn, sizeof...(L)> rows_inv_fns(std::integer_sequence<int, L...>) {
@@ -557,7 +585,7 @@ int dct_fft_run(DctPlan &p, const float *rho, float2 *field, float *phi, const D
     const int lx = f->lognx - kMinLog, ly = f->logny - kMinLog;
     launch_kp(kRowsFwdFns[ly], nx / (2 * f->pairs_fwd), kThreads, f->smem_rows_fwd, st, pr, rho, f->T,
               f->pairs_fwd, f->twy, f->qy, S);
-    launch_kp(kColsFns[lx], ny / kCols, kColThreads, f->smem_cols, st, pr, f->T, f->wx, f->wy, f->kscale, X1, X2, ny,
+    launch_kp(kColsFns[lx], ny / kCols, 128 * kCols, f->smem_cols, st, pr, f->T, f->wx, f->wy, f->kscale, X1, X2, ny,
               f->twx, f->qx, S);
     const size_t phi_seqs = sizeof(float2) * (size_t)seqs_per_block_rt(f->logny) * ny;
     launch_kp(phi ? kRowsInvPhiFns[ly] : kRowsInvFns[ly], nx / f->rows_inv, kThreads,
