@@ -108,6 +108,7 @@ EXPORTS = (
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
     "ep_netbin_write", "ep_netbin_open", "ep_netbin_close",
+    "ep_bookshelf_read", "ep_bookshelf_write_pl", "ep_bookshelf_close",
     "ep_density_scatter_noalloc",
 )
 
@@ -164,6 +165,11 @@ def load():
                                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(vp)]
     L.ep_netbin_close.argtypes = [vp]
     L.ep_netbin_close.restype = None
+    L.ep_bookshelf_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.c_char_p, ctypes.c_int32]
+    L.ep_bookshelf_write_pl.argtypes = [vp, ctypes.c_char_p, _f32p, _f32p]
+    L.ep_bookshelf_close.argtypes = [vp]
+    L.ep_bookshelf_close.restype = None
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
         [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
@@ -210,11 +216,28 @@ def netbin_write(nl, path):
     return path
 
 
+def _netlist_copy(c, name, target_density, bins):
+    """A synth.Netlist holding copies of the arrays an ep_netlist points at
+    (row site widths are not part of ep_netlist and come back as 1)."""
+    from .synth import Netlist as SynthNetlist
+    nn, nt, nnet, nr = c.num_nodes, c.num_terminals, c.num_nets, c.num_rows
+    a = lambda ptr, n: np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.float32)
+    np_ = int(np.ctypeslib.as_array(c.net_start, shape=(nnet + 1,))[nnet])
+    return SynthNetlist(
+        name=name,
+        node_w=a(c.node_w, nn), node_h=a(c.node_h, nn), node_cx=a(c.node_cx, nn), node_cy=a(c.node_cy, nn),
+        term_llx=a(c.term_llx, nt), term_lly=a(c.term_lly, nt), term_w=a(c.term_w, nt),
+        term_h=a(c.term_h, nt), term_is_ni=a(c.term_is_ni, nt).astype(np.uint8),
+        net_start=a(c.net_start, nnet + 1).astype(np.int32), pin_owner=a(c.pin_owner, np_).astype(np.int32),
+        pin_dx=a(c.pin_dx, np_), pin_dy=a(c.pin_dy, np_), row_llx=a(c.row_llx, nr), row_lly=a(c.row_lly, nr),
+        row_urx=a(c.row_urx, nr), row_h=a(c.row_h, nr), row_site_w=np.ones(nr, np.float32),
+        target_density=target_density, bins=bins)
+
+
 def netbin_read(path):
     """ep_netbin_open: map a binary netlist file; returns a synth.Netlist
     holding copies of its arrays (row site widths are not part of
     ep_netlist and come back as 1)."""
-    from .synth import Netlist as SynthNetlist
     L = load()
     c, td, bins, h = Netlist(), ctypes.c_float(), ctypes.c_int32(), ctypes.c_void_p()
     rc = L.ep_netbin_open(str(path).encode(), ctypes.byref(c), ctypes.byref(td), ctypes.byref(bins),
@@ -222,20 +245,53 @@ def netbin_read(path):
     if rc:
         raise EPError(rc, f"ep_netbin_open({path}): {STATUS_NAMES[rc]}")
     try:
-        nn, nt, nnet, nr = c.num_nodes, c.num_terminals, c.num_nets, c.num_rows
-        a = lambda ptr, n: np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.float32)
-        np_ = int(np.ctypeslib.as_array(c.net_start, shape=(nnet + 1,))[nnet])
-        return SynthNetlist(
-            name=str(path).rsplit("/", 1)[-1].split(".")[0],
-            node_w=a(c.node_w, nn), node_h=a(c.node_h, nn), node_cx=a(c.node_cx, nn), node_cy=a(c.node_cy, nn),
-            term_llx=a(c.term_llx, nt), term_lly=a(c.term_lly, nt), term_w=a(c.term_w, nt),
-            term_h=a(c.term_h, nt), term_is_ni=a(c.term_is_ni, nt).astype(np.uint8),
-            net_start=a(c.net_start, nnet + 1), pin_owner=a(c.pin_owner, np_), pin_dx=a(c.pin_dx, np_),
-            pin_dy=a(c.pin_dy, np_), row_llx=a(c.row_llx, nr), row_lly=a(c.row_lly, nr),
-            row_urx=a(c.row_urx, nr), row_h=a(c.row_h, nr), row_site_w=np.ones(nr, np.float32),
-            target_density=td.value, bins=bins.value)
+        return _netlist_copy(c, str(path).rsplit("/", 1)[-1].split(".")[0], td.value, bins.value)
     finally:
         L.ep_netbin_close(h)
+
+
+class BookshelfDesign:
+    """A Bookshelf design parsed by the library (ep_bookshelf_read).
+    `netlist` is a synth.Netlist with copies of the parsed arrays;
+    write_pl(path, cx, cy) writes movable-node centres back as a .pl file
+    under the design's own names (ep_bookshelf_write_pl)."""
+
+    def __init__(self, aux_path, target_density=1.0, bins=0):
+        self._L = load()
+        c, self._h = Netlist(), ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self._L.ep_bookshelf_read(str(aux_path).encode(), ctypes.byref(c), ctypes.byref(self._h), err, 512)
+        if rc:
+            raise EPError(rc, f"ep_bookshelf_read({aux_path}): {err.value.decode()}")
+        name = str(aux_path).rsplit("/", 1)[-1].rsplit(".", 1)[0]
+        self.netlist = _netlist_copy(c, name, target_density, bins)
+
+    def write_pl(self, path, node_cx, node_cy):
+        cx = np.ascontiguousarray(node_cx, np.float32)
+        cy = np.ascontiguousarray(node_cy, np.float32)
+        if len(cx) != self.netlist.num_nodes or len(cy) != self.netlist.num_nodes:
+            raise ValueError("one centre per movable node")
+        rc = self._L.ep_bookshelf_write_pl(self._h, str(path).encode(), _p(cx, _f32p), _p(cy, _f32p))
+        if rc:
+            raise EPError(rc, f"ep_bookshelf_write_pl({path}): {STATUS_NAMES[rc]}")
+        return path
+
+    def close(self):
+        if self._h:
+            self._L.ep_bookshelf_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_batch(engines, max_steps=0):

@@ -254,6 +254,25 @@ ep_status ep_netbin_write(const char *path, const ep_netlist *nl, float target_d
 ep_status ep_netbin_open(const char *path, ep_netlist *nl, float *target_density, int32_t *bins,
                          void **handle);
 void ep_netbin_close(void *handle);
+/* Native Bookshelf reader, replacing Parser/parser.cpp:44-819 for what the
+ * placer takes from a design (.aux naming .nodes/.nets/.pl/.scl; .wts is not
+ * read): movable nodes first in file order, then terminals (terminal and
+ * terminal_NI, the latter flagged) in file order; centres = .pl lower-left +
+ * size/2 in float; pin offsets from the owner's centre; rows from the .scl
+ * CoreRow blocks; common_row_height 0 (the last row's height).  *nl points
+ * into arrays owned by *handle, valid until ep_bookshelf_close(handle).  On
+ * failure *handle is NULL, the status EP_ERR_ARG (unreadable file, malformed
+ * line, pin of an unknown node) or EP_ERR_NOMEM, and errbuf (may be NULL)
+ * receives a message of at most errlen - 1 characters. */
+ep_status ep_bookshelf_read(const char *aux_path, ep_netlist *nl, void **handle, char *errbuf, int32_t errlen);
+/* .pl file of a design read by ep_bookshelf_read, its movable nodes at the
+ * given centres (lower-left = centre - size/2 in float) and its terminals
+ * where they were read (/FIXED, /FIXED_NI), under the design's own names.
+ * Coordinates print with 9 significant digits, so a float read back is the
+ * float written; PlaceDB::outputPL (PlaceDB/placedb.cpp:1159-1214, called
+ * by outputBookShelf) prints them with %.0f. */
+ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const float *node_cx, const float *node_cy);
+void ep_bookshelf_close(void *handle);
 
 /* ep_nesterov_run for several independent engines (designs) at once, no
  * counterpart in the reference (which places one design per process): each
