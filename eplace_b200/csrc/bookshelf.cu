@@ -1,4 +1,4 @@
-// bookshelf.cu -- native Bookshelf reader and full-precision .pl writer for
+// bookshelf.cu -- native Bookshelf reader and full-precision writers for
 // the engine's array netlist.  Host code only; no CUDA call.
 //
 // The reader restates what Parser/parser.cpp:44-819 takes from a design:
@@ -46,6 +46,7 @@ struct BookshelfDesign {
     std::vector<int32_t> net_start, pin_owner;
     std::vector<float> pin_dx, pin_dy;
     std::vector<float> row_llx, row_lly, row_urx, row_h;
+    std::vector<float> row_site_w;  // not part of ep_netlist; kept for the writer
 };
 
 struct ParseError {
@@ -276,6 +277,7 @@ void parse_scl(const std::string &buf, BookshelfDesign &out) {
         out.row_lly.push_back((float)r.bottom);
         out.row_urx.push_back((float)(r.sites * r.site + r.origin));
         out.row_h.push_back((float)r.height);
+        out.row_site_w.push_back((float)r.site);
     }
 }
 
@@ -286,6 +288,69 @@ void fail(char *errbuf, int32_t errlen, const std::string &msg) {
 template <typename T>
 const T *data_or_null(const std::vector<T> &v) {
     return v.empty() ? nullptr : v.data();
+}
+
+// Buffered text output: numbers with std::to_chars(general, 9), which
+// prints what printf("%.9g") prints, written to the file in large blocks.
+class Out {
+  public:
+    explicit Out(const std::string &path) : f_(std::fopen(path.c_str(), "w")) { buf_.reserve(1 << 20); }
+    ~Out() { close(); }
+    Out &s(const char *t) {
+        buf_.append(t);
+        return spill();
+    }
+    Out &s(const std::string &t) {
+        buf_.append(t);
+        return spill();
+    }
+    Out &g(double v) {  // %.9g
+        char tmp[40];
+        const auto r = std::to_chars(tmp, tmp + sizeof tmp, v, std::chars_format::general, 9);
+        buf_.append(tmp, (size_t)(r.ptr - tmp));
+        return spill();
+    }
+    Out &d(long long v) {
+        char tmp[24];
+        const auto r = std::to_chars(tmp, tmp + sizeof tmp, v);
+        buf_.append(tmp, (size_t)(r.ptr - tmp));
+        return spill();
+    }
+    // true when the file was opened and everything reached it
+    bool close() {
+        if (!f_) return false;
+        flush();
+        const bool ok = ok_ && std::fclose(f_) == 0;
+        f_ = nullptr;
+        return ok;
+    }
+
+  private:
+    Out &spill() {
+        if (buf_.size() >= (1 << 20)) flush();
+        return *this;
+    }
+    void flush() {
+        if (f_ && !buf_.empty()) ok_ = ok_ && std::fwrite(buf_.data(), 1, buf_.size(), f_) == buf_.size();
+        buf_.clear();
+    }
+    FILE *f_;
+    std::string buf_;
+    bool ok_ = true;
+};
+
+// The .pl file: movable nodes at lower-left = centre - size/2 (float), then
+// the terminals with /FIXED or /FIXED_NI; %.9g, so a float round-trips.
+template <typename NameOf>
+ep_status write_pl(const std::string &path, int32_t nn, int32_t nt, const float *w, const float *h, const float *cx,
+                   const float *cy, const float *tllx, const float *tlly, const uint8_t *tni, NameOf name_of) {
+    Out o(path);
+    o.s("UCLA pl 1.0\n\n");
+    for (int32_t i = 0; i < nn; i++)
+        o.s(name_of(i)).s(" ").g(cx[i] - 0.5f * w[i]).s(" ").g(cy[i] - 0.5f * h[i]).s(" : N\n");
+    for (int32_t k = 0; k < nt; k++)
+        o.s(name_of(nn + k)).s(" ").g(tllx[k]).s(" ").g(tlly[k]).s(tni && tni[k] ? " : N /FIXED_NI\n" : " : N /FIXED\n");
+    return o.close() ? EP_OK : EP_ERR_ARG;
 }
 
 }  // namespace
@@ -399,17 +464,72 @@ ep_status ep_bookshelf_read(const char *aux_path, ep_netlist *nl, void **handle,
 ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const float *node_cx, const float *node_cy) {
     const BookshelfDesign *d = static_cast<const BookshelfDesign *>(handle);
     if (!d || !path || (!d->node_w.empty() && (!node_cx || !node_cy))) return EP_ERR_ARG;
-    FILE *f = std::fopen(path, "w");
-    if (!f) return EP_ERR_ARG;
-    bool ok = std::fprintf(f, "UCLA pl 1.0\n\n") > 0;
-    const size_t nn = d->node_w.size();
-    for (size_t i = 0; ok && i < nn; i++)
-        ok = std::fprintf(f, "%s %.9g %.9g : N\n", d->names[i].c_str(), (double)(node_cx[i] - 0.5f * d->node_w[i]),
-                          (double)(node_cy[i] - 0.5f * d->node_h[i])) > 0;
-    for (size_t k = 0; ok && k < d->term_w.size(); k++)
-        ok = std::fprintf(f, "%s %.9g %.9g : N %s\n", d->names[nn + k].c_str(), (double)d->term_llx[k],
-                          (double)d->term_lly[k], d->term_ni[k] ? "/FIXED_NI" : "/FIXED") > 0;
-    ok = std::fclose(f) == 0 && ok;
+    const int32_t nn = (int32_t)d->node_w.size(), nt = (int32_t)d->term_w.size();
+    return write_pl(path, nn, nt, d->node_w.data(), d->node_h.data(), node_cx, node_cy, d->term_llx.data(),
+                    d->term_lly.data(), d->term_ni.data(), [&](int32_t i) -> const std::string & { return d->names[i]; });
+}
+
+ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist *nl, const void *design) {
+    if (!dir || !name || !nl || nl->num_nodes < 0 || nl->num_terminals < 0 || nl->num_nets < 0 || nl->num_rows < 0)
+        return EP_ERR_ARG;
+    const BookshelfDesign *d = static_cast<const BookshelfDesign *>(design);
+    const int32_t nn = nl->num_nodes, nt = nl->num_terminals, nnet = nl->num_nets, nr = nl->num_rows;
+    if (d && ((int32_t)d->node_w.size() != nn || (int32_t)d->term_w.size() != nt)) return EP_ERR_ARG;
+    const int32_t np = nnet > 0 ? nl->net_start[nnet] : 0;
+    std::string tmp;
+    auto node_name = [&](int32_t i) -> const std::string & {
+        if (d) return d->names[i];
+        tmp = (i < nn ? "o" : "t") + std::to_string(i < nn ? i : i - nn);
+        return tmp;
+    };
+    const std::string base = std::string(dir) + "/" + name, nm(name);
+    bool ok;
+    {
+        Out o(base + ".aux");
+        o.s("RowBasedPlacement : ").s(nm + ".nodes ").s(nm + ".nets ").s(nm + ".wts ").s(nm + ".pl ");
+        o.s(nm + ".scl\n");
+        ok = o.close();
+    }
+    if (ok) {
+        Out o(base + ".nodes");
+        o.s("UCLA nodes 1.0\nNumNodes : ").d(nn + nt).s("\nNumTerminals : ").d(nt).s("\n");
+        for (int32_t i = 0; i < nn; i++) o.s(node_name(i)).s(" ").g(nl->node_w[i]).s(" ").g(nl->node_h[i]).s("\n");
+        for (int32_t k = 0; k < nt; k++)
+            o.s(node_name(nn + k)).s(" ").g(nl->term_w[k]).s(" ").g(nl->term_h[k])
+                .s(nl->term_is_ni && nl->term_is_ni[k] ? " terminal_NI\n" : " terminal\n");
+        ok = o.close();
+    }
+    if (ok) {
+        Out o(base + ".nets");
+        o.s("UCLA nets 1.0\nNumNets : ").d(nnet).s("\nNumPins : ").d(np).s("\n");
+        for (int32_t n = 0; n < nnet; n++) {
+            o.s("NetDegree : ").d(nl->net_start[n + 1] - nl->net_start[n]).s(" n").d(n).s("\n");
+            for (int32_t p = nl->net_start[n]; p < nl->net_start[n + 1]; p++)
+                o.s(node_name(nl->pin_owner[p])).s(" B : ").g(nl->pin_dx[p]).s(" ").g(nl->pin_dy[p]).s("\n");
+        }
+        ok = o.close();
+    }
+    if (ok) {
+        Out o(base + ".wts");
+        o.s("UCLA wts 1.0\n");
+        ok = o.close();
+    }
+    if (ok)
+        ok = write_pl(base + ".pl", nn, nt, nl->node_w, nl->node_h, nl->node_cx, nl->node_cy, nl->term_llx,
+                      nl->term_lly, nl->term_is_ni, node_name) == EP_OK;
+    if (ok) {
+        Out o(base + ".scl");
+        o.s("UCLA scl 1.0\nNumRows : ").d(nr).s("\n");
+        for (int32_t r = 0; r < nr; r++) {
+            const float site = d && (int32_t)d->row_site_w.size() == nr ? d->row_site_w[r] : 1.f;
+            const float sites = (nl->row_urx[r] - nl->row_llx[r]) / site;
+            o.s("CoreRow Horizontal\n Coordinate : ").g(nl->row_lly[r]).s("\n Height : ").g(nl->row_h[r]);
+            o.s("\n Sitewidth : ").g(site).s("\n Sitespacing : ").g(site);
+            o.s("\n Siteorient : N\n Sitesymmetry : Y\n SubrowOrigin : ").g(nl->row_llx[r]).s(" Numsites : ");
+            o.g(sites).s("\nEnd\n");
+        }
+        ok = o.close();
+    }
     return ok ? EP_OK : EP_ERR_ARG;
 }
 

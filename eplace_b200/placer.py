@@ -108,7 +108,7 @@ EXPORTS = (
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
     "ep_netbin_write", "ep_netbin_open", "ep_netbin_close",
-    "ep_bookshelf_read", "ep_bookshelf_write_pl", "ep_bookshelf_close",
+    "ep_bookshelf_read", "ep_bookshelf_write_pl", "ep_bookshelf_write", "ep_bookshelf_close",
     "ep_density_scatter_noalloc",
 )
 
@@ -168,6 +168,7 @@ def load():
     L.ep_bookshelf_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.c_char_p, ctypes.c_int32]
     L.ep_bookshelf_write_pl.argtypes = [vp, ctypes.c_char_p, _f32p, _f32p]
+    L.ep_bookshelf_write.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Netlist), vp]
     L.ep_bookshelf_close.argtypes = [vp]
     L.ep_bookshelf_close.restype = None
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
@@ -250,6 +251,21 @@ def netbin_read(path):
         L.ep_netbin_close(h)
 
 
+def bookshelf_write(nl, directory, name=None, design=None):
+    """ep_bookshelf_write: the netlist as Bookshelf files in `directory`
+    (names o<i> / t<i> unless `design`, a BookshelfDesign of the same
+    design, gives the original ones); returns the .aux path."""
+    import os
+    os.makedirs(directory, exist_ok=True)
+    name = name or nl.name
+    c, keep = netlist_struct(nl)
+    h = design._h if design is not None else None
+    rc = load().ep_bookshelf_write(str(directory).encode(), name.encode(), ctypes.byref(c), h)
+    if rc:
+        raise EPError(rc, f"ep_bookshelf_write({directory}, {name}): {STATUS_NAMES[rc]}")
+    return os.path.join(str(directory), name + ".aux")
+
+
 class BookshelfDesign:
     """A Bookshelf design parsed by the library (ep_bookshelf_read).
     `netlist` is a synth.Netlist with copies of the parsed arrays;
@@ -275,6 +291,11 @@ class BookshelfDesign:
         if rc:
             raise EPError(rc, f"ep_bookshelf_write_pl({path}): {STATUS_NAMES[rc]}")
         return path
+
+    def write(self, directory, name=None, netlist=None):
+        """All files of the design (ep_bookshelf_write) under its own names;
+        `netlist` (default: the one read) may carry moved centres."""
+        return bookshelf_write(netlist if netlist is not None else self.netlist, directory, name, design=self)
 
     def close(self):
         if self._h:

@@ -372,11 +372,12 @@ def write_bookshelf(nl, directory):
     with open(base + ".wts", "w") as f:
         f.write("UCLA wts 1.0\n")
     with open(base + ".pl", "w") as f:
-        f.write("UCLA pl 1.0\n")
+        f.write("UCLA pl 1.0\n\n")
         for i in range(nn):
             f.write(f"{names[i]} {nl.node_cx[i] - 0.5 * nl.node_w[i]:.9g} {nl.node_cy[i] - 0.5 * nl.node_h[i]:.9g} : N\n")
         for i in range(nt):
-            f.write(f"{names[nn + i]} {nl.term_llx[i]:.9g} {nl.term_lly[i]:.9g} : N /FIXED\n")
+            fixed = "/FIXED_NI" if nl.term_is_ni[i] else "/FIXED"
+            f.write(f"{names[nn + i]} {nl.term_llx[i]:.9g} {nl.term_lly[i]:.9g} : N {fixed}\n")
     with open(base + ".scl", "w") as f:
         f.write(f"UCLA scl 1.0\nNumRows : {nl.num_rows}\n")
         for r in range(nl.num_rows):

@@ -272,6 +272,14 @@ ep_status ep_bookshelf_read(const char *aux_path, ep_netlist *nl, void **handle,
  * float written; PlaceDB::outputPL (PlaceDB/placedb.cpp:1159-1214, called
  * by outputBookShelf) prints them with %.0f. */
 ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const float *node_cx, const float *node_cy);
+/* All files of a Bookshelf design (<dir>/<name>.aux, .nodes, .nets, .wts,
+ * .pl at nl's centres, .scl) with sizes, offsets and coordinates printed
+ * with 9 significant digits; PlaceDB::outputBookShelf
+ * (PlaceDB/placedb.cpp:1022-1046) prints them with %.0f (offsets %.2f).
+ * Node names and row site widths come from `design` (a handle of
+ * ep_bookshelf_read whose node and terminal counts match nl) or, when it is
+ * NULL, are o<i> / t<i> and 1; nets are named n<i>. */
+ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist *nl, const void *design);
 void ep_bookshelf_close(void *handle);
 
 /* ep_nesterov_run for several independent engines (designs) at once, no

@@ -130,3 +130,38 @@ def test_native_reader_faster_than_python(tmp_path):
         pass
     t_native = time.perf_counter() - t0
     assert t_native * 3 < t_py, (t_native, t_py)
+
+
+def test_native_writer_matches_python_writer(tmp_path):
+    nl = synth.mixed_size(1500, 4, 6, seed=8)
+    synth.write_bookshelf(nl, str(tmp_path / "py"))
+    placer.bookshelf_write(nl, str(tmp_path / "native"))
+    for ext in ("aux", "nodes", "nets", "wts", "pl", "scl"):
+        f = f"{nl.name}.{ext}"
+        assert (tmp_path / "native" / f).read_bytes() == (tmp_path / "py" / f).read_bytes(), ext
+
+
+def test_read_write_round_trip_keeps_names_and_site_widths(tmp_path):
+    for ext, text in CORNER.items():
+        _write(tmp_path, "c." + ext, text)
+    with placer.BookshelfDesign(str(tmp_path / "c.aux")) as bd:
+        first = bd.netlist
+        aux = bd.write(str(tmp_path / "out"), "c")
+    with placer.BookshelfDesign(aux) as bd:
+        assert_same(bd.netlist, first)
+    nodes = (tmp_path / "out" / "c.nodes").read_text().split("\n")
+    assert nodes[3:9] == ["a 4 12", "b 2.5 12", "c 3 12", "d 8 24", "P1 1 1 terminal", "P2 2 3 terminal_NI"]
+    scl = (tmp_path / "out" / "c.scl").read_text()
+    assert scl.count("Sitewidth : 0.5") == 2 and scl.count("Sitewidth : 1\n") == 1
+    assert "SubrowOrigin : 2 Numsites : 90" in scl
+
+
+def test_native_writer_faster_than_python(tmp_path):
+    nl = synth.standard_cell(40_000, seed=4)
+    t0 = time.perf_counter()
+    synth.write_bookshelf(nl, str(tmp_path / "py"))
+    t_py = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    placer.bookshelf_write(nl, str(tmp_path / "native"))
+    t_native = time.perf_counter() - t0
+    assert t_native * 3 < t_py, (t_native, t_py)
