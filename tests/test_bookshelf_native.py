@@ -165,3 +165,33 @@ def test_native_writer_faster_than_python(tmp_path):
     placer.bookshelf_write(nl, str(tmp_path / "native"))
     t_native = time.perf_counter() - t0
     assert t_native * 3 < t_py, (t_native, t_py)
+
+
+def test_native_reader_agrees_with_reference_parser(tmp_path):
+    """Against BookshelfParser::ReadFile itself (the reference compiled from
+    its sources into oracle/_ref): the same counts, node centres bit for bit,
+    and the same HPWL (PlaceDB::calcHPWL) as pins at owner centre + offset on
+    the native arrays."""
+    from oracle import refharness as R
+    if not R.available():
+        pytest.skip("the reference build (oracle/_ref) is not present")
+    nl = synth.mixed_size(3000, 5, 8, seed=2)
+    aux = synth.write_bookshelf(nl, str(tmp_path))
+    ref = R.RefPlacer(aux=aux)
+    with placer.BookshelfDesign(aux) as bd:
+        n = bd.netlist
+    assert (ref.num_nodes, ref.num_terminals, ref.num_nets, ref.num_pins, ref.num_rows) == \
+        (n.num_nodes, n.num_terminals, n.num_nets, n.num_pins, n.num_rows)
+    cx, cy = ref.node_centers()
+    assert np.array_equal(cx, n.node_cx) and np.array_equal(cy, n.node_cy)
+    tcx = n.term_llx + np.float32(0.5) * n.term_w
+    tcy = n.term_lly + np.float32(0.5) * n.term_h
+    ox, oy = np.concatenate([n.node_cx, tcx]), np.concatenate([n.node_cy, tcy])
+    px = (ox[n.pin_owner] + n.pin_dx).astype(np.float64)
+    py = (oy[n.pin_owner] + n.pin_dy).astype(np.float64)
+    seg = n.net_start[:-1]
+    deg = np.diff(n.net_start)
+    hp = ((np.maximum.reduceat(px, seg) - np.minimum.reduceat(px, seg)) +
+          (np.maximum.reduceat(py, seg) - np.minimum.reduceat(py, seg)))[deg >= 2].sum()
+    assert hp == pytest.approx(ref.hpwl(), rel=1e-7)
+    ref.close()
