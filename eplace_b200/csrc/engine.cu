@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <random>
 #include <string>
 #include <vector>
@@ -452,11 +453,9 @@ void ep_default_params(ep_params *p) {
 
 const char *ep_last_error(const ep_engine *e) { return e ? e->err.c_str() : "null engine"; }
 
-ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **out) {
-    if (!out || !params) return EP_ERR_ARG;
-    *out = nullptr;
-    ep_engine *e = new ep_engine();
-    *out = e;
+// ep_create's body; the host arrays it builds may throw std::bad_alloc,
+// which ep_create turns into EP_ERR_NOMEM.
+static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_params *params) {
     e->prm = *params;
     const ep_params &P = e->prm;
     ep_status s = check_netlist(e, nl);
@@ -892,6 +891,20 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
     if (s) return s;
     CK(cudaDeviceSynchronize());
     return EP_OK;
+}
+
+ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **out) {
+    if (!out || !params) return EP_ERR_ARG;
+    *out = nullptr;
+    ep_engine *e = new (std::nothrow) ep_engine();
+    if (!e) return EP_ERR_NOMEM;
+    *out = e;
+    try {
+        return create_engine(e, nl, params);
+    } catch (const std::bad_alloc &) {
+        e->err = "out of host memory";
+        return EP_ERR_NOMEM;
+    }
 }
 
 void ep_destroy(ep_engine *e) {
@@ -1690,8 +1703,8 @@ ep_status qp_solve(ep_engine *e, int max_it, double err[2], int &iters) {
 
 extern "C" {
 
-ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
-    if (!e) return EP_ERR_ARG;
+// ep_quadratic_placement's body (its set-up builds host arrays).
+static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
     if (e->in_run) {
         e->err = "ep_quadratic_placement cannot run inside an optimizer run";
         return EP_ERR_STATE;
@@ -1735,6 +1748,16 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
         stats->seconds = ms * 1e-3;
     }
     return EP_OK;
+}
+
+ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
+    if (!e) return EP_ERR_ARG;
+    try {
+        return quadratic_placement(e, max_iterations, stats);
+    } catch (const std::bad_alloc &) {
+        e->err = "out of host memory";
+        return EP_ERR_NOMEM;
+    }
 }
 
 }  // extern "C"
