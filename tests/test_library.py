@@ -1,5 +1,4 @@
 """CPU checks of the C-ABI library and the host-side helpers (no GPU needed)."""
-import ctypes
 import os
 import re
 

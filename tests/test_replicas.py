@@ -8,7 +8,6 @@ import os
 import socket
 import sys
 
-import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
