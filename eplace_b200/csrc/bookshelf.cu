@@ -533,6 +533,13 @@ ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist
     return ok ? EP_OK : EP_ERR_ARG;
 }
 
+ep_status ep_bookshelf_row_site_widths(const void *handle, float *out, int32_t count) {
+    const BookshelfDesign *d = static_cast<const BookshelfDesign *>(handle);
+    if (!d || count < 0 || (size_t)count != d->row_site_w.size() || (count > 0 && !out)) return EP_ERR_ARG;
+    for (int32_t r = 0; r < count; r++) out[r] = d->row_site_w[r];
+    return EP_OK;
+}
+
 void ep_bookshelf_close(void *handle) { delete static_cast<BookshelfDesign *>(handle); }
 
 }  // extern "C"

@@ -108,7 +108,8 @@ EXPORTS = (
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
     "ep_netbin_write", "ep_netbin_open", "ep_netbin_close",
-    "ep_bookshelf_read", "ep_bookshelf_write_pl", "ep_bookshelf_write", "ep_bookshelf_close",
+    "ep_bookshelf_read", "ep_bookshelf_write_pl", "ep_bookshelf_write", "ep_bookshelf_row_site_widths",
+    "ep_bookshelf_close",
     "ep_density_scatter_noalloc",
 )
 
@@ -169,6 +170,7 @@ def load():
                                     ctypes.c_char_p, ctypes.c_int32]
     L.ep_bookshelf_write_pl.argtypes = [vp, ctypes.c_char_p, _f32p, _f32p]
     L.ep_bookshelf_write.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Netlist), vp]
+    L.ep_bookshelf_row_site_widths.argtypes = [vp, _f32p, ctypes.c_int32]
     L.ep_bookshelf_close.argtypes = [vp]
     L.ep_bookshelf_close.restype = None
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
@@ -281,6 +283,9 @@ class BookshelfDesign:
             raise EPError(rc, f"ep_bookshelf_read({aux_path}): {err.value.decode()}")
         name = str(aux_path).rsplit("/", 1)[-1].rsplit(".", 1)[0]
         self.netlist = _netlist_copy(c, name, target_density, bins)
+        site = np.zeros(c.num_rows, np.float32)
+        self._L.ep_bookshelf_row_site_widths(self._h, _p(site, _f32p), int(c.num_rows))
+        self.netlist.row_site_w = site
 
     def write_pl(self, path, node_cx, node_cy):
         cx = np.ascontiguousarray(node_cx, np.float32)

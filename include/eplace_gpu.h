@@ -280,6 +280,9 @@ ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const floa
  * ep_bookshelf_read whose node and terminal counts match nl) or, when it is
  * NULL, are o<i> / t<i> and 1; nets are named n<i>. */
 ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist *nl, const void *design);
+/* Site width of each row of a design read by ep_bookshelf_read (not part of
+ * ep_netlist): count must equal its num_rows. */
+ep_status ep_bookshelf_row_site_widths(const void *handle, float *out, int32_t count);
 void ep_bookshelf_close(void *handle);
 
 /* ep_nesterov_run for several independent engines (designs) at once, no

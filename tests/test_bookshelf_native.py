@@ -13,7 +13,7 @@ import pytest
 from eplace_b200 import bookshelf, placer, synth
 
 ARRAYS = ("node_w", "node_h", "node_cx", "node_cy", "term_llx", "term_lly", "term_w", "term_h", "term_is_ni",
-          "net_start", "pin_owner", "pin_dx", "pin_dy", "row_llx", "row_lly", "row_urx", "row_h")
+          "net_start", "pin_owner", "pin_dx", "pin_dy", "row_llx", "row_lly", "row_urx", "row_h", "row_site_w")
 
 
 def assert_same(a, b):
