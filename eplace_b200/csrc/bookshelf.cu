@@ -461,15 +461,17 @@ ep_status ep_bookshelf_read(const char *aux_path, ep_netlist *nl, void **handle,
     return EP_OK;
 }
 
-ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const float *node_cx, const float *node_cy) {
+ep_status ep_bookshelf_write_pl(const void *handle, const char *path, const float *node_cx, const float *node_cy) try {
     const BookshelfDesign *d = static_cast<const BookshelfDesign *>(handle);
     if (!d || !path || (!d->node_w.empty() && (!node_cx || !node_cy))) return EP_ERR_ARG;
     const int32_t nn = (int32_t)d->node_w.size(), nt = (int32_t)d->term_w.size();
     return write_pl(path, nn, nt, d->node_w.data(), d->node_h.data(), node_cx, node_cy, d->term_llx.data(),
                     d->term_lly.data(), d->term_ni.data(), [&](int32_t i) -> const std::string & { return d->names[i]; });
+} catch (const std::bad_alloc &) {
+    return EP_ERR_NOMEM;
 }
 
-ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist *nl, const void *design) {
+ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist *nl, const void *design) try {
     if (!dir || !name || !nl || nl->num_nodes < 0 || nl->num_terminals < 0 || nl->num_nets < 0 || nl->num_rows < 0)
         return EP_ERR_ARG;
     const BookshelfDesign *d = static_cast<const BookshelfDesign *>(design);
@@ -531,6 +533,8 @@ ep_status ep_bookshelf_write(const char *dir, const char *name, const ep_netlist
         ok = o.close();
     }
     return ok ? EP_OK : EP_ERR_ARG;
+} catch (const std::bad_alloc &) {
+    return EP_ERR_NOMEM;
 }
 
 ep_status ep_bookshelf_row_site_widths(const void *handle, float *out, int32_t count) {

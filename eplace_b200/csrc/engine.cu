@@ -23,6 +23,9 @@
 using namespace ep;
 
 struct ep_engine {
+    // the error text keeps room for the out-of-memory message, so reporting
+    // that one never allocates
+    ep_engine() { err.reserve(256); }
     ep_params prm{};
     std::string err;
     int device = 0;
@@ -90,6 +93,13 @@ struct ep_engine {
 namespace {
 
 constexpr double kHostEps = 1.0e-15;
+
+// A host allocation failed inside an entry point: the message fits the
+// capacity reserved at construction, so this assignment does not allocate.
+ep_status host_oom(ep_engine *e) {
+    if (e) e->err.assign("out of host memory");
+    return EP_ERR_NOMEM;
+}
 
 bool f_less_h(float a, float b) { return (double)(a - b) < -1.0 * kHostEps; }
 bool f_greater_h(float a, float b) { return (double)(a - b) > 1.0 * kHostEps; }
@@ -896,14 +906,17 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
 ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **out) {
     if (!out || !params) return EP_ERR_ARG;
     *out = nullptr;
-    ep_engine *e = new (std::nothrow) ep_engine();
-    if (!e) return EP_ERR_NOMEM;
+    ep_engine *e = nullptr;
+    try {
+        e = new ep_engine();
+    } catch (const std::bad_alloc &) {
+        return EP_ERR_NOMEM;
+    }
     *out = e;
     try {
         return create_engine(e, nl, params);
     } catch (const std::bad_alloc &) {
-        e->err = "out of host memory";
-        return EP_ERR_NOMEM;
+        return host_oom(e);
     }
 }
 
@@ -987,7 +1000,7 @@ ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count)
     return EP_OK;
 }
 
-ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count) {
+ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count) try {
     if (!e || !xy) return EP_ERR_ARG;
     ep_status s = check_view(e, view, count);
     if (s) return s;
@@ -998,6 +1011,8 @@ ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t 
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_eval_gradient(ep_engine *e) {
@@ -1009,7 +1024,7 @@ ep_status ep_eval_gradient(ep_engine *e) {
     return device_status(e);
 }
 
-ep_status ep_initialize(ep_engine *e) {
+ep_status ep_initialize(ep_engine *e) try {
     if (!e) return EP_ERR_ARG;
     ep_status s = update_scalars(e, [](DevScalars &h) {
         h.lambda0_mode = 1;
@@ -1024,6 +1039,8 @@ ep_status ep_initialize(ep_engine *e) {
     if (s) return s;
     e->initialized = true;
     return device_status(e);
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_get_gradient(ep_engine *e, int32_t view, float *xy, int32_t count) {
@@ -1053,7 +1070,7 @@ ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wir
 }
 
 ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *terminal, float *base,
-                          float *ex, float *ey, float *phi) {
+                          float *ex, float *ey, float *phi) try {
     if (!e) return EP_ERR_ARG;
     const int nb = e->grid.nx * e->grid.ny;
     if ((node || filler || ex || ey || phi) && !e->prm.keep_maps) {
@@ -1083,6 +1100,8 @@ ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *termi
     }
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_get_density_fixed(ep_engine *e, int64_t *node, int64_t *filler) {
@@ -1156,7 +1175,7 @@ ep_status ep_hpwl(ep_engine *e, double *hpwl) {
     return EP_OK;
 }
 
-ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy) {
+ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy) try {
     if (!e) return EP_ERR_ARG;
     if (stage < 0 || stage > 2) {
         e->err = "unknown stage";
@@ -1195,6 +1214,8 @@ ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy) {
         e->graph = nullptr;
     }
     return upload_view(e, stage);
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_nesterov_begin(ep_engine *e) {
@@ -1212,7 +1233,7 @@ ep_status ep_nesterov_begin(ep_engine *e) {
     return EP_OK;
 }
 
-ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
+ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) try {
     if (!e) return EP_ERR_ARG;
     if (!e->in_run) {
         e->err = "ep_nesterov_begin must run first";
@@ -1236,6 +1257,8 @@ ep_status ep_nesterov_step(ep_engine *e, int32_t *stopped) {
     s = fetch_scalars(e);
     if (s) return s;
     return device_status(e);
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_nesterov_end(ep_engine *e) {
@@ -1348,7 +1371,7 @@ ep_status run_finish(ep_engine *e, RunState &r, ep_run_stats *stats) {
 
 extern "C" {
 
-ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) {
+ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) try {
     if (!e) return EP_ERR_ARG;
     RunState r;
     ep_status s = run_start(e, max_steps, r);
@@ -1360,9 +1383,11 @@ ep_status ep_nesterov_run(ep_engine *e, int32_t max_steps, ep_run_stats *stats) 
         }
     }
     return run_finish(e, r, stats);
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
-ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep_run_stats *stats) {
+ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep_run_stats *stats) try {
     if (!engines || count < 0) return EP_ERR_ARG;
     for (int i = 0; i < count; i++)
         if (!engines[i]) return EP_ERR_ARG;
@@ -1406,6 +1431,9 @@ ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep
         }
     }
     return first_error;
+} catch (const std::bad_alloc &) {
+    for (int i = 0; i < count; i++) engines[i]->in_run = false;
+    return EP_ERR_NOMEM;
 }
 
 ep_status ep_save_positions(ep_engine *e) {
@@ -1430,7 +1458,7 @@ ep_status ep_load_positions(ep_engine *e) {
     return EP_OK;
 }
 
-ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
+ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try {
     if (!e || !out || reps <= 0) return EP_ERR_ARG;
     std::memset(out, 0, sizeof(*out));
     const int no = e->n_obj, np = e->n_pins, nb = e->grid.nx * e->grid.ny;
@@ -1540,6 +1568,8 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) {
     if (!keep_maps) zero_maps();
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 }  // extern "C"
@@ -1755,8 +1785,7 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
     try {
         return quadratic_placement(e, max_iterations, stats);
     } catch (const std::bad_alloc &) {
-        e->err = "out of host memory";
-        return EP_ERR_NOMEM;
+        return host_oom(e);
     }
 }
 

@@ -66,7 +66,7 @@ size_t align64(size_t x) { return (x + 63) & ~(size_t)63; }
 
 extern "C" {
 
-ep_status ep_netbin_write(const char *path, const ep_netlist *nl, float target_density, int32_t bins) {
+ep_status ep_netbin_write(const char *path, const ep_netlist *nl, float target_density, int32_t bins) try {
     if (!path || !nl || nl->num_nodes < 0 || nl->num_terminals < 0 || nl->num_nets < 0 || nl->num_rows < 0)
         return EP_ERR_ARG;
     if (nl->num_nets > 0 && !nl->net_start) return EP_ERR_ARG;
@@ -123,6 +123,8 @@ ep_status ep_netbin_write(const char *path, const ep_netlist *nl, float target_d
     }
     ok = std::fclose(f) == 0 && ok;
     return ok ? EP_OK : EP_ERR_ARG;
+} catch (const std::bad_alloc &) {
+    return EP_ERR_NOMEM;
 }
 
 ep_status ep_netbin_open(const char *path, ep_netlist *nl, float *target_density, int32_t *bins,

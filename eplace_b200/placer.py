@@ -284,7 +284,10 @@ class BookshelfDesign:
         name = str(aux_path).rsplit("/", 1)[-1].rsplit(".", 1)[0]
         self.netlist = _netlist_copy(c, name, target_density, bins)
         site = np.zeros(c.num_rows, np.float32)
-        self._L.ep_bookshelf_row_site_widths(self._h, _p(site, _f32p), int(c.num_rows))
+        rc = self._L.ep_bookshelf_row_site_widths(self._h, _p(site, _f32p), int(c.num_rows))
+        if rc:
+            self.close()
+            raise EPError(rc, f"ep_bookshelf_row_site_widths({aux_path}): {STATUS_NAMES[rc]}")
         self.netlist.row_site_w = site
 
     def write_pl(self, path, node_cx, node_cy):

@@ -175,9 +175,36 @@ def smoke(seed=1):
         meta=dict(generator="smoke", seed=seed), **rows)
 
 
+def _morton_home(idx, n):
+    """Home of cell ``idx`` (of ``n``) in the unit square: the cell's place in
+    the index order read as a Morton (Z-order) code, so that every aligned
+    index range of the cluster hierarchy maps to one compact region (x from
+    the even bits, y from the odd bits of a 20-bit code)."""
+    code = ((np.asarray(idx, np.float64) + 0.5) / n * (1 << 20)).astype(np.int64)
+    x = np.zeros(code.shape, np.float64)
+    y = np.zeros(code.shape, np.float64)
+    for b in range(10):
+        x += ((code >> (2 * b + 1)) & 1) * 2.0 ** (b - 10)
+        y += ((code >> (2 * b)) & 1) * 2.0 ** (b - 10)
+    return x + 2.0 ** -11, y + 2.0 ** -11
+
+
+def _nearest_pads(hx, hy, nt, rng, spread=2):
+    """Pad index nearest to each home point (unit square), by the pad ring's
+    parameter of the closest core edge (the ring order of ``_pad_ring``:
+    bottom, right, top, left), plus a seeded offset of up to ``spread`` pads."""
+    d = np.stack([hy, 1.0 - hx, 1.0 - hy, hx])  # distance to bottom, right, top, left
+    edge = np.argmin(d, axis=0)
+    f = np.select([edge == 0, edge == 1, edge == 2, edge == 3], [hx, hy, 1.0 - hx, 1.0 - hy])
+    u = (edge + f) / 4.0
+    k = np.floor(u * nt).astype(np.int64) + rng.integers(-spread, spread + 1, hx.shape[0])
+    return np.mod(k, nt)
+
+
 def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
                   utilisation=0.7, target_density=1.0, mean_degree=3.6, max_degree=500,
-                  rent_p=0.6, leaf_cluster=8, terminal_net_fraction=0.05, bins=0):
+                  rent_p=0.6, leaf_cluster=8, terminal_net_fraction=0.05, bins=0,
+                  every_cell_pinned=False, local_pads=False):
     """Standard-cell design: cells of height 1 row with widths log-normal
     (mean 3 sites) clipped to 1..20 sites; ``num_terminals`` fixed I/O pads in a
     ring just outside the core; nets with power-law degree (alpha fitted so the
@@ -186,7 +213,17 @@ def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
     order one level at a time with probability ``rent_p`` (starting from
     clusters of ``leaf_cluster`` cells) and draws its other pins uniformly in
     that cluster; a ``terminal_net_fraction`` of nets also takes one pad.
-    Defaults give the 200k-cell / 220k-net / 2k-pad / 512x512-bin workload."""
+    Defaults give the 200k-cell / 220k-net / 2k-pad / 512x512-bin workload.
+
+    ``every_cell_pinned``: the first ``num_cells`` nets start at the cells in
+    a seeded random order (so no cell is left without a pin; otherwise about
+    e^-4 of the cells have none, and quadratic placement leaves all of those
+    at one point).  ``local_pads``: a net's pad is one of the pads nearest to
+    its first cell's home (the cell's index read as a Morton code over the
+    core, so each cluster of the hierarchy has a region) instead of a pad
+    drawn uniformly from the ring, as I/O-connected logic sits near its pads.
+    Both change the random stream, so a seed names a different design when
+    either is set."""
     rng = np.random.default_rng(seed)
     nc = int(num_cells)
     nn = int(num_nets if num_nets is not None else round(1.1 * nc))
@@ -210,6 +247,8 @@ def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
 
     # Rent-style cluster level per net: leaf size * 2^level >= pins needed
     root = rng.integers(0, nc, nn)
+    if every_cell_pinned:
+        root[:min(nc, nn)] = rng.permutation(nc)[:min(nc, nn)]
     level = rng.geometric(1.0 - rent_p, nn) - 1
     need = np.ceil(np.log2(np.maximum(n_cell_pins, 1) * 2.0 / leaf_cluster)).clip(0, None)
     level = np.maximum(level, need.astype(np.int64))
@@ -253,7 +292,11 @@ def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
                 c[0] = root[n] if root[n] not in c[1:] else c[0]
                 owner[net_start[n]:net_start[n] + kk] = c
     pad_nets = np.nonzero(has_pad)[0]
-    owner[net_start[pad_nets + 1] - 1] = nc + rng.integers(0, nt, pad_nets.size)
+    if local_pads:
+        hx, hy = _morton_home(root[pad_nets], nc)
+        owner[net_start[pad_nets + 1] - 1] = nc + _nearest_pads(hx, hy, nt, rng)
+    else:
+        owner[net_start[pad_nets + 1] - 1] = nc + rng.integers(0, nt, pad_nets.size)
 
     ww = np.concatenate([w, np.ones(nt)])
     hh = np.concatenate([h, np.ones(nt)])
@@ -268,7 +311,8 @@ def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
         term_is_ni=np.zeros(nt, np.uint8), net_start=_i32(net_start), pin_owner=_i32(owner),
         pin_dx=_f32(dx), pin_dy=_f32(dy), target_density=target_density, bins=bins,
         meta=dict(generator="standard_cell", seed=seed, alpha=alpha, utilisation=utilisation,
-                  rent_p=rent_p, mean_degree=float(deg.mean())), **rows)
+                  rent_p=rent_p, mean_degree=float(deg.mean()), every_cell_pinned=every_cell_pinned,
+                  local_pads=local_pads), **rows)
     return nl
 
 

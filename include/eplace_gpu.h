@@ -331,12 +331,17 @@ typedef struct ep_scatter_grid {
  * The int64 fixed-point scratch is a fixed file-scope device array of
  * 2 x 512 x 512 entries (4 MiB), held by every GPU that loads this library
  * until the process exits.  Grids beyond 512 x 512 bins are rejected with
- * EP_ERR_ARG and a message in err (err_len bytes, may be NULL); the total
- * object area must stay below 2^30.  The first call on each device, made with
- * that device current, looks up the scratch array's device address; make that
- * first call before any stream capture.  Every call zeroes and reuses the same
- * scratch, so calls that overlap on the GPU (on different streams, or from
- * several threads) race and must be serialised by the caller.  Work is
+ * EP_ERR_ARG and a message in err (err_len bytes, may be NULL).  The map
+ * values are sums of contributions rounded to 2^-k area units, with
+ * k = min(40, floor(62 - log2(1.05 * num_objects * bin_step_x * bin_step_y + 1)))
+ * so that no bin sum can pass the int64 range (a contribution is at most a
+ * bin's area); calls that would need k < 8 are rejected with EP_ERR_ARG.
+ * target_density must be in (0, 1].  The first call in each CUDA context of
+ * a device, made with that device current, looks up the scratch array's
+ * device address (again after a cudaDeviceReset); make that first call before
+ * any stream capture.  Every call zeroes and reuses the same scratch, so calls
+ * that overlap on the GPU (on different streams, or from several threads)
+ * race and must be serialised by the caller.  Work is
  * enqueued on `stream` (cudaStream_t, NULL = default stream). */
 ep_status ep_density_scatter_noalloc(const ep_scatter_grid *grid, int32_t num_objects,
                                      const float *cx, const float *cy, const float *w,

@@ -1,7 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the REFERENCE itself.
 
-Runs in the build container only (it needs /root/reference and the harness
-library oracle/_ref/libeplace_ref.so built by `make -C oracle`).  For each
+Runs where the reference sources are (their directory in the environment
+variable EPLACE_REF_SRC) with the harness library oracle/_ref/libeplace_ref.so
+built by `make -C oracle`.  For each
 design it records, at full float precision, what the unmodified reference
 computes on the same netlist and starting positions:
 
@@ -28,7 +29,8 @@ sys.path.insert(0, ROOT)
 from eplace_b200 import bookshelf, synth  # noqa: E402
 from oracle import refharness as R  # noqa: E402
 
-REF_SMOKE = "/root/reference/examples/smoke/smoke.aux"
+REF_SRC = os.environ.get("EPLACE_REF_SRC", "")
+REF_SMOKE = os.path.join(REF_SRC, "examples", "smoke", "smoke.aux")
 TRAJ_STEPS = 5
 
 
@@ -218,6 +220,8 @@ def record_bench_reference():
 
 
 if __name__ == "__main__":
+    if not REF_SRC or not os.path.exists(REF_SMOKE) or not R.available():
+        sys.exit("make_golden.py needs EPLACE_REF_SRC (the reference sources) and oracle/_ref built")
     if "--variants-only" not in sys.argv:
         check_reader()
         for name, nl, qp in designs():
