@@ -39,10 +39,17 @@ REF_RUNS = os.path.join(ROOT, "tests", "golden", "reference_runs.json")
 SAMPLE_ITERS = 8  # reference optimizer steps per CPU sample
 
 
-def design():
+def netlist():
+    """The 200k-cell standard-cell design: every cell on a net, pads attached
+    near their cluster (synth.standard_cell's every_cell_pinned / local_pads)."""
     from eplace_b200 import synth
-    nl = synth.standard_cell(DESIGN["cells"], seed=DESIGN["seed"])
-    return synth.blob_start(nl, seed=DESIGN["start_seed"], sigma_frac=DESIGN["start_sigma"])
+    return synth.standard_cell(DESIGN["cells"], seed=DESIGN["seed"], every_cell_pinned=True, local_pads=True)
+
+
+def design():
+    """The same design started from a seeded blob at the core centre."""
+    from eplace_b200 import synth
+    return synth.blob_start(netlist(), seed=DESIGN["start_seed"], sigma_frac=DESIGN["start_sigma"])
 
 
 def workload_config(nl, extra=None):
@@ -59,7 +66,7 @@ def workload_config(nl, extra=None):
 
 def reference_iterations():
     with open(REF_RUNS) as f:
-        return json.load(f)["stdcell_200k_mgp"]["iterations"]
+        return json.load(f)["stdcell_200k_blob_mgp"]["iterations"]
 
 
 def cpu_sample(warmup, steps, iters_per_step=SAMPLE_ITERS):

@@ -52,7 +52,51 @@ struct DevScalars {
     int mgp_iterations;
     int step_cap;      // > 0: also stop after this many steps (bounded runs)
     int bk_accept;     // backtracking: the last trial was accepted
+    double bk_ratio;   // backtracking: a trial is accepted when 1/L >= bk_ratio * step
 };
+
+// ----- working precision ------------------------------------------------------
+// The loop runs in one of two precisions (ep_params.precision): FP32 ("mixed":
+// float positions, field and wirelength terms, FP64 reductions) or FP64
+// throughout.  Kernels are templates on the real type R; Vec2<R> is its
+// two-component vector (float2 / double2).
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    using type = float2;
+    static __host__ __device__ __forceinline__ float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <>
+struct Vec2<double> {
+    using type = double2;
+    static __host__ __device__ __forceinline__ double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <typename R>
+using vec2 = typename Vec2<R>::type;
+template <typename R>
+__host__ __device__ __forceinline__ vec2<R> mk2(R x, R y) {
+    return Vec2<R>::make(x, y);
+}
+
+// Round-to-nearest arithmetic that nvcc does not contract into FMAs, in the
+// working precision (the FP32 forms keep the reference's float rounding).
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float rcp_rn(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double rcp_rn(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float max_r(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double max_r(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float min_r(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double min_r(double a, double b) { return fmin(a, b); }
 
 // ----- geometry (reference float semantics) -------------------------------
 struct Grid {
@@ -83,12 +127,17 @@ __device__ __forceinline__ double overlap_area(double l1, double b1, double r1, 
 __device__ __forceinline__ bool f_less(float a, float b) {
     return (double)__fsub_rn(a, b) < -kEps;
 }
+__device__ __forceinline__ bool f_less(double a, double b) { return __dsub_rn(a, b) < -kEps; }
 
-struct Rect {
-    float llx, lly, urx, ury, sx, sy;
+template <typename R>
+struct RectT {
+    R llx, lly, urx, ury, sx, sy;
 };
+using Rect = RectT<float>;
 
-// Object rectangle with local smoothing, EPlace/eplace.cpp:1052-1072.
+// Object rectangle with local smoothing, EPlace/eplace.cpp:1052-1072 (the
+// reference's float steps for R = float; the same steps in double for the
+// FP64 arm).
 __device__ __forceinline__ Rect object_rect(const Grid &g, float cx, float cy, float w, float h) {
     Rect r;
     float cllx = __fsub_rn(cx, __fmul_rn(0.5f, w));
@@ -114,14 +163,37 @@ __device__ __forceinline__ Rect object_rect(const Grid &g, float cx, float cy, f
     return r;
 }
 
+__device__ __forceinline__ RectT<double> object_rect(const Grid &g, double cx, double cy, double w, double h) {
+    RectT<double> r;
+    const double gx = g.sx, gy = g.sy;
+    r.llx = __dsub_rn(cx, __dmul_rn(0.5, w));
+    r.urx = __dadd_rn(r.llx, w);
+    r.lly = __dsub_rn(cy, __dmul_rn(0.5, h));
+    r.ury = __dadd_rn(r.lly, h);
+    r.sx = 1.0;
+    r.sy = 1.0;
+    if (f_less(w, gx)) {
+        r.sx = __ddiv_rn(w, gx);
+        r.llx = __dsub_rn(cx, __dmul_rn(0.5, gx));
+        r.urx = __dadd_rn(cx, __dmul_rn(0.5, gx));
+    }
+    if (f_less(h, gy)) {
+        r.sy = __ddiv_rn(h, gy);
+        r.lly = __dsub_rn(cy, __dmul_rn(0.5, gy));
+        r.ury = __dadd_rn(cy, __dmul_rn(0.5, gy));
+    }
+    return r;
+}
+
 // INT_DOWN bin range, end clamped (EPlace/eplace.cpp:1079-1104); the start is
 // clamped at 0 (the reference asserts it; the core clamp keeps it there).
-__device__ __forceinline__ void bin_range(const Grid &g, const Rect &r, int &i0, int &i1, int &j0,
+template <typename R>
+__device__ __forceinline__ void bin_range(const Grid &g, const RectT<R> &r, int &i0, int &i1, int &j0,
                                           int &j1) {
-    i0 = (int)__fdiv_rn(__fsub_rn(r.llx, g.llx), g.sx);
-    i1 = (int)__fdiv_rn(__fsub_rn(r.urx, g.llx), g.sx);
-    j0 = (int)__fdiv_rn(__fsub_rn(r.lly, g.lly), g.sy);
-    j1 = (int)__fdiv_rn(__fsub_rn(r.ury, g.lly), g.sy);
+    i0 = (int)div_rn(sub_rn(r.llx, (R)g.llx), (R)g.sx);
+    i1 = (int)div_rn(sub_rn(r.urx, (R)g.llx), (R)g.sx);
+    j0 = (int)div_rn(sub_rn(r.lly, (R)g.lly), (R)g.sy);
+    j1 = (int)div_rn(sub_rn(r.ury, (R)g.lly), (R)g.sy);
     i0 = max(i0, 0);
     j0 = max(j0, 0);
     i1 = min(i1, g.nx - 1);
@@ -129,39 +201,43 @@ __device__ __forceinline__ void bin_range(const Grid &g, const Rect &r, int &i0,
 }
 
 // Bin corners as binInitialization stores them (EPlace/eplace.cpp:300-307).
-__device__ __forceinline__ void bin_box(const Grid &g, int i, int j, float &l, float &b, float &r,
-                                        float &t) {
-    l = __fadd_rn(__fmul_rn((float)i, g.sx), g.llx);
-    b = __fadd_rn(__fmul_rn((float)j, g.sy), g.lly);
-    r = __fadd_rn(l, g.sx);
-    t = __fadd_rn(b, g.sy);
+template <typename R>
+__device__ __forceinline__ void bin_box(const Grid &g, int i, int j, R &l, R &b, R &r, R &t) {
+    l = add_rn(mul_rn((R)i, (R)g.sx), (R)g.llx);
+    b = add_rn(mul_rn((R)j, (R)g.sy), (R)g.lly);
+    r = add_rn(l, (R)g.sx);
+    t = add_rn(b, (R)g.sy);
 }
 
-__device__ __forceinline__ double rect_bin_overlap(const Grid &g, const Rect &r, int i, int j) {
-    float l, b, rr, t;
-    bin_box(g, i, j, l, b, rr, t);
+template <typename R>
+__device__ __forceinline__ double rect_bin_overlap(const Grid &g, const RectT<R> &r, int i, int j) {
+    R l, b, rr, t;
+    bin_box<R>(g, i, j, l, b, rr, t);
     return overlap_area(l, b, rr, t, r.llx, r.lly, r.urx, r.ury);
 }
 
 // PlaceDB::setModuleCenter_2D clamp (PlaceDB/placedb.cpp:257-281), double
-// compares and double sums stored to float, as the reference evaluates them.
-__device__ __forceinline__ float2 clamp_center(const Grid &g, float2 c, float2 s) {
+// compares and double sums stored in the working precision, as the reference
+// evaluates them.
+template <typename R>
+__device__ __forceinline__ vec2<R> clamp_center(const Grid &g, vec2<R> c, float2 s) {
     double hw = 0.5 * (double)s.x, hh = 0.5 * (double)s.y;
-    float x = c.x, y = c.y;
-    if ((double)x - hw < (double)g.llx) x = (float)((double)g.llx + hw + kEps);
-    if ((double)x + hw > (double)g.urx) x = (float)((double)g.urx - hw - kEps);
-    if ((double)y - hh < (double)g.lly) y = (float)((double)g.lly + hh + kEps);
-    if ((double)y + hh > (double)g.ury) y = (float)((double)g.ury - hh - kEps);
-    return make_float2(x, y);
+    R x = c.x, y = c.y;
+    if ((double)x - hw < (double)g.llx) x = (R)((double)g.llx + hw + kEps);
+    if ((double)x + hw > (double)g.urx) x = (R)((double)g.urx - hw - kEps);
+    if ((double)y - hh < (double)g.lly) y = (R)((double)g.lly + hh + kEps);
+    if ((double)y + hh > (double)g.ury) y = (R)((double)g.ury - hh - kEps);
+    return mk2<R>(x, y);
 }
 
-// fastExp, PlaceCommon/global.h:457-471 (float, ten squarings).  a / 1024 is
-// an exact power-of-two scaling, so the multiply rounds identically to the
-// reference's division.
-__device__ __forceinline__ float fast_exp(float a) {
-    a = __fadd_rn(1.0f, __fmul_rn(a, 0x1p-10f));
+// fastExp, PlaceCommon/global.h:457-471 (ten squarings of 1 + a/1024).  a /
+// 1024 is an exact power-of-two scaling, so the multiply rounds identically
+// to the reference's division.
+template <typename R>
+__device__ __forceinline__ R fast_exp(R a) {
+    a = add_rn((R)1, mul_rn(a, (R)0x1p-10));
 #pragma unroll
-    for (int i = 0; i < 10; i++) a = __fmul_rn(a, a);
+    for (int i = 0; i < 10; i++) a = mul_rn(a, a);
     return a;
 }
 

@@ -31,9 +31,9 @@ namespace ep {
 int dct_tc_init(DctPlan &p, std::string &err);
 void dct_tc_free(DctPlan &p);
 int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaStream_t st);
-int dct_fft_init(DctPlan &p, const std::vector<double> &wx, const std::vector<double> &wy, std::string &err);
+int dct_fft_init(DctPlan &p, const std::vector<double> &wx, const std::vector<double> &wy, int fp64, std::string &err);
 void dct_fft_free(DctPlan &p);
-int dct_fft_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S, cudaStream_t st);
+int dct_fft_run(DctPlan &p, const void *rho, void *field, void *phi, const DevScalars *S, cudaStream_t st);
 
 namespace {
 
@@ -143,16 +143,21 @@ int upload(T *&dst, const std::vector<T> &src, std::string &err) {
 
 }  // namespace
 
-int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode,
+int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode, int fp64,
                   std::string &err) {
     p.nx = nx;
     p.ny = ny;
     p.mode = mode;
+    p.fp64 = fp64;
+    if (fp64 && mode != EP_DCT_FFT) {
+        err = "the FP64 Poisson solve uses the fast transforms only (power-of-two bin counts in [8, 2048])";
+        return EP_ERR_UNSUPPORTED;
+    }
     const double pi = 3.14159265358979323846;
     std::vector<double> wx(nx), wy(ny);
     for (int u = 0; u < nx; u++) wx[u] = pi * u / nx;
     for (int v = 0; v < ny; v++) wy[v] = pi * v / ny * ((double)step_y / (double)step_x);
-    if (mode == EP_DCT_FFT) return dct_fft_init(p, wx, wy, err);
+    if (mode == EP_DCT_FFT) return dct_fft_init(p, wx, wy, fp64, err);
     std::vector<float> Cy((size_t)ny * ny), Cx((size_t)nx * nx), K((size_t)nx * ny),
         B3((size_t)2 * ny * ny), A4((size_t)2 * nx * nx);
     for (int v = 0; v < ny; v++)
@@ -197,10 +202,13 @@ void dct_plan_free(DctPlan &p) {
     p = DctPlan();
 }
 
-int dct_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S,
-            cudaStream_t st) {
+int dct_run(DctPlan &p, const void *rho_v, void *field_v, void *phi_v, const DevScalars *S, cudaStream_t st) {
+    if (p.mode == EP_DCT_FFT) return dct_fft_run(p, rho_v, field_v, phi_v, S, st);
+    // the dense paths are FP32 only (dct_plan_init refuses them for FP64)
+    const float *rho = (const float *)rho_v;
+    float2 *field = (float2 *)field_v;
+    float *phi = (float *)phi_v;
     if (p.mode == EP_DCT_BF16X3) return dct_tc_run(p, field, phi, S, st);
-    if (p.mode == EP_DCT_FFT) return dct_fft_run(p, rho, field, phi, S, st);
     const int nx = p.nx, ny = p.ny;
     GemmArgs a{};
     // G1: Tt = (rho Cy^T)^T

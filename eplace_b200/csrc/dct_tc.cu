@@ -59,6 +59,7 @@ struct TcGemmParams {
     const float *kscale;        // spectral scale, laid out like the output
     float2 *field;              // kTcField, batches 0 (x) and 1 (y)
     float *phi;                 // kTcField, batch 2
+    unsigned wait_limit;        // try_wait rounds of a pipeline wait before it gives up
 };
 
 // ---- PTX wrappers -------------------------------------------------------------
@@ -87,15 +88,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait; returns false (and raises the abort flag) when it gives up or
-// when another role already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
-    for (unsigned it = 0; it < kWaitLimit; it++) {
+// Bounded wait of the pipeline (limit: the engine's poll count, kWaitLimit by
+// default); returns false (and raises the abort flag) when it gives up or when
+// another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort, unsigned limit) {
+    for (unsigned it = 0; it < limit; it++) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort) return false;
     }
     *abort = 1;
     return false;
+}
+
+// The wait of the abort path for work this CTA already started (TMA loads
+// into its shared memory, MMAs into its TMEM): always kWaitLimit rounds, so
+// that a lowered pipeline limit never lets the CTA free TMEM or exit while its
+// own copies or MMAs are in flight.
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity) {
+    for (unsigned it = 0; it < kWaitLimit && !mbar_try_wait(bar, parity); it++) {
+    }
 }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,
@@ -240,6 +251,7 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     }
     pdl_begin();
 
+    int issued = pre;  // TMA stages thread 0 has issued (drained on an abort)
     if (threadIdx.x == 0) {
         // ---- TMA producer ----
         for (int kb = 0; kb < pre; kb++) {
@@ -248,10 +260,9 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
             tma_load_2d(st, &p.a_hi[bz], &full[kb], kc, m0);
             tma_load_2d(st + kATile, &p.a_lo[bz], &full[kb], kc, m0);
         }
-        int issued = pre;
         for (int kb = pre; kb < nk; kb++) {
             int s = kb % kStages, use = kb / kStages;
-            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, abort)) break;
+            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, abort, p.wait_limit)) break;
             uint8_t *st = smem + s * kStageBytes;
             const int kc = (kb0 + kb) * kBK;
             mbar_expect_tx(&full[s], kStageBytes);
@@ -261,19 +272,13 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
             tma_load_2d(st + 2 * kATile + kBTile, &p.b_lo[bz], &full[s], kc, n0);
             issued = kb + 1;
         }
-        if (*abort) {
-            // drain: the last loads issued into each stage must land before exit
-            for (int kb = issued - kStages > 0 ? issued - kStages : 0; kb < issued; kb++)
-                for (unsigned it = 0; it < kWaitLimit && !mbar_try_wait(&full[kb % kStages], (kb / kStages) & 1); it++) {
-                }
-        }
     } else if (threadIdx.x == 32) {
         // ---- MMA issuer ----
         const uint32_t idesc = umma_idesc(kBM, kBN);
         bool ok = true;
         for (int kb = 0; kb < nk && ok; kb++) {
             int s = kb % kStages, use = kb / kStages;
-            if (!mbar_wait(&full[s], use & 1, abort)) {
+            if (!mbar_wait(&full[s], use & 1, abort, p.wait_limit)) {
                 ok = false;
                 break;
             }
@@ -298,8 +303,13 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     // lane 0 waits, the warp follows its verdict (tcgen05.ld is warp-aligned).
     // Every GEMM stores its tile transposed, C[m][n] -> out[n * ldo + m], so
     // the 32 lanes of a warp (consecutive m) write consecutive addresses.
+    // On an abort, `done` still completes: the issuer commits it after its
+    // last MMA on every path, and the CTA waits for it before freeing TMEM.
     int ready = 0;
-    if (lane == 0) ready = mbar_wait(done, 0, abort) && !*abort;
+    if (lane == 0) {
+        ready = mbar_wait(done, 0, abort, p.wait_limit) && !*abort;
+        if (!ready) mbar_drain(done, 0);
+    }
     ready = __shfl_sync(0xffffffffu, ready, 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = warp * 32 + lane, m = m0 + row;
@@ -381,6 +391,12 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    // every role is past its last wait, so the abort flag is final: on an
+    // abort the loads thread 0 issued may not all have been consumed, and the
+    // last one into each stage must land before the CTA exits
+    if (threadIdx.x == 0 && *abort)
+        for (int kb = issued - kStages > 0 ? issued - kStages : 0; kb < issued; kb++)
+            mbar_drain(&full[kb % kStages], (kb / kStages) & 1);
     if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
@@ -605,6 +621,7 @@ int dct_tc_run(DctPlan &p, float2 *field, float *phi, const DevScalars *S, cudaS
     DevScalars *s = const_cast<DevScalars *>(S);
     for (int i = 0; i < 4; i++) {
         TcGemmParams &g = t->g[i];
+        g.wait_limit = p.wait_limit;
         int batch = 1;
         if (i == 3) {
             g.field = field;

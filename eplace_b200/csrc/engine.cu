@@ -47,16 +47,25 @@ struct ep_engine {
     std::vector<float2> h_size;
     std::vector<int32_t> h_view[3];
 
+    // working precision of the loop (ep_params.precision): vectors of the
+    // optimizer, pin gradients and the field hold vec2<R> (v2 bytes each),
+    // rho and phi hold R (r bytes each); R = double when fp64, else float
+    int fp64 = 0;
+    size_t v2 = sizeof(float2), r = sizeof(float);
     // device buffers
-    float2 *pos = nullptr, *x = nullptr, *g = nullptr, *y_prev = nullptr, *g_prev = nullptr;
-    float2 *size = nullptr, *pin_off = nullptr, *pin_grad = nullptr, *gd_big = nullptr;
-    float2 *dump_gd = nullptr, *dump_gwl = nullptr, *field = nullptr, *static_map = nullptr;
-    float2 *staging = nullptr;
-    float2 *bk_ysave = nullptr, *bk_gtrial = nullptr, *bk_xtrial = nullptr;  // backtracking trials
+    void *pos = nullptr, *x = nullptr, *g = nullptr, *y_prev = nullptr, *g_prev = nullptr;
+    void *pin_grad = nullptr, *gd_big = nullptr, *field = nullptr;
+    float2 *size = nullptr, *pin_off = nullptr;
+    void *dump_gd = nullptr, *dump_gwl = nullptr;  // component gradients (vec2<R>), keep_maps only
+    float2 *static_map = nullptr;
+    double2 *staging64 = nullptr;  // FP64 read-back of a view (made on first use)
+    float2 *staging = nullptr;  // host-facing float2 positions / gradients of a view
+    float2 *qp_pos = nullptr;   // FP32 centres the quadratic placement works on (FP64 engines)
+    void *bk_ysave = nullptr, *bk_gtrial = nullptr, *bk_xtrial = nullptr;  // backtracking trials
     uint8_t *flags = nullptr;
-    float *npins = nullptr, *area = nullptr, *rho = nullptr, *node_f = nullptr, *filler_f = nullptr;
+    float *npins = nullptr, *area = nullptr, *node_f = nullptr, *filler_f = nullptr;
+    void *rho = nullptr, *phi = nullptr;
     float *sxy = nullptr;
-    float *phi = nullptr;
     int32_t *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pin_dev = nullptr;
     int32_t *big_objs = nullptr, *big_slot = nullptr;
     int4 *net_tasks = nullptr;
@@ -78,7 +87,7 @@ struct ep_engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_poll = nullptr;  // the run's read-back of `done` has landed
     std::mt19937_64 rng;
-    float2 *snap = nullptr;   // ep_save_positions
+    void *snap = nullptr;     // ep_save_positions
     bool has_snap = false;
     // quadratic placement (qp.cu): net -> first device pin / pins, pin -> net
     std::vector<int32_t> h_net_first, h_net_deg, h_pin_net;
@@ -86,6 +95,7 @@ struct ep_engine {
     bool qp_ready = false;
     size_t qp_cap_x = 0, qp_cap_y = 0;
     double *qp_out_h = nullptr;  // pinned mirror of qp.out
+    int bk_trials = 64;       // backtracking trials per step before EP_ERR_TIMEOUT (ep_limits)
     int64_t launches = 0;     // engine kernels launched so far
     int64_t graph_kernels = 0;  // kernels in one replay of the step graph
 };
@@ -159,6 +169,15 @@ ep_status dalloc(ep_engine *e, T *&p, size_t n) {
     }
     e->allocs.push_back((void *)p);
     return EP_OK;
+}
+
+// n bytes of device memory for a buffer whose element type is the working
+// precision's (vec2<R> or R).
+ep_status dalloc_bytes(ep_engine *e, void *&p, size_t n) {
+    unsigned char *q = nullptr;
+    ep_status s = dalloc(e, q, n);
+    p = q;
+    return s;
 }
 
 template <typename T>
@@ -286,8 +305,8 @@ int kernels_per_hpwl(const ep_engine *e) { return e->dn.n_net_tasks > 0; }
 // totalGradientUpdate: enqueue one gradient evaluation at the current
 // positions.  The direction goes to gout; the Lipschitz sums compare with
 // (g_ref, y_ref).
-void enqueue_eval_to(ep_engine *e, int stepping, float2 *gout, const float2 *g_ref,
-                     const float2 *y_ref, bool scatter = true) {
+void enqueue_eval_to(ep_engine *e, int stepping, void *gout, const void *g_ref, const void *y_ref,
+                     bool scatter = true) {
     e->launches += kernels_per_eval(e) - (scatter ? 0 : 1);
     cudaStream_t st = e->st;
     bool keep = e->prm.keep_maps != 0;
@@ -343,17 +362,15 @@ void enqueue_hpwl(ep_engine *e, int mode) {
     e->launches += kernels_per_hpwl(e);
 }
 
-// The reference retries forever when no trial is accepted; the engine stops
-// after this many trials of one step and reports EP_ERR_TIMEOUT.
-constexpr int kBktrkMaxTrials = 64;
-
 // One step of EplaceNesterovOpt::opt_step_bktrk (Optimization/nesterov.hpp:
 // 310-369) plus updatePenaltyFactor: evaluate at y_k (1/L step, a_{k+1}),
 // then move from y_k along g_k and re-evaluate at the trial point until the
 // new 1/L is at least 0.95 of the step tried (combine, stepping mode 2),
 // then make the trial the new iterate.  Returns with the step committed.
+// The reference retries forever when no trial is accepted; the engine stops
+// after e->bk_trials trials of one step and reports EP_ERR_TIMEOUT.
 ep_status bktrk_step(ep_engine *e) {
-    const size_t bytes = sizeof(float2) * e->n_obj;
+    const size_t bytes = e->v2 * e->n_obj;
     cudaStream_t st = e->st;
     enqueue_eval(e, 1);
     CK(cudaMemcpyAsync(e->bk_ysave, e->pos, bytes, cudaMemcpyDeviceToDevice, st));
@@ -365,7 +382,7 @@ ep_status bktrk_step(ep_engine *e) {
         ep_status s = fetch_scalars(e);
         if (s) return s;
         if (e->hS->bk_accept || e->hS->status) break;
-        if (t + 1 >= kBktrkMaxTrials) {
+        if (t + 1 >= e->bk_trials) {
             s = update_scalars(e, [](DevScalars &h) {
                 h.status |= 1 << EP_ERR_TIMEOUT;
                 h.stop_pending = 1;
@@ -409,26 +426,52 @@ ep_status build_graph(ep_engine *e, int iters) {
     return EP_OK;
 }
 
-__global__ void k_gather_view(const int32_t *__restrict__ idx, int n, const float2 *__restrict__ src,
+// A stage view of a working-precision vector, as float2 (the boundary's type).
+template <typename R>
+__global__ void k_gather_view(const int32_t *__restrict__ idx, int n, const vec2<R> *__restrict__ src,
                               float2 *__restrict__ dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[idx[i]];
+    if (i < n) {
+        const vec2<R> v = src[idx[i]];
+        dst[i] = make_float2((float)v.x, (float)v.y);
+    }
 }
 
-__global__ void k_scatter_view(Grid g, const int32_t *__restrict__ idx, int n,
-                               const float2 *__restrict__ src, const float2 *__restrict__ size,
-                               float2 *__restrict__ pos) {
+// setPosition of a stage view: float2 centres clamped into the core
+// (PlaceDB::setModuleCenter_2D) and stored in the working precision.
+template <typename R>
+__global__ void k_scatter_view(Grid g, const int32_t *__restrict__ idx, int n, const float2 *__restrict__ src,
+                               const float2 *__restrict__ size, vec2<R> *__restrict__ pos) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int o = idx[i];
-    float2 c = src[i], s = size[o];
-    double hw = 0.5 * (double)s.x, hh = 0.5 * (double)s.y;
-    float xx = c.x, yy = c.y;
-    if ((double)xx - hw < (double)g.llx) xx = (float)((double)g.llx + hw + 1.0e-15);
-    if ((double)xx + hw > (double)g.urx) xx = (float)((double)g.urx - hw - 1.0e-15);
-    if ((double)yy - hh < (double)g.lly) yy = (float)((double)g.lly + hh + 1.0e-15);
-    if ((double)yy + hh > (double)g.ury) yy = (float)((double)g.ury - hh - 1.0e-15);
-    pos[o] = make_float2(xx, yy);
+    float2 c = src[i];
+    pos[o] = clamp_center<R>(g, mk2<R>((R)c.x, (R)c.y), size[o]);
+}
+
+// Precision conversion of n vec2 entries.
+template <typename A, typename B>
+__global__ void k_convert2(const vec2<A> *__restrict__ src, vec2<B> *__restrict__ dst, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = mk2<B>((B)src[i].x, (B)src[i].y);
+}
+
+template <typename R>
+__global__ void k_gather_view64(const int32_t *__restrict__ idx, int n, const vec2<R> *__restrict__ src,
+                                double2 *__restrict__ dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const vec2<R> v = src[idx[i]];
+        dst[i] = make_double2(v.x, v.y);
+    }
+}
+
+void gather_view(ep_engine *e, int view, const void *src, int count) {
+    const int32_t *idx = e->view_idx[view];
+    if (e->fp64)
+        k_gather_view<double><<<(count + 255) / 256, 256, 0, e->st>>>(idx, count, (const double2 *)src, e->staging);
+    else
+        k_gather_view<float><<<(count + 255) / 256, 256, 0, e->st>>>(idx, count, (const float2 *)src, e->staging);
 }
 
 ep_status check_view(ep_engine *e, int view, int count) {
@@ -479,6 +522,13 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         e->err = "unknown dct_mode";
         return EP_ERR_ARG;
     }
+    if (P.precision != EP_PREC_MIXED && P.precision != EP_PREC_FP64) {
+        e->err = "unknown precision";
+        return EP_ERR_ARG;
+    }
+    e->fp64 = P.precision == EP_PREC_FP64;
+    e->v2 = e->fp64 ? sizeof(double2) : sizeof(float2);
+    e->r = e->fp64 ? sizeof(double) : sizeof(float);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         e->err = "no CUDA device: the engine has no CPU fallback";
@@ -811,40 +861,52 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     kc.exact_exp = P.exp_mode == EP_EXP_EXACT;
     kc.lse = P.wl_model == EP_WL_LSE;
     kc.want_wl_value = P.keep_maps ? 1 : 0;
+    kc.fp64 = e->fp64;
 
     // ---- device ----
-    if ((s = dupload(e, e->pos, pos)) || (s = dalloc(e, e->x, no)) || (s = dalloc(e, e->g, no)) ||
-        (s = dalloc(e, e->y_prev, no)) || (s = dalloc(e, e->g_prev, no)) ||
-        (s = dupload(e, e->size, e->h_size)) || (s = dupload(e, e->pin_off, dev_off)) ||
-        (s = dalloc(e, e->pin_grad, np)) || (s = dalloc(e, e->gd_big, big.size())) ||
-        (s = dalloc(e, e->field, nb)) || (s = dupload(e, e->static_map, stat)) ||
-        (s = dalloc(e, e->staging, no)) || (s = dalloc(e, e->flags, no)) ||
+    const size_t v2 = e->v2;
+    if ((s = dalloc_bytes(e, e->pos, v2 * (no + nt))) || (s = dalloc_bytes(e, e->x, v2 * no)) ||
+        (s = dalloc_bytes(e, e->g, v2 * no)) || (s = dalloc_bytes(e, e->y_prev, v2 * no)) ||
+        (s = dalloc_bytes(e, e->g_prev, v2 * no)) || (s = dupload(e, e->size, e->h_size)) ||
+        (s = dupload(e, e->pin_off, dev_off)) || (s = dalloc_bytes(e, e->pin_grad, v2 * std::max(np, 1))) ||
+        (s = dalloc_bytes(e, e->gd_big, v2 * std::max<size_t>(big.size(), 1))) ||
+        (s = dalloc_bytes(e, e->field, v2 * nb)) || (s = dupload(e, e->static_map, stat)) ||
+        (s = dalloc(e, e->staging, no + nt)) || (s = dalloc(e, e->flags, no)) ||
         (s = dupload(e, e->npins, h_npins)) || (s = dupload(e, e->area, h_area)) ||
-        (s = dalloc(e, e->rho, nb)) || (s = dupload(e, e->sxy, h_sxy)) ||
+        (s = dalloc_bytes(e, e->rho, e->r * nb)) || (s = dupload(e, e->sxy, h_sxy)) ||
         (s = dupload(e, e->pin_owner, dev_owner)) || (s = dupload(e, e->obj_pin_start, ops)) ||
         (s = dupload(e, e->obj_pin_dev, obj_pin_dev)) || (s = dupload(e, e->net_tasks, net_tasks)) ||
         (s = dupload(e, e->big_objs, big)) ||
         (s = dupload(e, e->big_slot, big_slot)) || (s = dalloc(e, e->node_q, nb)) ||
         (s = dalloc(e, e->filler_q, nb)) || (s = dalloc(e, e->S, 1)))
         return s;
+    // centres: through the float2 staging buffer into the working precision
+    // (exact for FP64)
+    CK(cudaMemcpy(e->staging, pos.data(), sizeof(float2) * (no + nt), cudaMemcpyHostToDevice));
+    if (e->fp64)
+        k_convert2<float, double><<<(no + nt + 255) / 256, 256>>>(e->staging, (double2 *)e->pos, no + nt);
+    else
+        CK(cudaMemcpy(e->pos, e->staging, sizeof(float2) * (no + nt), cudaMemcpyDeviceToDevice));
+    CK(cudaGetLastError());
     for (int v = 0; v < 3; v++)
         if ((s = dupload(e, e->view_idx[v], e->h_view[v]))) return s;
     if (P.step_rule == EP_STEP_BKTRK &&
-        ((s = dalloc(e, e->bk_ysave, no)) || (s = dalloc(e, e->bk_gtrial, no)) || (s = dalloc(e, e->bk_xtrial, no))))
+        ((s = dalloc_bytes(e, e->bk_ysave, v2 * no)) || (s = dalloc_bytes(e, e->bk_gtrial, v2 * no)) ||
+         (s = dalloc_bytes(e, e->bk_xtrial, v2 * no))))
         return s;
     if (P.keep_maps) {
         if ((s = dalloc(e, e->node_f, nb)) || (s = dalloc(e, e->filler_f, nb)) ||
-            (s = dalloc(e, e->phi, nb)) || (s = dalloc(e, e->dump_gd, no)) ||
-            (s = dalloc(e, e->dump_gwl, no)))
+            (s = dalloc_bytes(e, e->phi, e->r * nb)) || (s = dalloc_bytes(e, e->dump_gd, v2 * no)) ||
+            (s = dalloc_bytes(e, e->dump_gwl, v2 * no)))
             return s;
     }
     CK(cudaMemset(e->node_q, 0, sizeof(unsigned long long) * nb));
     CK(cudaMemset(e->filler_q, 0, sizeof(unsigned long long) * nb));
-    CK(cudaMemset(e->g, 0, sizeof(float2) * no));
-    CK(cudaMemset(e->g_prev, 0, sizeof(float2) * no));
-    CK(cudaMemset(e->y_prev, 0, sizeof(float2) * no));
-    CK(cudaMemset(e->x, 0, sizeof(float2) * no));
-    CK(cudaMemset(e->pin_grad, 0, sizeof(float2) * std::max(np, 1)));
+    CK(cudaMemset(e->g, 0, v2 * no));
+    CK(cudaMemset(e->g_prev, 0, v2 * no));
+    CK(cudaMemset(e->y_prev, 0, v2 * no));
+    CK(cudaMemset(e->x, 0, v2 * no));
+    CK(cudaMemset(e->pin_grad, 0, v2 * std::max(np, 1)));
     CK(cudaMallocHost((void **)&e->hS, sizeof(DevScalars)));
     std::memset(e->hS, 0, sizeof(DevScalars));
     e->hS->a = 1.0;
@@ -852,6 +914,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     e->hS->max_iter = P.max_iterations > 0 ? P.max_iterations : 1000;
     e->hS->target_overflow = P.target_overflow > 0 ? P.target_overflow : 0.10f;
     e->hS->step_rule = P.step_rule;
+    e->hS->bk_ratio = 0.95;
     CK(cudaMemcpy(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice));
 
     DeviceNetlist &d = e->dn;
@@ -882,17 +945,20 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         return s;
 
     int rc = EP_ERR_UNSUPPORTED;
-    if (P.dct_mode == EP_DCT_AUTO) {
+    if (P.dct_mode == EP_DCT_AUTO && e->fp64) {
+        // the FP64 form has the fast transforms only
+        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, EP_DCT_FFT, 1, e->err);
+    } else if (P.dct_mode == EP_DCT_AUTO) {
         // fast transforms where the grid allows (fastest and most accurate),
         // else the tensor-core GEMMs, else the FP32 GEMMs (any grid)
         for (int mode : {EP_DCT_FFT, EP_DCT_BF16X3, EP_DCT_FP32}) {
-            rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, mode, e->err);
+            rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, mode, 0, e->err);
             if (rc != EP_ERR_UNSUPPORTED) break;
             dct_plan_free(e->dct);
             e->err.clear();
         }
     } else {
-        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, P.dct_mode, e->err);
+        rc = dct_plan_init(e->dct, nbx, nby, g.sx, g.sy, P.dct_mode, e->fp64, e->err);
     }
     if (rc) return (ep_status)rc;
     set_loop_carveout();
@@ -962,7 +1028,32 @@ ep_status ep_get_info(const ep_engine *e, ep_info *info) {
     info->total_row_area = e->total_row_area;
     info->density_scale = e->kc.qscale;
     info->dct_mode = e->dct.mode;
+    info->precision = e->fp64 ? EP_PREC_FP64 : EP_PREC_MIXED;
     return EP_OK;
+}
+
+ep_status ep_get_limits(const ep_engine *e, ep_limits *l) {
+    if (!e || !l) return EP_ERR_ARG;
+    l->wait_polls = e->dct.wait_limit;
+    l->bktrk_trials = e->bk_trials;
+    l->bktrk_accept = e->hS->bk_ratio;
+    return EP_OK;
+}
+
+ep_status ep_set_limits(ep_engine *e, const ep_limits *l) {
+    if (!e || !l) return EP_ERR_ARG;
+    if (l->bktrk_trials < 1 || !(l->bktrk_accept > 0)) {
+        e->err = "ep_limits: bktrk_trials must be >= 1 and bktrk_accept > 0";
+        return EP_ERR_ARG;
+    }
+    e->dct.wait_limit = l->wait_polls;
+    e->bk_trials = l->bktrk_trials;
+    if (e->graph) {  // its launches hold the old poll limit
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    const double ratio = l->bktrk_accept;
+    return update_scalars(e, [ratio](DevScalars &h) { h.bk_ratio = ratio; });
 }
 
 ep_status ep_set_stream(ep_engine *e, void *stream) {
@@ -993,7 +1084,7 @@ ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count)
     ep_status s = check_view(e, view, count);
     if (s) return s;
     if (count == 0) return EP_OK;
-    k_gather_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->view_idx[view], count, e->pos, e->staging);
+    gather_view(e, view, e->pos, count);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(xy, e->staging, sizeof(float2) * count, cudaMemcpyDeviceToHost, e->st));
     CK(cudaStreamSynchronize(e->st));
@@ -1006,8 +1097,12 @@ ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t 
     if (s) return s;
     if (count == 0) return EP_OK;
     CK(cudaMemcpyAsync(e->staging, xy, sizeof(float2) * count, cudaMemcpyHostToDevice, e->st));
-    k_scatter_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[view], count,
-                                                           e->staging, e->size, e->pos);
+    if (e->fp64)
+        k_scatter_view<double><<<(count + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[view], count,
+                                                                       e->staging, e->size, (double2 *)e->pos);
+    else
+        k_scatter_view<float><<<(count + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[view], count,
+                                                                      e->staging, e->size, (float2 *)e->pos);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
@@ -1048,25 +1143,120 @@ ep_status ep_get_gradient(ep_engine *e, int32_t view, float *xy, int32_t count) 
     ep_status s = check_view(e, view, count);
     if (s) return s;
     if (count == 0) return EP_OK;
-    k_gather_view<<<(count + 255) / 256, 256, 0, e->st>>>(e->view_idx[view], count, e->g, e->staging);
+    gather_view(e, view, e->g, count);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(xy, e->staging, sizeof(float2) * count, cudaMemcpyDeviceToHost, e->st));
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
 }
 
-ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wirelength_xy) {
+ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wirelength_xy) try {
     if (!e) return EP_ERR_ARG;
     if (!e->prm.keep_maps) {
         e->err = "component gradients need keep_maps";
         return EP_ERR_STATE;
     }
-    if (density_xy)
-        CK(cudaMemcpyAsync(density_xy, e->dump_gd, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
-    if (wirelength_xy)
-        CK(cudaMemcpyAsync(wirelength_xy, e->dump_gwl, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+    const void *src[2] = {e->dump_gd, e->dump_gwl};
+    float *dst[2] = {density_xy, wirelength_xy};
+    std::vector<double2> tmp;
+    for (int k = 0; k < 2; k++) {
+        if (!dst[k]) continue;
+        if (e->fp64) {
+            tmp.resize(e->n_obj);
+            CK(cudaMemcpyAsync(tmp.data(), src[k], sizeof(double2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+            CK(cudaStreamSynchronize(e->st));
+            for (int o = 0; o < e->n_obj; o++) {
+                dst[k][2 * o] = (float)tmp[o].x;
+                dst[k][2 * o + 1] = (float)tmp[o].y;
+            }
+        } else {
+            CK(cudaMemcpyAsync(dst[k], src[k], sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+        }
+    }
     CK(cudaStreamSynchronize(e->st));
     return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
+}
+
+ep_status ep_get_component_gradients_f64(ep_engine *e, double *density_xy, double *wirelength_xy) try {
+    if (!e) return EP_ERR_ARG;
+    if (!e->prm.keep_maps) {
+        e->err = "component gradients need keep_maps";
+        return EP_ERR_STATE;
+    }
+    const void *src[2] = {e->dump_gd, e->dump_gwl};
+    double *dst[2] = {density_xy, wirelength_xy};
+    std::vector<float2> tmp;
+    for (int k = 0; k < 2; k++) {
+        if (!dst[k]) continue;
+        if (e->fp64) {
+            CK(cudaMemcpyAsync(dst[k], src[k], sizeof(double2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+        } else {
+            tmp.resize(e->n_obj);
+            CK(cudaMemcpyAsync(tmp.data(), src[k], sizeof(float2) * e->n_obj, cudaMemcpyDeviceToHost, e->st));
+            CK(cudaStreamSynchronize(e->st));
+            for (int o = 0; o < e->n_obj; o++) {
+                dst[k][2 * o] = tmp[o].x;
+                dst[k][2 * o + 1] = tmp[o].y;
+            }
+        }
+    }
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
+}
+
+ep_status ep_get_positions_f64(ep_engine *e, int32_t view, double *xy, int32_t count) {
+    if (!e || !xy) return EP_ERR_ARG;
+    ep_status s = check_view(e, view, count);
+    if (s) return s;
+    if (count == 0) return EP_OK;
+    if (!e->staging64 && (s = dalloc(e, e->staging64, e->n_obj))) return s;
+    const int32_t *idx = e->view_idx[view];
+    if (e->fp64)
+        k_gather_view64<double><<<(count + 255) / 256, 256, 0, e->st>>>(idx, count, (const double2 *)e->pos,
+                                                                        e->staging64);
+    else
+        k_gather_view64<float><<<(count + 255) / 256, 256, 0, e->st>>>(idx, count, (const float2 *)e->pos,
+                                                                       e->staging64);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(xy, e->staging64, sizeof(double2) * count, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_get_field_f64(ep_engine *e, double *ex, double *ey, double *phi) try {
+    if (!e) return EP_ERR_ARG;
+    if (!e->prm.keep_maps) {
+        e->err = "field maps need keep_maps";
+        return EP_ERR_STATE;
+    }
+    const int nb = e->grid.nx * e->grid.ny;
+    std::vector<double2> f64(nb);
+    std::vector<double> p64(phi ? nb : 0);
+    if (e->fp64) {
+        CK(cudaMemcpyAsync(f64.data(), e->field, sizeof(double2) * nb, cudaMemcpyDeviceToHost, e->st));
+        if (phi) CK(cudaMemcpyAsync(p64.data(), e->phi, sizeof(double) * nb, cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+    } else {
+        std::vector<float2> f32(nb);
+        std::vector<float> p32(phi ? nb : 0);
+        CK(cudaMemcpyAsync(f32.data(), e->field, sizeof(float2) * nb, cudaMemcpyDeviceToHost, e->st));
+        if (phi) CK(cudaMemcpyAsync(p32.data(), e->phi, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        for (int k = 0; k < nb; k++) f64[k] = make_double2(f32[k].x, f32[k].y);
+        for (size_t k = 0; k < p32.size(); k++) p64[k] = p32[k];
+    }
+    for (int k = 0; k < nb; k++) {
+        if (ex) ex[k] = f64[k].x;
+        if (ey) ey[k] = f64[k].y;
+        if (phi) phi[k] = p64[k];
+    }
+    return EP_OK;
+} catch (const std::bad_alloc &) {
+    return host_oom(e);
 }
 
 ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *terminal, float *base,
@@ -1079,7 +1269,13 @@ ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *termi
     }
     if (node) CK(cudaMemcpyAsync(node, e->node_f, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
     if (filler) CK(cudaMemcpyAsync(filler, e->filler_f, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
-    if (phi) CK(cudaMemcpyAsync(phi, e->phi, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+    std::vector<double> phi64;
+    if (phi && e->fp64) {
+        phi64.resize(nb);
+        CK(cudaMemcpyAsync(phi64.data(), e->phi, sizeof(double) * nb, cudaMemcpyDeviceToHost, e->st));
+    } else if (phi) {
+        CK(cudaMemcpyAsync(phi, e->phi, sizeof(float) * nb, cudaMemcpyDeviceToHost, e->st));
+    }
     std::vector<float2> tmp;
     if (terminal || base || ex || ey) tmp.resize(nb);
     if (terminal || base) {
@@ -1090,7 +1286,15 @@ ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *termi
             if (base) base[k] = tmp[k].y;
         }
     }
-    if (ex || ey) {
+    if ((ex || ey) && e->fp64) {
+        std::vector<double2> f64(nb);
+        CK(cudaMemcpyAsync(f64.data(), e->field, sizeof(double2) * nb, cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        for (int k = 0; k < nb; k++) {
+            if (ex) ex[k] = (float)f64[k].x;
+            if (ey) ey[k] = (float)f64[k].y;
+        }
+    } else if (ex || ey) {
         CK(cudaMemcpyAsync(tmp.data(), e->field, sizeof(float2) * nb, cudaMemcpyDeviceToHost, e->st));
         CK(cudaStreamSynchronize(e->st));
         for (int k = 0; k < nb; k++) {
@@ -1099,6 +1303,7 @@ ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *termi
         }
     }
     CK(cudaStreamSynchronize(e->st));
+    for (size_t k = 0; k < phi64.size(); k++) phi[k] = (float)phi64[k];
     return EP_OK;
 } catch (const std::bad_alloc &) {
     return host_oom(e);
@@ -1200,8 +1405,16 @@ ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy) t
             location_to_center_h(e->grid, llx, lly, e->filler_w, e->filler_h, cx, cy);
             fp[f] = make_float2(cx, cy);
         }
-        CK(cudaMemcpyAsync(e->pos + e->n_nodes, fp.data(), sizeof(float2) * e->n_fillers,
-                           cudaMemcpyHostToDevice, e->st));
+        if (e->fp64) {
+            std::vector<double2> fp64(e->n_fillers);
+            for (int f = 0; f < e->n_fillers; f++) fp64[f] = make_double2(fp[f].x, fp[f].y);
+            CK(cudaMemcpyAsync((double2 *)e->pos + e->n_nodes, fp64.data(), sizeof(double2) * e->n_fillers,
+                               cudaMemcpyHostToDevice, e->st));
+            CK(cudaStreamSynchronize(e->st));  // fp64 goes out of scope
+        } else {
+            CK(cudaMemcpyAsync((float2 *)e->pos + e->n_nodes, fp.data(), sizeof(float2) * e->n_fillers,
+                               cudaMemcpyHostToDevice, e->st));
+        }
     }
     s = update_scalars(e, [stage](DevScalars &h) {
         if (stage == EP_STAGE_CGP) h.lambda = h.lambda / std::pow(1.1, h.mgp_iterations * 0.1);
@@ -1226,7 +1439,7 @@ ep_status ep_nesterov_begin(ep_engine *e) {
     }
     ep_status s = update_scalars(e, [](DevScalars &h) { h.step_cap = 0; });
     if (s) return s;
-    launch_stage_begin(e->dn, e->pos, e->x, e->S, e->st);
+    launch_stage_begin(e->kc, e->dn, e->pos, e->x, e->S, e->st);
     e->launches += 1;
     CK(cudaGetLastError());
     e->in_run = true;
@@ -1439,10 +1652,10 @@ ep_status ep_run_batch(ep_engine **engines, int32_t count, int32_t max_steps, ep
 ep_status ep_save_positions(ep_engine *e) {
     if (!e) return EP_ERR_ARG;
     if (!e->snap) {
-        ep_status s = dalloc(e, e->snap, e->n_obj);
+        ep_status s = dalloc_bytes(e, e->snap, e->v2 * e->n_obj);
         if (s) return s;
     }
-    CK(cudaMemcpyAsync(e->snap, e->pos, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
+    CK(cudaMemcpyAsync(e->snap, e->pos, e->v2 * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
     CK(cudaStreamSynchronize(e->st));
     e->has_snap = true;
     return EP_OK;
@@ -1454,7 +1667,7 @@ ep_status ep_load_positions(ep_engine *e) {
         e->err = "ep_save_positions must run first";
         return EP_ERR_STATE;
     }
-    CK(cudaMemcpyAsync(e->pos, e->snap, sizeof(float2) * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
+    CK(cudaMemcpyAsync(e->pos, e->snap, e->v2 * e->n_obj, cudaMemcpyDeviceToDevice, e->st));
     return EP_OK;
 }
 
@@ -1464,11 +1677,11 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
     const int no = e->n_obj, np = e->n_pins, nb = e->grid.nx * e->grid.ny;
     const DeviceNetlist &d = e->dn;
     // state the timed launches mutate, restored at the end
-    std::vector<float2> keep[5];
-    float2 *bufs[5] = {e->pos, e->x, e->g, e->y_prev, e->g_prev};
+    std::vector<unsigned char> keep[5];
+    void *bufs[5] = {e->pos, e->x, e->g, e->y_prev, e->g_prev};
     for (int k = 0; k < 5; k++) {
-        keep[k].resize(no);
-        CK(cudaMemcpyAsync(keep[k].data(), bufs[k], sizeof(float2) * no, cudaMemcpyDeviceToHost, e->st));
+        keep[k].resize(e->v2 * no);
+        CK(cudaMemcpyAsync(keep[k].data(), bufs[k], e->v2 * no, cudaMemcpyDeviceToHost, e->st));
     }
     ep_status s = fetch_scalars(e);
     if (s) return s;
@@ -1519,12 +1732,13 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
         cudaMemsetAsync(e->filler_q, 0, sizeof(unsigned long long) * nb, e->st);
     };
     const double nobj = no, npin = np, nnet = e->n_nets, nbin = nb;
+    const double q = (double)e->v2 / sizeof(float2);  // 2 for the FP64 form's vectors
     const double nx = e->grid.nx, ny = e->grid.ny;
     // algorithmic bytes: compulsory reads + writes of each group, per launch
-    s = timed("scatter", 1 + (d.n_big_objs > 0), 17.0 * nobj + 16.0 * nbin, 0.0,
+    s = timed("scatter", 1 + (d.n_big_objs > 0), (9.0 + 8.0 * q) * nobj + 16.0 * nbin, 0.0,
               [&] { launch_scatter(e->kc, d, e->node_q, e->filler_q, e->S, e->st); }, zero_maps);
     if (s) return s;
-    s = timed("prep", 1, 8.0 * nbin + 8.0 * nbin + (tc ? 4.0 : 4.0) * nbin + (keep_maps ? 0.0 : 16.0 * nbin), 0.0,
+    s = timed("prep", 1, 24.0 * nbin + 4.0 * q * nbin + (keep_maps ? 0.0 : 16.0 * nbin), 0.0,
               [&] {
                   launch_prep(e->kc, e->node_q, e->filler_q, e->static_map, bf ? nullptr : e->rho, bf,
                               nullptr, nullptr, keep_maps ? 0 : 1, e->S, e->st);
@@ -1535,10 +1749,10 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
     // 8; X1, X2 8 -> field 8)
     const bool fft = e->dct.mode == EP_DCT_FFT;
     double dct_flops = fft ? 0.0 : 2 * nx * ny * ny + 2 * nx * nx * ny + 4 * nx * ny * ny + 4 * nx * ny * nx;
-    s = timed("poisson_dct", dct_launches(e->dct), (fft ? 36.0 : 16.0) * nbin, dct_flops,
+    s = timed("poisson_dct", dct_launches(e->dct), (fft ? 36.0 * q : 16.0) * nbin, dct_flops,
               [&] { dct_run(e->dct, e->rho, e->field, nullptr, e->S, e->st); }, nothing);
     if (s) return s;
-    s = timed("wirelength", d.n_net_tasks > 0, 28.0 * npin + 16.0 * d.n_net_tasks, 0.0,
+    s = timed("wirelength", d.n_net_tasks > 0, (12.0 + 16.0 * q) * npin + 16.0 * d.n_net_tasks, 0.0,
               [&] { launch_wirelength(e->kc, d, e->pin_grad, e->S, e->st); }, nothing);
     if (s) return s;
     if (d.n_big_objs > 0) {
@@ -1546,13 +1760,13 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
                   [&] { launch_gather_big(e->kc, d, e->field, e->gd_big, e->S, e->st); }, nothing);
         if (s) return s;
     }
-    s = timed("combine", 1, 85.0 * nobj + 12.0 * npin, 0.0,
+    s = timed("combine", 1, (29.0 + 56.0 * q) * nobj + (4.0 + 8.0 * q) * npin, 0.0,
               [&] {
                   launch_combine(e->kc, d, e->field, e->gd_big, e->pin_grad, e->g, e->g_prev,
                                  e->y_prev, nullptr, nullptr, 1, e->S, e->st);
               }, nothing);
     if (s) return s;
-    s = timed("update", 1, 65.0 * nobj, 0.0,
+    s = timed("update", 1, (9.0 + 56.0 * q) * nobj, 0.0,
               [&] { launch_update(e->kc, d, e->pos, e->x, e->g, e->y_prev, e->g_prev, e->S, e->st); },
               [&] {
                   // a pending stop would make the following repetitions no-ops
@@ -1562,7 +1776,7 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     for (int k = 0; k < 5; k++)
-        CK(cudaMemcpyAsync(bufs[k], keep[k].data(), sizeof(float2) * no, cudaMemcpyHostToDevice, e->st));
+        CK(cudaMemcpyAsync(bufs[k], keep[k].data(), e->v2 * no, cudaMemcpyHostToDevice, e->st));
     *e->hS = saved;
     CK(cudaMemcpyAsync(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice, e->st));
     if (!keep_maps) zero_maps();
@@ -1621,10 +1835,10 @@ ep_status qp_read(ep_engine *e, int n) {
 }
 
 // Build both systems at the current centres: count, prefix sum, fill.
-ep_status qp_build(ep_engine *e) {
+ep_status qp_build(ep_engine *e, const float2 *qpos) {
     QpDev &q = e->qp;
     const int nn = q.nn;
-    qp_rows(q, 0, e->pos, e->st);
+    qp_rows(q, 0, qpos, e->st);
     std::vector<int32_t> cnt(2 * (size_t)nn), rx(nn + 1), ry(nn + 1);
     CK(cudaMemcpyAsync(cnt.data(), q.count, cnt.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, e->st));
     CK(cudaStreamSynchronize(e->st));
@@ -1639,7 +1853,7 @@ ep_status qp_build(ep_engine *e) {
     }
     CK(cudaMemcpyAsync(q.row_x, rx.data(), rx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
     CK(cudaMemcpyAsync(q.row_y, ry.data(), ry.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
-    qp_rows(q, 1, e->pos, e->st);
+    qp_rows(q, 1, qpos, e->st);
     CK(cudaStreamSynchronize(e->st));  // the host vectors above go out of scope
     CK(cudaGetLastError());
     return EP_OK;
@@ -1650,11 +1864,11 @@ ep_status qp_build(ep_engine *e) {
 // |r|^2 <= (eps |b|)^2 with eps the float epsilon, or after max_it
 // iterations; the current centres are the initial guess.  err[c] = |r|/|b|
 // at the end, the value QPPlacer reads as solver.error().
-ep_status qp_solve(ep_engine *e, int max_it, double err[2], int &iters) {
+ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, double err[2], int &iters) {
     QpDev &q = e->qp;
     cudaStream_t st = e->st;
     const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
-    qp_to_x(q, e->pos, st);
+    qp_to_x(q, qpos, st);
     qp_init(q, st);
     ep_status s = qp_read(e, 4);
     if (s) return s;
@@ -1743,27 +1957,34 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp
     if (s) return s;
     QpDev &q = e->qp;
     cudaStream_t st = e->st;
+    // the quadratic placement works on FP32 centres; an FP64 engine's centres
+    // (terminals included) are rounded into qp_pos and the result copied back
+    const int ncent = e->n_obj + e->n_terms;
+    if (e->fp64 && !e->qp_pos && (s = dalloc(e, e->qp_pos, ncent))) return s;
+    float2 *qpos = e->fp64 ? e->qp_pos : (float2 *)e->pos;
+    if (e->fp64) k_convert2<double, float><<<(ncent + 255) / 256, 256, 0, st>>>((const double2 *)e->pos, qpos, ncent);
     const int max_outer = max_iterations > 0 ? max_iterations : 20;  // IPiteCount, default 20
     const double target_error = 0.000001;                           // qplace.cpp:47
     CK(cudaEventRecord(e->ev0, st));
-    qp_center(q, e->grid, e->size, e->pos, st);  // moveNodesCenterToCenter
-    qp_bounds(q, e->pos, q.out, st);
+    qp_center(q, e->grid, e->size, qpos, st);  // moveNodesCenterToCenter
+    qp_bounds(q, qpos, q.out, st);
     if ((s = qp_read(e, 1))) return s;
     double hpwl = e->qp_out_h[0], err[2] = {0, 0};
     int outer = 0, solver_iters = 0;
     for (int i = 0;; i++) {
-        if ((s = qp_build(e))) return s;
+        if ((s = qp_build(e, qpos))) return s;
         int it = 0;
-        if ((s = qp_solve(e, 100, err, it))) return s;  // solver.setMaxIterations(100)
+        if ((s = qp_solve(e, qpos, 100, err, it))) return s;  // solver.setMaxIterations(100)
         solver_iters += it;
-        qp_from_x(q, e->grid, e->size, e->pos, st);  // updateModuleLocation
-        qp_bounds(q, e->pos, q.out, st);             // calcNetBoundPins
+        qp_from_x(q, e->grid, e->size, qpos, st);  // updateModuleLocation
+        qp_bounds(q, qpos, q.out, st);             // calcNetBoundPins
         if ((s = qp_read(e, 1))) return s;
         hpwl = e->qp_out_h[0];
         outer = i + 1;
         if (std::fabs(err[0]) < target_error && std::fabs(err[1]) < target_error && i > 4) break;
         if (i >= max_outer) break;
     }
+    if (e->fp64) k_convert2<float, double><<<(ncent + 255) / 256, 256, 0, st>>>(qpos, (double2 *)e->pos, ncent);
     CK(cudaEventRecord(e->ev1, st));
     CK(cudaEventSynchronize(e->ev1));
     e->initialized = false;  // the gradient state belongs to the old positions

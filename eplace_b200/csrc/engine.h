@@ -69,6 +69,9 @@ constexpr int kSmallObjectBins = 16;
 struct DctPlan {
     int nx = 0, ny = 0;
     int mode = 0;  // ep_dct_mode
+    int fp64 = 0;  // maps in double (fast transforms only)
+    // polls of a tensor-core pipeline wait before it gives up (ep_set_limits)
+    unsigned wait_limit = 1u << 22;
     // FP32 operand tables (see dct.cu for their definitions)
     float *Cy = nullptr, *Cx = nullptr, *K = nullptr, *B3 = nullptr, *A4 = nullptr;
     // intermediates
@@ -79,12 +82,13 @@ struct DctPlan {
     void *fft = nullptr;
 };
 
-int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode,
+// fp64: the plan works on double maps (fast transforms only).
+int dct_plan_init(DctPlan &p, int nx, int ny, float step_x, float step_y, int mode, int fp64,
                   std::string &err);
 void dct_plan_free(DctPlan &p);
-// rho (fp32 [nx][ny]) -> field (float2 [nx][ny]) and, when phi != nullptr, phi.
-int dct_run(DctPlan &p, const float *rho, float2 *field, float *phi, const DevScalars *S,
-            cudaStream_t st);
+// rho (R [nx][ny]) -> field (vec2<R> [nx][ny]) and, when phi != nullptr, phi
+// (R [nx][ny]); R = double when the plan was made with fp64, else float.
+int dct_run(DctPlan &p, const void *rho, void *field, void *phi, const DevScalars *S, cudaStream_t st);
 // Kernel launches of one dct_run.
 inline int dct_launches(const DctPlan &p) { return p.mode == EP_DCT_FFT ? 3 : 4; }
 // The tensor-core path reads rho as bf16 hi/lo planes written by the prep kernel.
@@ -94,7 +98,7 @@ void *dct_tc_rho_planes(DctPlan &p);
 struct DeviceNetlist {
     int n_obj, n_nodes, n_terms;
     int n_nets, n_pins;
-    const float2 *pos;       // [n_obj + n_terms] centres; terminals after objects
+    const void *pos;         // [n_obj + n_terms] centres (vec2<R>); terminals after objects
     const float2 *size;      // [n_obj] (w, h)
     const uint8_t *flags;    // [n_obj]
     const float *npins;      // [n_obj] pin count (float, as the preconditioner reads it)
@@ -120,6 +124,7 @@ struct KernelCtx {
     double bin_area, inv_bin_area;
     double area_norm;  // stdArea + macroArea * td (overflow denominator)
     int exact_exp, lse;
+    int fp64;           // working precision of the loop: 0 = FP32 (mixed), 1 = FP64
     int want_wl_value;  // also sum the smooth wirelength value (off in the hot loop)
     // per-block partials of the deterministic grid reductions
     double *part_prep, *part_wl, *part_comb, *part_hp;
@@ -135,40 +140,38 @@ void set_sgemm_carveout(int carveout);
 // grid sizes of the reductions: 0 = per-net passes (both kernels), 1 = combine
 int reduction_blocks(const DeviceNetlist &d, int which);
 
+// Vectors typed void * hold vec2<R> (float2 / double2, KernelCtx::fp64) and
+// rho holds R.
 void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, unsigned long long *node_q,
                     unsigned long long *filler_q, const DevScalars *S, cudaStream_t st);
 void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long long *filler_q,
-                 const float2 *static_map, float *rho, void *rho_bf16, float *node_f,
+                 const float2 *static_map, void *rho, void *rho_bf16, float *node_f,
                  float *filler_f, int zero_maps, DevScalars *S, cudaStream_t st);
-void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad,
-                       DevScalars *S, cudaStream_t st);
-void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
-                       float2 *gd_big, const DevScalars *S, cudaStream_t st);
-void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
-                    const float2 *gd_big, const float2 *pin_grad, float2 *g, const float2 *g_prev,
-                    const float2 *y_prev, float2 *dump_gd, float2 *dump_gwl, int stepping,
-                    DevScalars *S, cudaStream_t st);
-void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
-                   const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S, cudaStream_t st);
+void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, void *pin_grad, DevScalars *S,
+                       cudaStream_t st);
+void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const void *field, void *gd_big,
+                       const DevScalars *S, cudaStream_t st);
+void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const void *field, const void *gd_big,
+                    const void *pin_grad, void *g, const void *g_prev, const void *y_prev, void *dump_gd,
+                    void *dump_gwl, int stepping, DevScalars *S, cudaStream_t st);
+void launch_update(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g, void *y_prev,
+                   void *g_prev, DevScalars *S, cudaStream_t st);
 // The update of the captured loop: also scatters the new positions into the
 // (clear) density maps for the next evaluation, unless the step ends the stage.
-void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
-                           const float2 *g, float2 *y_prev, float2 *g_prev, unsigned long long *node_q,
-                           unsigned long long *filler_q, DevScalars *S, cudaStream_t st);
+void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g,
+                           void *y_prev, void *g_prev, unsigned long long *node_q, unsigned long long *filler_q,
+                           DevScalars *S, cudaStream_t st);
 // Backtracking step rule: one trial move from y_k (ysave) along g_k, and the
 // scalar commit of an accepted trial (combine in stepping mode 2 decides).
-void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const float2 *ysave, const float2 *g,
-                       const float2 *x, float2 *pos, float2 *xtrial, const DevScalars *S,
-                       cudaStream_t st);
+void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const void *ysave, const void *g, const void *x,
+                       void *pos, void *xtrial, const DevScalars *S, cudaStream_t st);
 void launch_bktrk_commit(DevScalars *S, cudaStream_t st);
-void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
+void launch_stage_begin(const KernelCtx &c, const DeviceNetlist &d, const void *pos, void *x, DevScalars *S,
                         cudaStream_t st);
-void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, const float2 *x,
-                    cudaStream_t st);
+void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, void *pos, const void *x, cudaStream_t st);
 // HPWL at the current positions; mode 0 stores it, mode 1 also applies the
 // updatePenaltyFactor rule, mode 2 applies it only if a lambda update is pending.
-void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
-                 cudaStream_t st);
+void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S, cudaStream_t st);
 
 // ---- quadratic placement (qp.cu) ---------------------------------------------
 // Device view of one engine's quadratic placement: the netlist in device pin

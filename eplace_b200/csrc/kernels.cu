@@ -19,10 +19,14 @@
 //             (x_{k+1}-x_k), clamp into the core (PlaceDB/placedb.cpp:253-288)
 //
 // Every kernel of the loop returns at once when S->done is set, so a captured
-// multi-iteration graph stops doing work after the stop condition.
+// multi-iteration graph stops doing work after the stop condition.  Each is a
+// template on the working precision R (float: the engine's mixed-precision
+// form, whose arithmetic follows the reference's float steps; double: the
+// plain FP64 form); the launchers pick the instance from KernelCtx::fp64.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <iterator>
 #include <mutex>
 #include <vector>
 
@@ -37,71 +41,79 @@ constexpr int kPinChunk = 128;  // pin gradients a warp of the combine kernel st
 
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 
+using ull = unsigned long long;
+
+__device__ __forceinline__ float exact_exp(float a) { return expf(a); }
+__device__ __forceinline__ double exact_exp(double a) { return exp(a); }
+__device__ __forceinline__ float warp_sum_r(float v) { return warp_sum_f(v); }
+__device__ __forceinline__ double warp_sum_r(double v) { return warp_sum(v); }
+
 // ---------------------------------------------------------------- scatter --
-__device__ __forceinline__ void scatter_one(const Grid &g, const Rect &r, float scale, int i,
-                                            int j, double qscale,
-                                            unsigned long long *__restrict__ map) {
-    float ovl = (float)rect_bin_overlap(g, r, i, j);
-    if (ovl == 0.0f) return;
-    float c = __fmul_rn(scale, ovl);
+template <typename R>
+__device__ __forceinline__ void scatter_one(const Grid &g, const RectT<R> &r, R scale, int i, int j, double qscale,
+                                            ull *__restrict__ map) {
+    R ovl = (R)rect_bin_overlap<R>(g, r, i, j);
+    if (ovl == (R)0) return;
+    R c = mul_rn(scale, ovl);
     long long q = __double2ll_rn(__dmul_rn((double)c, qscale));
-    atomicAdd(&map[(size_t)i * g.ny + j], (unsigned long long)q);
+    atomicAdd(&map[(size_t)i * g.ny + j], (ull)q);
 }
 
 // Contribution scale: sx*sy, times the target density for macros
-// (EPlace/eplace.cpp:1114-1128, evaluated left to right in float).
-__device__ __forceinline__ float contrib_scale(const Rect &r, uint8_t f, float td) {
-    float s = __fmul_rn(r.sx, r.sy);
-    return (f & kMacro) ? __fmul_rn(s, td) : s;
+// (EPlace/eplace.cpp:1114-1128, evaluated left to right).
+template <typename R>
+__device__ __forceinline__ R contrib_scale(const RectT<R> &r, uint8_t f, float td) {
+    R s = mul_rn(r.sx, r.sy);
+    return (f & kMacro) ? mul_rn(s, (R)td) : s;
 }
 
 // One object of the thread-per-object path (kBig objects excluded).
-__device__ __forceinline__ void scatter_small_object(const Grid &g, float2 p, float2 s, uint8_t f, double qscale,
-                                                     unsigned long long *__restrict__ node_q,
-                                                     unsigned long long *__restrict__ filler_q) {
-    Rect r = object_rect(g, p.x, p.y, s.x, s.y);
+template <typename R>
+__device__ __forceinline__ void scatter_small_object(const Grid &g, vec2<R> p, float2 s, uint8_t f, double qscale,
+                                                     ull *__restrict__ node_q, ull *__restrict__ filler_q) {
+    RectT<R> r = object_rect(g, p.x, p.y, (R)s.x, (R)s.y);
     int i0, i1, j0, j1;
-    bin_range(g, r, i0, i1, j0, j1);
-    float scale = contrib_scale(r, f, g.td);
-    unsigned long long *map = (f & kFiller) ? filler_q : node_q;
+    bin_range<R>(g, r, i0, i1, j0, j1);
+    R scale = contrib_scale<R>(r, f, g.td);
+    ull *map = (f & kFiller) ? filler_q : node_q;
     for (int i = i0; i <= i1; i++)
-        for (int j = j0; j <= j1; j++) scatter_one(g, r, scale, i, j, qscale, map);
+        for (int j = j0; j <= j1; j++) scatter_one<R>(g, r, scale, i, j, qscale, map);
 }
 
 // One kBig object by a whole block, its bins strided over the threads.
-__device__ __forceinline__ void scatter_big_object(const Grid &g, float2 p, float2 s, uint8_t f, double qscale,
-                                                   unsigned long long *__restrict__ node_q,
-                                                   unsigned long long *__restrict__ filler_q) {
-    Rect r = object_rect(g, p.x, p.y, s.x, s.y);
+template <typename R>
+__device__ __forceinline__ void scatter_big_object(const Grid &g, vec2<R> p, float2 s, uint8_t f, double qscale,
+                                                   ull *__restrict__ node_q, ull *__restrict__ filler_q) {
+    RectT<R> r = object_rect(g, p.x, p.y, (R)s.x, (R)s.y);
     int i0, i1, j0, j1;
-    bin_range(g, r, i0, i1, j0, j1);
+    bin_range<R>(g, r, i0, i1, j0, j1);
     if (i1 < i0 || j1 < j0) return;
-    float scale = contrib_scale(r, f, g.td);
-    unsigned long long *map = (f & kFiller) ? filler_q : node_q;
+    R scale = contrib_scale<R>(r, f, g.td);
+    ull *map = (f & kFiller) ? filler_q : node_q;
     const int wy = j1 - j0 + 1, nb = (i1 - i0 + 1) * wy;
     for (int t = threadIdx.x; t < nb; t += blockDim.x)
-        scatter_one(g, r, scale, i0 + t / wy, j0 + t % wy, qscale, map);
+        scatter_one<R>(g, r, scale, i0 + t / wy, j0 + t % wy, qscale, map);
 }
 
 // Blocks [0, small_blocks): thread per object; the blocks after them: one
 // kBig object each.
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
-k_scatter(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
+k_scatter(Grid g, const vec2<R> *__restrict__ pos, const float2 *__restrict__ size,
           const uint8_t *__restrict__ flags, int n, int small_blocks, const int32_t *__restrict__ big,
-          double qscale, unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
-          const DevScalars *__restrict__ S) {
+          double qscale, ull *__restrict__ node_q, ull *__restrict__ filler_q, const DevScalars *__restrict__ S) {
     pdl_begin();
     if (S->done) return;
     if ((int)blockIdx.x >= small_blocks) {
         const int o = big[blockIdx.x - small_blocks];
-        scatter_big_object(g, pos[o], size[o], flags[o], qscale, node_q, filler_q);
+        scatter_big_object<R>(g, pos[o], size[o], flags[o], qscale, node_q, filler_q);
         return;
     }
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     const uint8_t f = flags[o];
     if (f & kBig) return;
-    scatter_small_object(g, pos[o], size[o], f, qscale, node_q, filler_q);
+    scatter_small_object<R>(g, pos[o], size[o], f, qscale, node_q, filler_q);
 }
 
 // ------------------------------------------------------------------- prep --
@@ -125,11 +137,11 @@ __device__ __forceinline__ void inv_gamma(double tau_d, float sx, float sy, doub
     gy = by;
 }
 
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
-k_prep(Grid g, unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
-       const float2 *__restrict__ stat, float *__restrict__ rho, uint16_t *__restrict__ rho_hi,
-       uint16_t *__restrict__ rho_lo, float *__restrict__ node_f, float *__restrict__ filler_f,
-       int zero, double inv_q, double inv_bin_area, double bin_area, double area_norm,
+k_prep(Grid g, ull *__restrict__ node_q, ull *__restrict__ filler_q, const float2 *__restrict__ stat,
+       R *__restrict__ rho, uint16_t *__restrict__ rho_hi, uint16_t *__restrict__ rho_lo, float *__restrict__ node_f,
+       float *__restrict__ filler_f, int zero, double inv_q, double inv_bin_area, double bin_area, double area_norm,
        double *__restrict__ partials, DevScalars *__restrict__ S) {
     pdl_begin();
     __shared__ double sh[32];
@@ -142,15 +154,16 @@ k_prep(Grid g, unsigned long long *__restrict__ node_q, unsigned long long *__re
         float2 st = stat[k];  // (terminal, base)
         // eDensity = node + base + filler + terminal (EPlace/eplace.cpp:576-577)
         double dens = (node + (double)st.y + fill + (double)st.x) * inv_bin_area;
-        float d = (float)dens;
+        R d = (R)dens;
         if (rho) rho[k] = d;
         if (rho_hi) {
-            // 3xBF16 operand split: hi = bf16(d), lo = bf16(d - hi)
-            uint32_t u = __float_as_uint(d);
+            // 3xBF16 operand split (FP32 path only): hi = bf16(d), lo = bf16(d - hi)
+            const float df = (float)d;
+            uint32_t u = __float_as_uint(df);
             uint32_t r = u + 0x7fffu + ((u >> 16) & 1u);
             uint16_t h = (uint16_t)(r >> 16);
             float hf = __uint_as_float((uint32_t)h << 16);
-            float rem = d - hf;
+            float rem = df - hf;
             uint32_t u2 = __float_as_uint(rem);
             uint32_t r2 = u2 + 0x7fffu + ((u2 >> 16) & 1u);
             rho_hi[k] = h;
@@ -182,71 +195,77 @@ k_prep(Grid g, unsigned long long *__restrict__ node_q, unsigned long long *__re
 }
 
 // ------------------------------------------------------------- wirelength --
+template <typename R>
 struct PinCtx {
     const int32_t *__restrict__ owner;
     const float2 *__restrict__ off;
-    const float2 *__restrict__ pos;
+    const vec2<R> *__restrict__ pos;
 };
 
-// Pin::calculateAbsolutePos: centre + offset in float.
-__device__ __forceinline__ float2 pin_xy(const PinCtx &c, int p) {
+// Pin::calculateAbsolutePos: centre + offset.
+template <typename R>
+__device__ __forceinline__ vec2<R> pin_xy(const PinCtx<R> &c, int p) {
     float2 o = c.off[p];
-    float2 q = c.pos[c.owner[p]];
-    return make_float2(__fadd_rn(q.x, o.x), __fadd_rn(q.y, o.y));
+    vec2<R> q = c.pos[c.owner[p]];
+    return mk2<R>(add_rn(q.x, (R)o.x), add_rn(q.y, (R)o.y));
 }
 
+template <typename R>
 struct NetSums {
-    float nmx, dmx, nnx, dnx, nmy, dmy, nny, dny;
+    R nmx, dmx, nnx, dnx, nmy, dmy, nny, dny;
 };
 
 // Exponential terms of one pin (calcWirelengthWA_2D, objects.cpp:275-332):
 // arguments <= -300 make the term zero.
+template <typename R>
 struct PinExp {
-    float emx, enx, emy, eny;
+    R emx, enx, emy, eny;
 };
 
-template <bool EXACT>
-__device__ __forceinline__ float term_exp(float a) {
-    if (!(a > (float)kNegMaxExp)) return 0.0f;
-    return EXACT ? expf(a) : fast_exp(a);
+template <bool EXACT, typename R>
+__device__ __forceinline__ R term_exp(R a) {
+    if (!(a > (R)kNegMaxExp)) return (R)0;
+    return EXACT ? exact_exp(a) : fast_exp<R>(a);
 }
 
-template <bool EXACT>
-__device__ __forceinline__ PinExp pin_exps(float2 xy, float x1, float x0, float y1, float y0, float igx,
-                                           float igy) {
-    PinExp e;
-    e.emx = term_exp<EXACT>(__fmul_rn(__fsub_rn(xy.x, x1), igx));
-    e.enx = term_exp<EXACT>(__fmul_rn(__fsub_rn(x0, xy.x), igx));
-    e.emy = term_exp<EXACT>(__fmul_rn(__fsub_rn(xy.y, y1), igy));
-    e.eny = term_exp<EXACT>(__fmul_rn(__fsub_rn(y0, xy.y), igy));
+template <bool EXACT, typename R>
+__device__ __forceinline__ PinExp<R> pin_exps(vec2<R> xy, R x1, R x0, R y1, R y0, R igx, R igy) {
+    PinExp<R> e;
+    e.emx = term_exp<EXACT, R>(mul_rn(sub_rn(xy.x, x1), igx));
+    e.enx = term_exp<EXACT, R>(mul_rn(sub_rn(x0, xy.x), igx));
+    e.emy = term_exp<EXACT, R>(mul_rn(sub_rn(xy.y, y1), igy));
+    e.eny = term_exp<EXACT, R>(mul_rn(sub_rn(y0, xy.y), igy));
     return e;
 }
 
 // Add one pin's terms to a running sum set (calcWirelengthWA_2D's sums).
-__device__ __forceinline__ void add_terms(float (&s)[8], const PinExp &e, float2 xy) {
-    s[0] = __fadd_rn(s[0], __fmul_rn(xy.x, e.emx));
-    s[1] = __fadd_rn(s[1], e.emx);
-    s[2] = __fadd_rn(s[2], __fmul_rn(xy.x, e.enx));
-    s[3] = __fadd_rn(s[3], e.enx);
-    s[4] = __fadd_rn(s[4], __fmul_rn(xy.y, e.emy));
-    s[5] = __fadd_rn(s[5], e.emy);
-    s[6] = __fadd_rn(s[6], __fmul_rn(xy.y, e.eny));
-    s[7] = __fadd_rn(s[7], e.eny);
+template <typename R>
+__device__ __forceinline__ void add_terms(R (&s)[8], const PinExp<R> &e, vec2<R> xy) {
+    s[0] = add_rn(s[0], mul_rn(xy.x, e.emx));
+    s[1] = add_rn(s[1], e.emx);
+    s[2] = add_rn(s[2], mul_rn(xy.x, e.enx));
+    s[3] = add_rn(s[3], e.enx);
+    s[4] = add_rn(s[4], mul_rn(xy.y, e.emy));
+    s[5] = add_rn(s[5], e.emy);
+    s[6] = add_rn(s[6], mul_rn(xy.y, e.eny));
+    s[7] = add_rn(s[7], e.eny);
 }
 
 // Per-net factors of the gradient: 1 / (sum of exponentials) and the
 // exponentially weighted mean coordinate of each of the four terms.  Every
 // denominator holds the bound pin's exp(0) = 1, so it is >= 1.
+template <typename R>
 struct NetCoef {
-    float rmx, mmx, rnx, mnx, rmy, mmy, rny, mny;
+    R rmx, mmx, rnx, mnx, rmy, mmy, rny, mny;
 };
 
-__device__ __forceinline__ NetCoef net_coef(const NetSums &s) {
-    NetCoef c;
-    c.rmx = __frcp_rn(s.dmx);
-    c.rnx = __frcp_rn(s.dnx);
-    c.rmy = __frcp_rn(s.dmy);
-    c.rny = __frcp_rn(s.dny);
+template <typename R>
+__device__ __forceinline__ NetCoef<R> net_coef(const NetSums<R> &s) {
+    NetCoef<R> c;
+    c.rmx = rcp_rn(s.dmx);
+    c.rnx = rcp_rn(s.dnx);
+    c.rmy = rcp_rn(s.dmy);
+    c.rny = rcp_rn(s.dny);
     c.mmx = s.nmx * c.rmx;
     c.mnx = s.nnx * c.rnx;
     c.mmy = s.nmy * c.rmy;
@@ -261,20 +280,18 @@ __device__ __forceinline__ NetCoef net_coef(const NetSums &s) {
 // avoids the cancellation of the expanded quotient (the two agree to the
 // reference's own rounding).  A zero exponential (argument <= -300) gives a
 // zero term as in the reference.  LSE (:423-437): e / d per term.
-template <bool LSE>
-__device__ __forceinline__ float2 pin_gradient(const PinExp &e, float2 xy, float igx, float igy,
-                                               const NetCoef &c) {
-    if (LSE)
-        return make_float2(e.emx * c.rmx - e.enx * c.rnx, e.emy * c.rmy - e.eny * c.rny);
-    const float gmx = e.emx * c.rmx * fmaf(igx, xy.x - c.mmx, 1.0f);
-    const float gnx = e.enx * c.rnx * fmaf(-igx, xy.x - c.mnx, 1.0f);
-    const float gmy = e.emy * c.rmy * fmaf(igy, xy.y - c.mmy, 1.0f);
-    const float gny = e.eny * c.rny * fmaf(-igy, xy.y - c.mny, 1.0f);
-    return make_float2(gmx - gnx, gmy - gny);
+template <bool LSE, typename R>
+__device__ __forceinline__ vec2<R> pin_gradient(const PinExp<R> &e, vec2<R> xy, R igx, R igy, const NetCoef<R> &c) {
+    if (LSE) return mk2<R>(e.emx * c.rmx - e.enx * c.rnx, e.emy * c.rmy - e.eny * c.rny);
+    const R gmx = e.emx * c.rmx * fma_r(igx, xy.x - c.mmx, (R)1);
+    const R gnx = e.enx * c.rnx * fma_r(-igx, xy.x - c.mnx, (R)1);
+    const R gmy = e.emy * c.rmy * fma_r(igy, xy.y - c.mmy, (R)1);
+    const R gny = e.eny * c.rny * fma_r(-igy, xy.y - c.mny, (R)1);
+    return mk2<R>(gmx - gnx, gmy - gny);
 }
 
-__device__ __forceinline__ double net_value(const NetSums &s, float x1, float x0, float y1,
-                                            float y0, float igx, float igy, bool lse) {
+template <typename R>
+__device__ __forceinline__ double net_value(const NetSums<R> &s, R x1, R x0, R y1, R y0, R igx, R igy, bool lse) {
     if (lse)
         return ((double)x1 - x0 + log((double)s.dmx) / igx + log((double)s.dnx) / igx) +
                ((double)y1 - y0 + log((double)s.dmy) / igy + log((double)s.dny) / igy);
@@ -292,7 +309,7 @@ __device__ __forceinline__ double lambda_multiplier(double cur, double last) {
 __device__ void finish_wirelength(DevScalars *S, double hp, double wl) {
     S->wirelength = wl;
     S->hpwl = hp;
-    // atomic: the Poisson GEMMs, running beside this pass, may raise a bit too
+    // atomic: the Poisson solve, running beside this pass, may raise a bit too
     if (!isfinite(hp)) atomicOr(&S->status, 1 << EP_ERR_NAN);
     if (S->lambda_pending) {
         S->lambda *= lambda_multiplier(hp, S->last_hpwl);
@@ -323,12 +340,12 @@ __device__ void finish_hpwl(DevScalars *S, double hp, int mode) {
 //   D >  kWarpPins: one net; the warp strides over its pins, keeping the
 //       first kStagedPins of them in shared memory between the passes.
 // Nets above kWarpPins pins come first (largest first), then degree 32 down
-// to 1, so the long tasks start early.  The sums are FP32 as in
-// Net::calcWirelengthWA_2D, added in a fixed tree order instead of pin order
-// (a few ulps apart).  Pin gradients are written in device pin order
-// (coalesced); the combine kernel gathers them back in each object's
-// reference pin order.  WL = false computes only the HPWL with the same
-// layout and reduction tree, so both passes give bitwise the same HPWL.
+// to 1, so the long tasks start early.  The sums are in the working precision
+// as in Net::calcWirelengthWA_2D (float there), added in a fixed tree order
+// instead of pin order (a few ulps apart).  Pin gradients are written in
+// device pin order (coalesced); the combine kernel gathers them back in each
+// object's reference pin order.  WL = false computes only the HPWL with the
+// same layout and reduction tree, so both passes give bitwise the same HPWL.
 struct NetOut {
     double hpwl, value;
 };
@@ -338,132 +355,132 @@ constexpr unsigned kFull = 0xffffffffu;
 // Bound pins of each aligned segment of D lanes (segment base `base`, this
 // lane's index k in it); every lane of the segment gets them.  The windows
 // double cyclically, which is exact for max / min.
-__device__ __forceinline__ void seg_bounds(float &x1, float &x0, float &y1, float &y0, int D,
-                                           int base, int k) {
+template <typename R>
+__device__ __forceinline__ void seg_bounds(R &x1, R &x0, R &y1, R &y0, int D, int base, int k) {
     for (int o = 1; o < D; o <<= 1) {
         const int j = k + o;
         const int src = base + (j < D ? j : j - D);
-        x1 = fmaxf(x1, __shfl_sync(kFull, x1, src));
-        x0 = fminf(x0, __shfl_sync(kFull, x0, src));
-        y1 = fmaxf(y1, __shfl_sync(kFull, y1, src));
-        y0 = fminf(y0, __shfl_sync(kFull, y0, src));
+        x1 = max_r(x1, __shfl_sync(kFull, x1, src));
+        x0 = min_r(x0, __shfl_sync(kFull, x0, src));
+        y1 = max_r(y1, __shfl_sync(kFull, y1, src));
+        y0 = min_r(y0, __shfl_sync(kFull, y0, src));
     }
 }
 
 // The eight exponential sums of each segment, every lane of the segment gets
 // bitwise the same totals: a butterfly when D is a power of two, else a tree
 // into the segment's first lane and a broadcast.
-__device__ __forceinline__ void seg_sums(float (&s)[8], int D, int base, int k) {
+template <typename R>
+__device__ __forceinline__ void seg_sums(R (&s)[8], int D, int base, int k) {
     if ((D & (D - 1)) == 0) {
         for (int o = D >> 1; o > 0; o >>= 1)
 #pragma unroll
-            for (int i = 0; i < 8; i++) s[i] = __fadd_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
+            for (int i = 0; i < 8; i++) s[i] = add_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
         return;
     }
     for (int o = 1; o < D; o <<= 1) {
         const bool take = k + o < D;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const float t = __shfl_down_sync(kFull, s[i], o);
-            if (take) s[i] = __fadd_rn(s[i], t);
+            const R t = __shfl_down_sync(kFull, s[i], o);
+            if (take) s[i] = add_rn(s[i], t);
         }
     }
 #pragma unroll
     for (int i = 0; i < 8; i++) s[i] = __shfl_sync(kFull, s[i], base);
 }
 
-__device__ __forceinline__ NetSums net_sums(const float (&s)[8]) {
-    return NetSums{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7]};
+template <typename R>
+__device__ __forceinline__ NetSums<R> net_sums(const R (&s)[8]) {
+    return NetSums<R>{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7]};
 }
 
 // Nets of degree D <= 32 packed on the lanes of one warp.
-template <bool WL, bool EXACT, bool LSE>
-__device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const PinCtx &pc,
-                                               float2 *__restrict__ out, float igx, float igy,
-                                               int want_value) {
+template <bool WL, bool EXACT, bool LSE, typename R>
+__device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const PinCtx<R> &pc, vec2<R> *__restrict__ out,
+                                               R igx, R igy, int want_value) {
     const int D = t.x, p0 = t.y;
     const int seg = (lane * t.w) >> 16, base = seg * D, k = lane - base;
     const bool act = seg < t.z;
-    const float2 xy = act ? pin_xy(pc, p0 + lane) : make_float2(0.f, 0.f);
+    const vec2<R> xy = act ? pin_xy<R>(pc, p0 + lane) : mk2<R>((R)0, (R)0);
     // bound pins (Net::calcBoundPin, PlaceCommon/objects.cpp:75-144)
-    float x1 = xy.x, x0 = xy.x, y1 = xy.y, y0 = xy.y;
-    seg_bounds(x1, x0, y1, y0, D, base, k);
+    R x1 = xy.x, x0 = xy.x, y1 = xy.y, y0 = xy.y;
+    seg_bounds<R>(x1, x0, y1, y0, D, base, k);
     NetOut r{0.0, 0.0};
     if (act && k == 0) r.hpwl = ((double)x1 - (double)x0) + ((double)y1 - (double)y0);
     if (WL) {
-        const PinExp e = pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy);
-        float s[8] = {__fmul_rn(xy.x, e.emx), e.emx, __fmul_rn(xy.x, e.enx), e.enx,
-                      __fmul_rn(xy.y, e.emy), e.emy, __fmul_rn(xy.y, e.eny), e.eny};
-        seg_sums(s, D, base, k);
-        const NetSums ns = net_sums(s);
-        if (act) out[p0 + lane] = pin_gradient<LSE>(e, xy, igx, igy, net_coef(ns));
-        if (want_value && act && k == 0) r.value = net_value(ns, x1, x0, y1, y0, igx, igy, LSE);
+        const PinExp<R> e = pin_exps<EXACT, R>(xy, x1, x0, y1, y0, igx, igy);
+        R s[8] = {mul_rn(xy.x, e.emx), e.emx, mul_rn(xy.x, e.enx), e.enx,
+                  mul_rn(xy.y, e.emy), e.emy, mul_rn(xy.y, e.eny), e.eny};
+        seg_sums<R>(s, D, base, k);
+        const NetSums<R> ns = net_sums<R>(s);
+        if (act) out[p0 + lane] = pin_gradient<LSE, R>(e, xy, igx, igy, net_coef<R>(ns));
+        if (want_value && act && k == 0) r.value = net_value<R>(ns, x1, x0, y1, y0, igx, igy, LSE);
     }
     return r;
 }
 
 // One net of D > 32 pins on one warp; `stage` holds kStagedPins pin positions.
-template <bool WL, bool EXACT, bool LSE>
-__device__ __forceinline__ NetOut net_in_warp(const int4 t, int lane, const PinCtx &pc,
-                                              float2 *__restrict__ out, float igx, float igy,
-                                              int want_value, float2 *__restrict__ stage) {
+template <bool WL, bool EXACT, bool LSE, typename R>
+__device__ __forceinline__ NetOut net_in_warp(const int4 t, int lane, const PinCtx<R> &pc, vec2<R> *__restrict__ out,
+                                              R igx, R igy, int want_value, vec2<R> *__restrict__ stage) {
     const int D = t.x, p0 = t.y;
-    float x1 = -3.4e38f, x0 = 3.4e38f, y1 = -3.4e38f, y0 = 3.4e38f;
+    R x1 = (R)-3.4e38f, x0 = (R)3.4e38f, y1 = (R)-3.4e38f, y0 = (R)3.4e38f;
 #pragma unroll 4
     for (int k = lane; k < D; k += 32) {
-        const float2 xy = pin_xy(pc, p0 + k);
+        const vec2<R> xy = pin_xy<R>(pc, p0 + k);
         if (k < kStagedPins) stage[k] = xy;  // read back by this lane only
-        x1 = fmaxf(x1, xy.x);
-        x0 = fminf(x0, xy.x);
-        y1 = fmaxf(y1, xy.y);
-        y0 = fminf(y0, xy.y);
+        x1 = max_r(x1, xy.x);
+        x0 = min_r(x0, xy.x);
+        y1 = max_r(y1, xy.y);
+        y0 = min_r(y0, xy.y);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        x1 = fmaxf(x1, __shfl_xor_sync(kFull, x1, o));
-        x0 = fminf(x0, __shfl_xor_sync(kFull, x0, o));
-        y1 = fmaxf(y1, __shfl_xor_sync(kFull, y1, o));
-        y0 = fminf(y0, __shfl_xor_sync(kFull, y0, o));
+        x1 = max_r(x1, __shfl_xor_sync(kFull, x1, o));
+        x0 = min_r(x0, __shfl_xor_sync(kFull, x0, o));
+        y1 = max_r(y1, __shfl_xor_sync(kFull, y1, o));
+        y0 = min_r(y0, __shfl_xor_sync(kFull, y0, o));
     }
     NetOut r{lane == 0 ? ((double)x1 - (double)x0) + ((double)y1 - (double)y0) : 0.0, 0.0};
     if (WL) {
-        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        R s[8] = {(R)0, (R)0, (R)0, (R)0, (R)0, (R)0, (R)0, (R)0};
         for (int k = lane; k < D; k += 32) {
-            const float2 xy = k < kStagedPins ? stage[k] : pin_xy(pc, p0 + k);
-            add_terms(s, pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy), xy);
+            const vec2<R> xy = k < kStagedPins ? stage[k] : pin_xy<R>(pc, p0 + k);
+            add_terms<R>(s, pin_exps<EXACT, R>(xy, x1, x0, y1, y0, igx, igy), xy);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-            for (int i = 0; i < 8; i++) s[i] = __fadd_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
-        const NetSums ns = net_sums(s);
-        const NetCoef c = net_coef(ns);
+            for (int i = 0; i < 8; i++) s[i] = add_rn(s[i], __shfl_xor_sync(kFull, s[i], o));
+        const NetSums<R> ns = net_sums<R>(s);
+        const NetCoef<R> c = net_coef<R>(ns);
         for (int k = lane; k < D; k += 32) {
-            const float2 xy = k < kStagedPins ? stage[k] : pin_xy(pc, p0 + k);
-            out[p0 + k] = pin_gradient<LSE>(pin_exps<EXACT>(xy, x1, x0, y1, y0, igx, igy), xy, igx, igy, c);
+            const vec2<R> xy = k < kStagedPins ? stage[k] : pin_xy<R>(pc, p0 + k);
+            out[p0 + k] = pin_gradient<LSE, R>(pin_exps<EXACT, R>(xy, x1, x0, y1, y0, igx, igy), xy, igx, igy, c);
         }
-        if (want_value && lane == 0) r.value = net_value(ns, x1, x0, y1, y0, igx, igy, LSE);
+        if (want_value && lane == 0) r.value = net_value<R>(ns, x1, x0, y1, y0, igx, igy, LSE);
     }
     return r;
 }
 
-template <bool WL, bool EXACT, bool LSE>
+template <bool WL, bool EXACT, bool LSE, typename R>
 __global__ void __launch_bounds__(kNetWarps * 32)
-k_wl(const int4 *__restrict__ tasks, int n_tasks, PinCtx pc, float2 *__restrict__ out,
-     int want_value, double *__restrict__ partials, int mode, DevScalars *__restrict__ S) {
+k_wl(const int4 *__restrict__ tasks, int n_tasks, PinCtx<R> pc, vec2<R> *__restrict__ out, int want_value,
+     double *__restrict__ partials, int mode, DevScalars *__restrict__ S) {
     pdl_begin();
     __shared__ double sh[64];
-    __shared__ float2 stage[WL ? kNetWarps : 1][WL ? kStagedPins : 1];
+    __shared__ vec2<R> stage[WL ? kNetWarps : 1][WL ? kStagedPins : 1];
     if (WL && S->done) return;
-    const float igx = (float)S->inv_gamma_x, igy = (float)S->inv_gamma_y;
+    const R igx = (R)S->inv_gamma_x, igy = (R)S->inv_gamma_y;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int w = blockIdx.x * kNetWarps + wid;
     NetOut r{0.0, 0.0};
     if (w < n_tasks) {  // warp-uniform
         const int4 t = tasks[w];
-        r = t.x <= kWarpPins ? nets_in_warp<WL, EXACT, LSE>(t, lane, pc, out, igx, igy, want_value)
-                             : net_in_warp<WL, EXACT, LSE>(t, lane, pc, out, igx, igy, want_value,
-                                                           stage[WL ? wid : 0]);
+        r = t.x <= kWarpPins ? nets_in_warp<WL, EXACT, LSE, R>(t, lane, pc, out, igx, igy, want_value)
+                             : net_in_warp<WL, EXACT, LSE, R>(t, lane, pc, out, igx, igy, want_value,
+                                                              stage[WL ? wid : 0]);
     }
     // the smooth wirelength value rides along only when asked for
     bool last;
@@ -485,63 +502,86 @@ k_wl(const int4 *__restrict__ tasks, int n_tasks, PinCtx pc, float2 *__restrict_
 }
 
 // ---------------------------------------------------------------- gather --
-// Field gather (EPlace/eplace.cpp:599-674) in FP32: the same smoothed
-// rectangle and bin range as the scatter, the overlap in float, and the
-// static smoothing scale sx*sy of the object.  (The scatter keeps the
-// reference's exact FP64 overlap arithmetic because its maps are compared
-// bit for bit; the gather is compared within tolerance.)
+// Field gather (EPlace/eplace.cpp:599-674) in the working precision: the same
+// smoothed rectangle and bin range as the scatter, the overlap in R, and the
+// smoothing scale sx*sy of the object (the static FP32 table in the FP32
+// path, formed in double from the size in the FP64 path).  (The scatter
+// keeps the reference's exact FP64 overlap arithmetic because its maps are
+// compared bit for bit; the gather is compared within tolerance.)
+template <typename R>
 struct FRect {
-    float l, b, r, t;
+    R l, b, r, t;
 };
 
-__device__ __forceinline__ FRect gather_rect(const Grid &g, float2 p, float2 s, uint8_t f) {
-    const float hw = 0.5f * ((f & kSmoothX) ? g.sx : s.x);
-    const float hh = 0.5f * ((f & kSmoothY) ? g.sy : s.y);
-    return FRect{p.x - hw, p.y - hh, p.x + hw, p.y + hh};
+template <typename R>
+__device__ __forceinline__ FRect<R> gather_rect(const Grid &g, vec2<R> p, float2 s, uint8_t f) {
+    const R hw = (R)0.5 * (R)((f & kSmoothX) ? g.sx : s.x);
+    const R hh = (R)0.5 * (R)((f & kSmoothY) ? g.sy : s.y);
+    return FRect<R>{p.x - hw, p.y - hh, p.x + hw, p.y + hh};
 }
 
-__device__ __forceinline__ void gather_range(const Grid &g, const FRect &r, int &i0, int &i1, int &j0,
-                                             int &j1) {
-    i0 = max(0, (int)((r.l - g.llx) * g.isx));
-    i1 = min(g.nx - 1, (int)((r.r - g.llx) * g.isx));
-    j0 = max(0, (int)((r.b - g.lly) * g.isy));
-    j1 = min(g.ny - 1, (int)((r.t - g.lly) * g.isy));
+template <typename R>
+__device__ __forceinline__ void gather_range(const Grid &g, const FRect<R> &r, int &i0, int &i1, int &j0, int &j1) {
+    if constexpr (sizeof(R) == 4) {
+        i0 = max(0, (int)((r.l - g.llx) * g.isx));
+        i1 = min(g.nx - 1, (int)((r.r - g.llx) * g.isx));
+        j0 = max(0, (int)((r.b - g.lly) * g.isy));
+        j1 = min(g.ny - 1, (int)((r.t - g.lly) * g.isy));
+    } else {
+        i0 = max(0, (int)((r.l - (R)g.llx) / (R)g.sx));
+        i1 = min(g.nx - 1, (int)((r.r - (R)g.llx) / (R)g.sx));
+        j0 = max(0, (int)((r.b - (R)g.lly) / (R)g.sy));
+        j1 = min(g.ny - 1, (int)((r.t - (R)g.lly) / (R)g.sy));
+    }
 }
 
-__device__ __forceinline__ float2 gather_bin(const Grid &g, const FRect &r, float sxy, int i, int j,
-                                             const float2 *__restrict__ field) {
-    const float bl = fmaf((float)i, g.sx, g.llx), bb = fmaf((float)j, g.sy, g.lly);
-    const float ox = fminf(r.r, bl + g.sx) - fmaxf(r.l, bl);
-    const float oy = fminf(r.t, bb + g.sy) - fmaxf(r.b, bb);
-    if (ox <= 0.0f || oy <= 0.0f) return make_float2(0.f, 0.f);
-    const float ov = sxy * ox * oy;
-    const float2 e = field[(size_t)i * g.ny + j];
-    return make_float2(ov * e.x, ov * e.y);
+template <typename R>
+__device__ __forceinline__ R smoothing_scale(const Grid &g, float table, float2 s, uint8_t f) {
+    if constexpr (sizeof(R) == 4) {
+        return table;
+    } else {
+        const R sx = (f & kSmoothX) ? (R)s.x / (R)g.sx : (R)1;
+        const R sy = (f & kSmoothY) ? (R)s.y / (R)g.sy : (R)1;
+        return sx * sy;
+    }
 }
 
+template <typename R>
+__device__ __forceinline__ vec2<R> gather_bin(const Grid &g, const FRect<R> &r, R sxy, int i, int j,
+                                              const vec2<R> *__restrict__ field) {
+    const R bl = fma_r((R)i, (R)g.sx, (R)g.llx), bb = fma_r((R)j, (R)g.sy, (R)g.lly);
+    const R ox = min_r(r.r, bl + (R)g.sx) - max_r(r.l, bl);
+    const R oy = min_r(r.t, bb + (R)g.sy) - max_r(r.b, bb);
+    if (ox <= (R)0 || oy <= (R)0) return mk2<R>((R)0, (R)0);
+    const R ov = sxy * ox * oy;
+    const vec2<R> e = field[(size_t)i * g.ny + j];
+    return mk2<R>(ov * e.x, ov * e.y);
+}
+
+template <typename R>
 __global__ void __launch_bounds__(128)
-k_gather_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ size,
-             const uint8_t *__restrict__ flags, const float *__restrict__ sxy_of,
-             const int32_t *__restrict__ big, const float2 *__restrict__ field,
-             float2 *__restrict__ out, const DevScalars *__restrict__ S) {
+k_gather_big(Grid g, const vec2<R> *__restrict__ pos, const float2 *__restrict__ size,
+             const uint8_t *__restrict__ flags, const float *__restrict__ sxy_of, const int32_t *__restrict__ big,
+             const vec2<R> *__restrict__ field, vec2<R> *__restrict__ out, const DevScalars *__restrict__ S) {
     pdl_begin();
-    __shared__ float shx[4], shy[4];
+    __shared__ R shx[4], shy[4];
     if (S->done) return;
     const int o = big[blockIdx.x];
-    const FRect r = gather_rect(g, pos[o], size[o], flags[o]);
-    const float sxy = sxy_of[o];
+    const uint8_t f = flags[o];
+    const FRect<R> r = gather_rect<R>(g, pos[o], size[o], f);
+    const R sxy = smoothing_scale<R>(g, sxy_of[o], size[o], f);
     int i0, i1, j0, j1;
-    gather_range(g, r, i0, i1, j0, j1);
+    gather_range<R>(g, r, i0, i1, j0, j1);
     const int wy = j1 - j0 + 1;
     const int nb = (i1 >= i0 && j1 >= j0) ? (i1 - i0 + 1) * wy : 0;
-    float gx = 0.f, gy = 0.f;
+    R gx = (R)0, gy = (R)0;
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-        float2 v = gather_bin(g, r, sxy, i0 + t / wy, j0 + t % wy, field);
+        vec2<R> v = gather_bin<R>(g, r, sxy, i0 + t / wy, j0 + t % wy, field);
         gx += v.x;
         gy += v.y;
     }
-    gx = warp_sum_f(gx);
-    gy = warp_sum_f(gy);
+    gx = warp_sum_r(gx);
+    gy = warp_sum_r(gy);
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) {
         shx[wid] = gx;
@@ -549,12 +589,12 @@ k_gather_big(Grid g, const float2 *__restrict__ pos, const float2 *__restrict__ 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        float ax = 0.f, ay = 0.f;
+        R ax = (R)0, ay = (R)0;
         for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
             ax += shx[k];
             ay += shy[k];
         }
-        out[blockIdx.x] = make_float2(ax, ay);
+        out[blockIdx.x] = mk2<R>(ax, ay);
     }
 }
 
@@ -574,18 +614,18 @@ __device__ int stop_after_step(const DevScalars *S, double tau, int it) {
     return stop;
 }
 
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
-k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
-          const float2 *__restrict__ gd_big, const float2 *__restrict__ pin_grad,
-          float2 *__restrict__ gout, const float2 *__restrict__ g_prev,
-          const float2 *__restrict__ y_prev, float2 *__restrict__ dump_gd,
-          float2 *__restrict__ dump_gwl, int stepping, double *__restrict__ partials,
-          DevScalars *__restrict__ S) {
+k_combine(Grid g, DeviceNetlist d, const vec2<R> *__restrict__ field, const vec2<R> *__restrict__ gd_big,
+          const vec2<R> *__restrict__ pin_grad, vec2<R> *__restrict__ gout, const vec2<R> *__restrict__ g_prev,
+          const vec2<R> *__restrict__ y_prev, vec2<R> *__restrict__ dump_gd, vec2<R> *__restrict__ dump_gwl,
+          int stepping, double *__restrict__ partials, DevScalars *__restrict__ S) {
     pdl_begin();
     __shared__ double sh[32 * 5];
     if (S->done) return;
+    const vec2<R> *__restrict__ pos = (const vec2<R> *)d.pos;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
-    float lam = S->lambda0_mode ? 0.0f : (float)S->lambda;
+    R lam = S->lambda0_mode ? (R)0 : (R)S->lambda;
     int iter = S->iter;
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // dg2, dy2, s.y, |gwl|, |gd|
 
@@ -595,11 +635,11 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
     // in shared memory with all its loads in flight at once (kPinChunk per
     // round), then every lane adds its own pins from there in order.
     // Fillers own no pins.
-    __shared__ float2 pin_sm[kThreads / 32][kPinChunk];
-    float wx = 0.f, wy = 0.f;
+    __shared__ vec2<R> pin_sm[kThreads / 32][kPinChunk];
+    R wx = (R)0, wy = (R)0;
     {
         const int lane = threadIdx.x & 31;
-        float2 *sm = pin_sm[threadIdx.x >> 5];
+        vec2<R> *sm = pin_sm[threadIdx.x >> 5];
         const bool valid = o < d.n_obj;
         const int ps = valid ? d.obj_pin_start[o] : 0, pe = valid ? d.obj_pin_start[o + 1] : 0;
         const int wbeg = __shfl_sync(0xffffffffu, ps, 0);
@@ -618,55 +658,56 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
             __syncwarp();
             const int k1 = min(pe, base + n);
             for (int k = max(ps, base); k < k1; k++) {
-                const float2 v = sm[k - base];
-                wx = __fadd_rn(wx, v.x);
-                wy = __fadd_rn(wy, v.y);
+                const vec2<R> v = sm[k - base];
+                wx = add_rn(wx, v.x);
+                wy = add_rn(wy, v.y);
             }
             __syncwarp();
         }
     }
     if (o < d.n_obj) {
         uint8_t f = d.flags[o];
-        float2 p = d.pos[o];
-        float gdx = 0.f, gdy = 0.f;
+        vec2<R> p = pos[o];
+        R gdx = (R)0, gdy = (R)0;
         if (f & kBig) {
-            float2 v = gd_big[d.big_slot[o]];
+            vec2<R> v = gd_big[d.big_slot[o]];
             gdx = v.x;
             gdy = v.y;
         } else {
-            const FRect r = gather_rect(g, p, d.size[o], f);
-            const float sxy = d.sxy[o];
+            const float2 sz = d.size[o];
+            const FRect<R> r = gather_rect<R>(g, p, sz, f);
+            const R sxy = smoothing_scale<R>(g, d.sxy[o], sz, f);
             int i0, i1, j0, j1;
-            gather_range(g, r, i0, i1, j0, j1);
+            gather_range<R>(g, r, i0, i1, j0, j1);
             for (int i = i0; i <= i1; i++)
                 for (int j = j0; j <= j1; j++) {
-                    float2 v = gather_bin(g, r, sxy, i, j, field);
+                    vec2<R> v = gather_bin<R>(g, r, sxy, i, j, field);
                     gdx += v.x;
                     gdy += v.y;
                 }
         }
         // preconditioner 1/max(1, #pins + lambda*area) and direction
-        float den = fmaxf(1.0f, __fadd_rn(d.npins[o], __fmul_rn(lam, d.area[o])));
-        float pre = __fdiv_rn(1.0f, den);
-        float2 gg;
+        R den = max_r((R)1, add_rn((R)d.npins[o], mul_rn(lam, (R)d.area[o])));
+        R pre = div_rn((R)1, den);
+        vec2<R> gg;
         if (f & kFiller) {
-            gg.x = __fmul_rn(__fmul_rn(pre, lam), gdx);
-            gg.y = __fmul_rn(__fmul_rn(pre, lam), gdy);
+            gg.x = mul_rn(mul_rn(pre, lam), gdx);
+            gg.y = mul_rn(mul_rn(pre, lam), gdy);
         } else {
-            gg.x = __fmul_rn(pre, __fsub_rn(__fmul_rn(lam, gdx), wx));
-            gg.y = __fmul_rn(pre, __fsub_rn(__fmul_rn(lam, gdy), wy));
+            gg.x = mul_rn(pre, sub_rn(mul_rn(lam, gdx), wx));
+            gg.y = mul_rn(pre, sub_rn(mul_rn(lam, gdy), wy));
         }
         gout[o] = gg;
         if (dump_gd) {
-            dump_gd[o] = make_float2(gdx, gdy);
-            dump_gwl[o] = make_float2(wx, wy);
+            dump_gd[o] = mk2<R>(gdx, gdy);
+            dump_gwl[o] = mk2<R>(wx, wy);
         }
         // Lipschitz sums against the previous reference point: from the
         // second step on, and for every backtracking trial (stepping == 2)
         if ((stepping == 2 || (stepping && iter > 0)) && (f & kInView)) {
-            float2 gp = g_prev[o], yp = y_prev[o];
-            double dgx = __fsub_rn(gg.x, gp.x), dgy = __fsub_rn(gg.y, gp.y);
-            double dyx = __fsub_rn(p.x, yp.x), dyy = __fsub_rn(p.y, yp.y);
+            vec2<R> gp = g_prev[o], yp = y_prev[o];
+            double dgx = sub_rn(gg.x, gp.x), dgy = sub_rn(gg.y, gp.y);
+            double dyx = sub_rn(p.x, yp.x), dyy = sub_rn(p.y, yp.y);
             acc[0] = dgx * dgx + dgy * dgy;
             acc[1] = dyx * dyx + dyy * dyy;
             acc[2] = dyx * dgx + dyy * dgy;
@@ -689,13 +730,13 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
             if (stepping == 2) {
                 // backtracking trial (opt_step_bktrk, Optimization/nesterov.hpp:351-364):
                 // 1/L between the trial point and y_k; accepted when it is at
-                // least BKTRK_EPS (0.95, nesterov.hpp:37) of the step tried
+                // least BKTRK_EPS (0.95, nesterov.hpp:37; ep_limits) of the step tried
                 double ns = sqrt(dy2) / sqrt(dg2);
                 if (!isfinite(ns)) {
                     S->status |= 1 << EP_ERR_NAN;
                     ns = 0.0;
                 }
-                S->bk_accept = 0.95 * S->step <= ns;
+                S->bk_accept = S->bk_ratio * S->step <= ns;
                 S->step = ns;
                 S->stop_pending = stop_after_step(S, S->tau, S->iter + 1);
             } else if (stepping) {
@@ -730,18 +771,18 @@ k_combine(Grid g, DeviceNetlist d, const float2 *__restrict__ field,
 // x_{k+1} = y_k + s g_k, y_{k+1} = x_{k+1} + c (x_{k+1} - x_k)
 // (opt_step_vanilla, Optimization/nesterov.hpp:391-404); returns the clamped
 // new position, which becomes the object's position.
-__device__ __forceinline__ float2 nesterov_move(const Grid &g, int o, float s, float c,
-                                                const float2 *__restrict__ size, float2 *__restrict__ pos,
-                                                float2 *__restrict__ x, const float2 *__restrict__ gin,
-                                                float2 *__restrict__ y_prev, float2 *__restrict__ g_prev) {
-    float2 y = pos[o], gg = gin[o], xo = x[o];
-    float2 xn = make_float2(__fadd_rn(y.x, __fmul_rn(gg.x, s)), __fadd_rn(y.y, __fmul_rn(gg.y, s)));
-    float2 yn = make_float2(__fadd_rn(xn.x, __fmul_rn(__fsub_rn(xn.x, xo.x), c)),
-                            __fadd_rn(xn.y, __fmul_rn(__fsub_rn(xn.y, xo.y), c)));
+template <typename R>
+__device__ __forceinline__ vec2<R> nesterov_move(const Grid &g, int o, R s, R c, const float2 *__restrict__ size,
+                                                 vec2<R> *__restrict__ pos, vec2<R> *__restrict__ x,
+                                                 const vec2<R> *__restrict__ gin, vec2<R> *__restrict__ y_prev,
+                                                 vec2<R> *__restrict__ g_prev) {
+    vec2<R> y = pos[o], gg = gin[o], xo = x[o];
+    vec2<R> xn = mk2<R>(add_rn(y.x, mul_rn(gg.x, s)), add_rn(y.y, mul_rn(gg.y, s)));
+    vec2<R> yn = mk2<R>(add_rn(xn.x, mul_rn(sub_rn(xn.x, xo.x), c)), add_rn(xn.y, mul_rn(sub_rn(xn.y, xo.y), c)));
     y_prev[o] = y;
     g_prev[o] = gg;
     x[o] = xn;
-    const float2 p = clamp_center(g, yn, size[o]);
+    const vec2<R> p = clamp_center<R>(g, yn, size[o]);
     pos[o] = p;
     return p;
 }
@@ -756,15 +797,16 @@ __device__ __forceinline__ void end_step(DevScalars *S) {
     }
 }
 
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
-k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
-         float2 *__restrict__ pos, float2 *__restrict__ x, const float2 *__restrict__ gin,
-         float2 *__restrict__ y_prev, float2 *__restrict__ g_prev, DevScalars *__restrict__ S) {
+k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size, vec2<R> *__restrict__ pos,
+         vec2<R> *__restrict__ x, const vec2<R> *__restrict__ gin, vec2<R> *__restrict__ y_prev,
+         vec2<R> *__restrict__ g_prev, DevScalars *__restrict__ S) {
     pdl_begin();
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o < n && (flags[o] & kInView))
-        nesterov_move(g, o, (float)S->step, (float)S->coef, size, pos, x, gin, y_prev, g_prev);
+        nesterov_move<R>(g, o, (R)S->step, (R)S->coef, size, pos, x, gin, y_prev, g_prev);
     if (threadIdx.x == 0 && last_block(&S->cnt_upd, gridDim.x)) end_step(S);
 }
 
@@ -774,32 +816,32 @@ k_update(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restr
 // moved and scattered by a block of their own (the blocks after
 // small_blocks).  The step that ends the stage scatters nothing, so the maps
 // stay clear (prep clears them after each read).
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
-k_update_scatter(Grid g, int n, int small_blocks, const int32_t *__restrict__ big,
-                 const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
-                 float2 *__restrict__ pos, float2 *__restrict__ x, const float2 *__restrict__ gin,
-                 float2 *__restrict__ y_prev, float2 *__restrict__ g_prev, double qscale,
-                 unsigned long long *__restrict__ node_q, unsigned long long *__restrict__ filler_q,
-                 DevScalars *__restrict__ S) {
+k_update_scatter(Grid g, int n, int small_blocks, const int32_t *__restrict__ big, const uint8_t *__restrict__ flags,
+                 const float2 *__restrict__ size, vec2<R> *__restrict__ pos, vec2<R> *__restrict__ x,
+                 const vec2<R> *__restrict__ gin, vec2<R> *__restrict__ y_prev, vec2<R> *__restrict__ g_prev,
+                 double qscale, ull *__restrict__ node_q, ull *__restrict__ filler_q, DevScalars *__restrict__ S) {
     pdl_begin();
-    __shared__ float2 big_pos;
+    __shared__ vec2<R> big_pos;
     if (S->done) return;
-    const float s = (float)S->step, c = (float)S->coef;
+    const R s = (R)S->step, c = (R)S->coef;
     const bool scatter = !S->stop_pending;
     if ((int)blockIdx.x >= small_blocks) {
         const int o = big[blockIdx.x - small_blocks];
         const uint8_t f = flags[o];
         if (threadIdx.x == 0)
-            big_pos = (f & kInView) ? nesterov_move(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
+            big_pos = (f & kInView) ? nesterov_move<R>(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
         __syncthreads();
-        if (scatter) scatter_big_object(g, big_pos, size[o], f, qscale, node_q, filler_q);
+        if (scatter) scatter_big_object<R>(g, big_pos, size[o], f, qscale, node_q, filler_q);
     } else {
         const int o = blockIdx.x * blockDim.x + threadIdx.x;
         if (o < n) {
             const uint8_t f = flags[o];
             if (!(f & kBig)) {
-                const float2 p = (f & kInView) ? nesterov_move(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
-                if (scatter) scatter_small_object(g, p, size[o], f, qscale, node_q, filler_q);
+                const vec2<R> p =
+                    (f & kInView) ? nesterov_move<R>(g, o, s, c, size, pos, x, gin, y_prev, g_prev) : pos[o];
+                if (scatter) scatter_small_object<R>(g, p, size[o], f, qscale, node_q, filler_q);
             }
         }
     }
@@ -809,11 +851,11 @@ k_update_scatter(Grid g, int n, int small_blocks, const int32_t *__restrict__ bi
 // Backtracking trial move (opt_step_bktrk, Optimization/nesterov.hpp:337-349):
 // from y_k (kept in ysave) x_t = y_k + step g_k, y_t = x_t + coef (x_t - x_k);
 // the positions become clamp(y_t) and x_t is kept in xtrial until accepted.
+template <typename R>
 __global__ void __launch_bounds__(kThreads)
 k_bktrk_move(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
-             const float2 *__restrict__ ysave, const float2 *__restrict__ gin,
-             const float2 *__restrict__ x, float2 *__restrict__ pos, float2 *__restrict__ xtrial,
-             const DevScalars *__restrict__ S) {
+             const vec2<R> *__restrict__ ysave, const vec2<R> *__restrict__ gin, const vec2<R> *__restrict__ x,
+             vec2<R> *__restrict__ pos, vec2<R> *__restrict__ xtrial, const DevScalars *__restrict__ S) {
     pdl_begin();
     if (S->done) return;
     int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -822,13 +864,12 @@ k_bktrk_move(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__r
         xtrial[o] = x[o];
         return;
     }
-    float s = (float)S->step, c = (float)S->coef;
-    float2 y = ysave[o], gg = gin[o], xo = x[o];
-    float2 xn = make_float2(__fadd_rn(y.x, __fmul_rn(gg.x, s)), __fadd_rn(y.y, __fmul_rn(gg.y, s)));
-    float2 yn = make_float2(__fadd_rn(xn.x, __fmul_rn(__fsub_rn(xn.x, xo.x), c)),
-                            __fadd_rn(xn.y, __fmul_rn(__fsub_rn(xn.y, xo.y), c)));
+    R s = (R)S->step, c = (R)S->coef;
+    vec2<R> y = ysave[o], gg = gin[o], xo = x[o];
+    vec2<R> xn = mk2<R>(add_rn(y.x, mul_rn(gg.x, s)), add_rn(y.y, mul_rn(gg.y, s)));
+    vec2<R> yn = mk2<R>(add_rn(xn.x, mul_rn(sub_rn(xn.x, xo.x), c)), add_rn(xn.y, mul_rn(sub_rn(xn.y, xo.y), c)));
     xtrial[o] = xn;
-    pos[o] = clamp_center(g, yn, size[o]);
+    pos[o] = clamp_center<R>(g, yn, size[o]);
 }
 
 // The accepted trial ends the step: the scalar side of k_update.
@@ -844,9 +885,9 @@ __global__ void k_bktrk_commit(DevScalars *__restrict__ S) {
 }
 
 // EplaceNesterovOpt::init (nesterov.hpp:207-214): x_0 = current positions.
-__global__ void k_stage_begin(int n, const uint8_t *__restrict__ flags,
-                              const float2 *__restrict__ pos, float2 *__restrict__ x,
-                              DevScalars *__restrict__ S) {
+template <typename R>
+__global__ void k_stage_begin(int n, const uint8_t *__restrict__ flags, const vec2<R> *__restrict__ pos,
+                              vec2<R> *__restrict__ x, DevScalars *__restrict__ S) {
     pdl_begin();
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x)
         if (flags[o] & kInView) x[o] = pos[o];
@@ -870,12 +911,12 @@ __global__ void k_stage_begin(int n, const uint8_t *__restrict__ flags,
 }
 
 // wrap_up (nesterov.hpp:216-223): positions = main solution, clamped.
-__global__ void k_wrap_up(Grid g, int n, const uint8_t *__restrict__ flags,
-                          const float2 *__restrict__ size, float2 *__restrict__ pos,
-                          const float2 *__restrict__ x) {
+template <typename R>
+__global__ void k_wrap_up(Grid g, int n, const uint8_t *__restrict__ flags, const float2 *__restrict__ size,
+                          vec2<R> *__restrict__ pos, const vec2<R> *__restrict__ x) {
     pdl_begin();
     int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o < n && (flags[o] & kInView)) pos[o] = clamp_center(g, x[o], size[o]);
+    if (o < n && (flags[o] & kInView)) pos[o] = clamp_center<R>(g, x[o], size[o]);
 }
 
 }  // namespace
@@ -901,97 +942,156 @@ int reduction_blocks(const DeviceNetlist &d, int which) {
     }
 }
 
-void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, unsigned long long *node_q,
-                    unsigned long long *filler_q, const DevScalars *S, cudaStream_t st) {
+namespace {
+template <typename R>
+inline vec2<R> *V(void *p) {
+    return static_cast<vec2<R> *>(p);
+}
+template <typename R>
+inline const vec2<R> *V(const void *p) {
+    return static_cast<const vec2<R> *>(p);
+}
+}  // namespace
+
+template <typename R>
+static void scatter_t(const KernelCtx &c, const DeviceNetlist &d, ull *node_q, ull *filler_q, const DevScalars *S,
+                      cudaStream_t st) {
     const int sb = blocks_for(d.n_obj, kThreads);
-    launch_k(k_scatter, sb + d.n_big_objs, kThreads, 0, st, c.grid, d.pos, d.size, d.flags, d.n_obj, sb,
+    launch_k(k_scatter<R>, sb + d.n_big_objs, kThreads, 0, st, c.grid, V<R>(d.pos), d.size, d.flags, d.n_obj, sb,
              d.big_objs, c.qscale, node_q, filler_q, S);
 }
 
-void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
-                           const float2 *g, float2 *y_prev, float2 *g_prev, unsigned long long *node_q,
-                           unsigned long long *filler_q, DevScalars *S, cudaStream_t st) {
-    const int sb = blocks_for(d.n_obj, kThreads);
-    launch_k(k_update_scatter, sb + d.n_big_objs, kThreads, 0, st, c.grid, d.n_obj, sb, d.big_objs,
-             d.flags, d.size, pos, x, g, y_prev, g_prev, c.qscale, node_q, filler_q, S);
+void launch_scatter(const KernelCtx &c, const DeviceNetlist &d, ull *node_q, ull *filler_q, const DevScalars *S,
+                    cudaStream_t st) {
+    c.fp64 ? scatter_t<double>(c, d, node_q, filler_q, S, st) : scatter_t<float>(c, d, node_q, filler_q, S, st);
 }
 
-void launch_prep(const KernelCtx &c, unsigned long long *node_q, unsigned long long *filler_q,
-                 const float2 *static_map, float *rho, void *rho_bf16, float *node_f,
-                 float *filler_f, int zero_maps, DevScalars *S, cudaStream_t st) {
+template <typename R>
+static void update_scatter_t(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g,
+                             void *y_prev, void *g_prev, ull *node_q, ull *filler_q, DevScalars *S, cudaStream_t st) {
+    const int sb = blocks_for(d.n_obj, kThreads);
+    launch_k(k_update_scatter<R>, sb + d.n_big_objs, kThreads, 0, st, c.grid, d.n_obj, sb, d.big_objs, d.flags,
+             d.size, V<R>(pos), V<R>(x), V<R>(g), V<R>(y_prev), V<R>(g_prev), c.qscale, node_q, filler_q, S);
+}
+
+void launch_update_scatter(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g,
+                           void *y_prev, void *g_prev, ull *node_q, ull *filler_q, DevScalars *S, cudaStream_t st) {
+    c.fp64 ? update_scatter_t<double>(c, d, pos, x, g, y_prev, g_prev, node_q, filler_q, S, st)
+           : update_scatter_t<float>(c, d, pos, x, g, y_prev, g_prev, node_q, filler_q, S, st);
+}
+
+void launch_prep(const KernelCtx &c, ull *node_q, ull *filler_q, const float2 *static_map, void *rho,
+                 void *rho_bf16, float *node_f, float *filler_f, int zero_maps, DevScalars *S, cudaStream_t st) {
     int nb = c.grid.nx * c.grid.ny;
     int blocks = prep_blocks(c.grid);
     uint16_t *hi = (uint16_t *)rho_bf16;
     uint16_t *lo = hi ? hi + nb : nullptr;
-    launch_k(k_prep, blocks, kThreads, 0, st, c.grid, node_q, filler_q, static_map, rho, hi, lo, node_f,
-             filler_f, zero_maps, c.inv_qscale, c.inv_bin_area, c.bin_area, c.area_norm, c.part_prep, S);
-}
-
-template <bool WL, bool EXACT, bool LSE>
-void launch_nets(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad, double *partials,
-                 int mode, DevScalars *S, cudaStream_t st) {
-    PinCtx pc{d.pin_owner, d.pin_off, d.pos};
-    if (d.n_net_tasks == 0) return;
-    launch_kp(k_wl<WL, EXACT, LSE>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, launch_priority(false),
-              d.net_tasks, d.n_net_tasks, pc, pin_grad, c.want_wl_value, partials, mode, S);
-}
-
-void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, float2 *pin_grad,
-                       DevScalars *S, cudaStream_t st) {
-    if (c.exact_exp)
-        c.lse ? launch_nets<true, true, true>(c, d, pin_grad, c.part_wl, 0, S, st)
-              : launch_nets<true, true, false>(c, d, pin_grad, c.part_wl, 0, S, st);
+    if (c.fp64)
+        launch_k(k_prep<double>, blocks, kThreads, 0, st, c.grid, node_q, filler_q, static_map, (double *)rho,
+                 (uint16_t *)nullptr, (uint16_t *)nullptr, node_f, filler_f, zero_maps, c.inv_qscale,
+                 c.inv_bin_area, c.bin_area, c.area_norm, c.part_prep, S);
     else
-        c.lse ? launch_nets<true, false, true>(c, d, pin_grad, c.part_wl, 0, S, st)
-              : launch_nets<true, false, false>(c, d, pin_grad, c.part_wl, 0, S, st);
+        launch_k(k_prep<float>, blocks, kThreads, 0, st, c.grid, node_q, filler_q, static_map, (float *)rho, hi, lo,
+                 node_f, filler_f, zero_maps, c.inv_qscale, c.inv_bin_area, c.bin_area, c.area_norm, c.part_prep,
+                 S);
 }
 
-void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
-                       float2 *gd_big, const DevScalars *S, cudaStream_t st) {
-    if (d.n_big_objs > 0)
-        launch_k(k_gather_big, d.n_big_objs, 128, 0, st, c.grid, d.pos, d.size, d.flags, d.sxy,
-                 d.big_objs, field, gd_big, S);
+template <bool WL, bool EXACT, bool LSE, typename R>
+static void launch_nets(const KernelCtx &c, const DeviceNetlist &d, void *pin_grad, double *partials, int mode,
+                        DevScalars *S, cudaStream_t st) {
+    PinCtx<R> pc{d.pin_owner, d.pin_off, V<R>(d.pos)};
+    if (d.n_net_tasks == 0) return;
+    launch_kp(k_wl<WL, EXACT, LSE, R>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, launch_priority(false),
+              d.net_tasks, d.n_net_tasks, pc, V<R>(pin_grad), c.want_wl_value, partials, mode, S);
 }
 
-void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const float2 *field,
-                    const float2 *gd_big, const float2 *pin_grad, float2 *g, const float2 *g_prev,
-                    const float2 *y_prev, float2 *dump_gd, float2 *dump_gwl, int stepping,
-                    DevScalars *S, cudaStream_t st) {
-    launch_k(k_combine, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d, field, gd_big,
-             pin_grad, g, g_prev, y_prev, dump_gd, dump_gwl, stepping, c.part_comb, S);
+template <typename R>
+static void wirelength_t(const KernelCtx &c, const DeviceNetlist &d, void *pin_grad, DevScalars *S, cudaStream_t st) {
+    if (c.exact_exp)
+        c.lse ? launch_nets<true, true, true, R>(c, d, pin_grad, c.part_wl, 0, S, st)
+              : launch_nets<true, true, false, R>(c, d, pin_grad, c.part_wl, 0, S, st);
+    else
+        c.lse ? launch_nets<true, false, true, R>(c, d, pin_grad, c.part_wl, 0, S, st)
+              : launch_nets<true, false, false, R>(c, d, pin_grad, c.part_wl, 0, S, st);
 }
 
-void launch_update(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, float2 *x,
-                   const float2 *g, float2 *y_prev, float2 *g_prev, DevScalars *S,
-                   cudaStream_t st) {
-    launch_k(k_update, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
-             pos, x, g, y_prev, g_prev, S);
+void launch_wirelength(const KernelCtx &c, const DeviceNetlist &d, void *pin_grad, DevScalars *S, cudaStream_t st) {
+    c.fp64 ? wirelength_t<double>(c, d, pin_grad, S, st) : wirelength_t<float>(c, d, pin_grad, S, st);
 }
 
-void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const float2 *ysave, const float2 *g,
-                       const float2 *x, float2 *pos, float2 *xtrial, const DevScalars *S,
-                       cudaStream_t st) {
-    launch_k(k_bktrk_move, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags,
-             d.size, ysave, g, x, pos, xtrial, S);
+void launch_gather_big(const KernelCtx &c, const DeviceNetlist &d, const void *field, void *gd_big,
+                       const DevScalars *S, cudaStream_t st) {
+    if (d.n_big_objs == 0) return;
+    if (c.fp64)
+        launch_k(k_gather_big<double>, d.n_big_objs, 128, 0, st, c.grid, V<double>(d.pos), d.size, d.flags, d.sxy,
+                 d.big_objs, V<double>(field), V<double>(gd_big), S);
+    else
+        launch_k(k_gather_big<float>, d.n_big_objs, 128, 0, st, c.grid, V<float>(d.pos), d.size, d.flags, d.sxy,
+                 d.big_objs, V<float>(field), V<float>(gd_big), S);
+}
+
+void launch_combine(const KernelCtx &c, const DeviceNetlist &d, const void *field, const void *gd_big,
+                    const void *pin_grad, void *g, const void *g_prev, const void *y_prev, void *dump_gd,
+                    void *dump_gwl, int stepping, DevScalars *S, cudaStream_t st) {
+    if (c.fp64)
+        launch_k(k_combine<double>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d, V<double>(field),
+                 V<double>(gd_big), V<double>(pin_grad), V<double>(g), V<double>(g_prev), V<double>(y_prev),
+                 V<double>(dump_gd), V<double>(dump_gwl), stepping, c.part_comb, S);
+    else
+        launch_k(k_combine<float>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d, V<float>(field),
+                 V<float>(gd_big), V<float>(pin_grad), V<float>(g), V<float>(g_prev), V<float>(y_prev),
+                 V<float>(dump_gd), V<float>(dump_gwl), stepping, c.part_comb, S);
+}
+
+template <typename R>
+static void update_t(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g, void *y_prev,
+                     void *g_prev, DevScalars *S, cudaStream_t st) {
+    launch_k(k_update<R>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+             V<R>(pos), V<R>(x), V<R>(g), V<R>(y_prev), V<R>(g_prev), S);
+}
+
+void launch_update(const KernelCtx &c, const DeviceNetlist &d, void *pos, void *x, const void *g, void *y_prev,
+                   void *g_prev, DevScalars *S, cudaStream_t st) {
+    c.fp64 ? update_t<double>(c, d, pos, x, g, y_prev, g_prev, S, st)
+           : update_t<float>(c, d, pos, x, g, y_prev, g_prev, S, st);
+}
+
+template <typename R>
+static void bktrk_move_t(const KernelCtx &c, const DeviceNetlist &d, const void *ysave, const void *g,
+                         const void *x, void *pos, void *xtrial, const DevScalars *S, cudaStream_t st) {
+    launch_k(k_bktrk_move<R>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+             V<R>(ysave), V<R>(g), V<R>(x), V<R>(pos), V<R>(xtrial), S);
+}
+
+void launch_bktrk_move(const KernelCtx &c, const DeviceNetlist &d, const void *ysave, const void *g, const void *x,
+                       void *pos, void *xtrial, const DevScalars *S, cudaStream_t st) {
+    c.fp64 ? bktrk_move_t<double>(c, d, ysave, g, x, pos, xtrial, S, st)
+           : bktrk_move_t<float>(c, d, ysave, g, x, pos, xtrial, S, st);
 }
 
 void launch_bktrk_commit(DevScalars *S, cudaStream_t st) { launch_k(k_bktrk_commit, 1, 1, 0, st, S); }
 
-void launch_stage_begin(const DeviceNetlist &d, const float2 *pos, float2 *x, DevScalars *S,
+void launch_stage_begin(const KernelCtx &c, const DeviceNetlist &d, const void *pos, void *x, DevScalars *S,
                         cudaStream_t st) {
-    launch_k(k_stage_begin, std::min(blocks_for(d.n_obj, kThreads), 148 * 4), kThreads, 0, st, d.n_obj,
-             d.flags, pos, x, S);
+    const int blocks = std::min(blocks_for(d.n_obj, kThreads), 148 * 4);
+    if (c.fp64)
+        launch_k(k_stage_begin<double>, blocks, kThreads, 0, st, d.n_obj, d.flags, V<double>(pos), V<double>(x), S);
+    else
+        launch_k(k_stage_begin<float>, blocks, kThreads, 0, st, d.n_obj, d.flags, V<float>(pos), V<float>(x), S);
 }
 
-void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, float2 *pos, const float2 *x,
-                    cudaStream_t st) {
-    launch_k(k_wrap_up, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
-             pos, x);
+void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, void *pos, const void *x, cudaStream_t st) {
+    if (c.fp64)
+        launch_k(k_wrap_up<double>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+                 V<double>(pos), V<double>(x));
+    else
+        launch_k(k_wrap_up<float>, blocks_for(d.n_obj, kThreads), kThreads, 0, st, c.grid, d.n_obj, d.flags, d.size,
+                 V<float>(pos), V<float>(x));
 }
 
-void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S,
-                 cudaStream_t st) {
-    launch_nets<false, false, false>(c, d, nullptr, c.part_hp, mode, S, st);
+void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S, cudaStream_t st) {
+    c.fp64 ? launch_nets<false, false, false, double>(c, d, nullptr, c.part_hp, mode, S, st)
+           : launch_nets<false, false, false, float>(c, d, nullptr, c.part_hp, mode, S, st);
 }
 
 int carveout_percent(size_t smem_bytes) {
@@ -1003,6 +1103,17 @@ int carveout_percent(size_t smem_bytes) {
     for (int i = 1; i < 10; i++)
         if (kConfigs[i] >= kb) return (int)std::ceil(50.0 * (kConfigs[i - 1] + kConfigs[i]) / 228.0);
     return 100;
+}
+
+template <typename R>
+static void loop_kernels(std::vector<const void *> &fns) {
+    const void *f[] = {(const void *)k_scatter<R>, (const void *)k_prep<R>, (const void *)k_wl<true, false, false, R>,
+                       (const void *)k_wl<true, true, false, R>, (const void *)k_wl<true, false, true, R>,
+                       (const void *)k_wl<true, true, true, R>, (const void *)k_wl<false, false, false, R>,
+                       (const void *)k_gather_big<R>, (const void *)k_combine<R>, (const void *)k_update<R>,
+                       (const void *)k_update_scatter<R>, (const void *)k_bktrk_move<R>,
+                       (const void *)k_stage_begin<R>, (const void *)k_wrap_up<R>};
+    fns.insert(fns.end(), std::begin(f), std::end(f));
 }
 
 // One L1/shared split, kLoopSmemBytes of shared memory, for every kernel of
@@ -1024,13 +1135,9 @@ void set_loop_carveout() {
         done_devices.push_back(dev);
     }
     const int carveout = carveout_percent(kLoopSmemBytes);
-    const void *fns[] = {(const void *)k_scatter, (const void *)k_prep, (const void *)k_wl<true, false, false>,
-                         (const void *)k_wl<true, true, false>, (const void *)k_wl<true, false, true>,
-                         (const void *)k_wl<true, true, true>, (const void *)k_wl<false, false, false>,
-                         (const void *)k_wl<false, true, false>, (const void *)k_wl<false, false, true>,
-                         (const void *)k_wl<false, true, true>, (const void *)k_gather_big, (const void *)k_combine,
-                         (const void *)k_update, (const void *)k_update_scatter, (const void *)k_bktrk_move,
-                         (const void *)k_bktrk_commit, (const void *)k_stage_begin, (const void *)k_wrap_up};
+    std::vector<const void *> fns = {(const void *)k_bktrk_commit};
+    loop_kernels<float>(fns);
+    loop_kernels<double>(fns);
     for (const void *f : fns) cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
     set_sgemm_carveout(carveout);
 }

@@ -329,7 +329,7 @@ __global__ void k_qp_to_x(int nn, const float2 *__restrict__ pos, float2 *__rest
 __global__ void k_qp_from_x(Grid g, int nn, const float2 *__restrict__ x, const float2 *__restrict__ size,
                             float2 *__restrict__ pos) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nn) pos[i] = clamp_center(g, x[i], size[i]);
+    if (i < nn) pos[i] = clamp_center<float>(g, x[i], size[i]);
 }
 
 // PlaceDB::moveNodesCenterToCenter (PlaceDB/placedb.cpp:591-598).
@@ -338,7 +338,7 @@ __global__ void k_qp_center(Grid g, int nn, const float2 *__restrict__ size, flo
     if (i < nn) {
         const float2 c = make_float2((float)(0.5 * ((double)g.urx + (double)g.llx)),
                                      (float)(0.5 * ((double)g.ury + (double)g.lly)));
-        pos[i] = clamp_center(g, c, size[i]);
+        pos[i] = clamp_center<float>(g, c, size[i]);
     }
 }
 

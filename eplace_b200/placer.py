@@ -23,11 +23,14 @@ WL_WA, WL_LSE = 0, 1
 EXP_FAST, EXP_EXACT = 0, 1
 STEP_LIPSCHITZ, STEP_BB, STEP_BKTRK = 0, 1, 2
 DCT_FP32, DCT_BF16X3, DCT_AUTO, DCT_FFT = 0, 1, 2, 3
+PREC_MIXED, PREC_FP64 = 0, 1
+ABI_VERSION = 2
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
+_f64p = ctypes.POINTER(ctypes.c_double)
 
 
 class EPError(RuntimeError):
@@ -52,7 +55,13 @@ class Params(ctypes.Structure):
                 ("max_iterations", ctypes.c_int32), ("wl_model", ctypes.c_int32),
                 ("exp_mode", ctypes.c_int32), ("step_rule", ctypes.c_int32),
                 ("dct_mode", ctypes.c_int32), ("filler_seed", ctypes.c_uint64),
-                ("device", ctypes.c_int32), ("keep_maps", ctypes.c_int32)]
+                ("device", ctypes.c_int32), ("keep_maps", ctypes.c_int32),
+                ("precision", ctypes.c_int32)]
+
+
+class Limits(ctypes.Structure):
+    _fields_ = [("wait_polls", ctypes.c_uint32), ("bktrk_trials", ctypes.c_int32),
+                ("bktrk_accept", ctypes.c_double)]
 
 
 class Scalars(ctypes.Structure):
@@ -76,7 +85,7 @@ class Info(ctypes.Structure):
                 ("filler_w", ctypes.c_float), ("filler_h", ctypes.c_float),
                 ("std_area", ctypes.c_double), ("macro_area", ctypes.c_double),
                 ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double),
-                ("dct_mode", ctypes.c_int32)]
+                ("dct_mode", ctypes.c_int32), ("precision", ctypes.c_int32)]
 
 
 class RunStats(ctypes.Structure):
@@ -104,6 +113,8 @@ EXPORTS = (
     "ep_default_params", "ep_abi_version", "ep_create", "ep_destroy", "ep_last_error", "ep_get_info",
     "ep_set_stream", "ep_synchronize", "ep_get_positions", "ep_set_positions", "ep_initialize",
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
+    "ep_get_positions_f64", "ep_get_field_f64", "ep_get_component_gradients_f64",
+    "ep_get_limits", "ep_set_limits",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
@@ -145,6 +156,8 @@ def load():
     L.ep_default_params.argtypes = [ctypes.POINTER(Params)]
     L.ep_default_params.restype = None
     L.ep_abi_version.restype = ctypes.c_int32
+    if L.ep_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{LIB_PATH} has ABI {L.ep_abi_version()}, this binding {ABI_VERSION}: rebuild it")
     L.ep_create.argtypes = [ctypes.POINTER(Netlist), ctypes.POINTER(Params), ctypes.POINTER(vp)]
     L.ep_destroy.argtypes = [vp]
     L.ep_destroy.restype = None
@@ -176,6 +189,11 @@ def load():
     L.ep_density_scatter_noalloc.argtypes = [ctypes.POINTER(ScatterGrid), ctypes.c_int32] + [vp] * 8 + \
         [ctypes.c_char_p, ctypes.c_int32]
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
+    L.ep_get_component_gradients_f64.argtypes = [vp, _f64p, _f64p]
+    L.ep_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
+    L.ep_set_limits.argtypes = [vp, ctypes.POINTER(Limits)]
+    L.ep_get_positions_f64.argtypes = [vp, ctypes.c_int32, _f64p, ctypes.c_int32]
+    L.ep_get_field_f64.argtypes = [vp, _f64p, _f64p, _f64p]
     L.ep_get_bin_maps.argtypes = [vp] + [_f32p] * 7
     L.ep_get_density_fixed.argtypes = [vp, _i64p, _i64p]
     L.ep_query.argtypes = [vp, ctypes.POINTER(Scalars)]
@@ -398,6 +416,24 @@ class Engine:
         self._check(self._L.ep_get_positions(self.h, view, _p(xy, _f32p), n))
         return xy
 
+    def limits(self):
+        lim = Limits()
+        self._check(self._L.ep_get_limits(self.h, ctypes.byref(lim)))
+        return {k: getattr(lim, k) for k, _ in Limits._fields_}
+
+    def set_limits(self, **kw):
+        lim = Limits()
+        self._check(self._L.ep_get_limits(self.h, ctypes.byref(lim)))
+        for k, v in kw.items():
+            setattr(lim, k, v)
+        self._check(self._L.ep_set_limits(self.h, ctypes.byref(lim)))
+
+    def get_positions_f64(self, view=MGP):
+        n = self.view_size(view)
+        xy = np.zeros((n, 2), np.float64)
+        self._check(self._L.ep_get_positions_f64(self.h, view, _p(xy, _f64p), n))
+        return xy
+
     def set_positions(self, xy, view=MGP):
         xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
         self._check(self._L.ep_set_positions(self.h, view, _p(xy, _f32p), xy.shape[0]))
@@ -421,6 +457,19 @@ class Engine:
         gw = np.zeros((n, 2), np.float32)
         self._check(self._L.ep_get_component_gradients(self.h, _p(gd, _f32p), _p(gw, _f32p)))
         return gd, gw
+
+    def component_gradients_f64(self):
+        n = self.info.num_objects
+        gd = np.zeros((n, 2), np.float64)
+        gw = np.zeros((n, 2), np.float64)
+        self._check(self._L.ep_get_component_gradients_f64(self.h, _p(gd, _f64p), _p(gw, _f64p)))
+        return gd, gw
+
+    def field_f64(self):
+        nx, ny = self.info.bins_x, self.info.bins_y
+        out = {k: np.zeros((nx, ny), np.float64) for k in ("ex", "ey", "phi")}
+        self._check(self._L.ep_get_field_f64(self.h, *[_p(out[k], _f64p) for k in ("ex", "ey", "phi")]))
+        return out
 
     def bin_maps(self, which=("node", "filler", "terminal", "base", "ex", "ey", "phi")):
         nx, ny = self.info.bins_x, self.info.bins_y

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define EP_ABI_VERSION 1
+#define EP_ABI_VERSION 2
 
 typedef enum ep_status {
     EP_OK = 0,
@@ -64,6 +64,16 @@ typedef enum ep_dct_mode {
     EP_DCT_FFT = 3
 } ep_dct_mode;
 
+/* Working precision of the global-placement loop.  EP_PREC_MIXED (the
+ * default): positions, the optimizer's vectors, the Poisson solve, the field
+ * gather and the wirelength terms in FP32 (as the reference computes them,
+ * EPlace/eplace.cpp, PlaceCommon/objects.cpp), the overflow / HPWL /
+ * Lipschitz / lambda reductions in FP64.  EP_PREC_FP64: the same kernels with
+ * every vector, map and wirelength term in FP64 (the plain FP64 form; the
+ * Poisson solve by fast transforms only, so bin counts must be powers of two
+ * in [8, 2048]).  The density maps are int64 fixed point in both. */
+typedef enum ep_precision { EP_PREC_MIXED = 0, EP_PREC_FP64 = 1 } ep_precision;
+
 /* Netlist in plain arrays (what Parser/parser.cpp:44-97 builds into PlaceDB).
  * Nodes are movable; a node is a macro iff its height exceeds
  * common_row_height (PlaceDB/placedb.cpp:96-114).  Terminals are fixed.
@@ -100,6 +110,7 @@ typedef struct ep_params {
     uint64_t filler_seed;   /* seed of the engine's own filler placement */
     int32_t device;         /* CUDA device ordinal */
     int32_t keep_maps;      /* 1 = keep per-evaluation bin maps queryable (tests) */
+    int32_t precision;      /* ep_precision */
 } ep_params;
 
 /* Scalars of EPlacer_2D (EPlace/eplace.h:108-136) and the optimizer. */
@@ -130,6 +141,7 @@ typedef struct ep_info {
     double total_row_area;
     double density_scale;         /* fixed-point units per unit area of the bin maps */
     int32_t dct_mode;             /* ep_dct_mode in use (never EP_DCT_AUTO) */
+    int32_t precision;            /* ep_precision in use */
 } ep_info;
 
 typedef struct ep_run_stats {
@@ -163,6 +175,21 @@ typedef struct ep_kernel_times {
 
 typedef struct ep_engine ep_engine;
 
+/* Limits of the engine's bounded device waits and retries; no counterpart in
+ * the reference, which waits and retries without limit.  A tensor-core
+ * pipeline wait gives up after wait_polls polls (default 2^22, about a
+ * second), and the call that launched it ends with EP_ERR_TIMEOUT, the
+ * engine still usable; a backtracking step (EP_STEP_BKTRK) gives up after
+ * bktrk_trials rejected trials (default 64) with EP_ERR_TIMEOUT; a trial is
+ * accepted when its 1/L is at least bktrk_accept times the step tried
+ * (default 0.95, BKTRK_EPS of Optimization/nesterov.hpp:37).  Lowering them
+ * exercises the give-up paths. */
+typedef struct ep_limits {
+    uint32_t wait_polls;
+    int32_t bktrk_trials;
+    double bktrk_accept;
+} ep_limits;
+
 /* ep_params with the reference defaults (rho_t 1.0, overflow 0.10, 1000 iterations). */
 void ep_default_params(ep_params *p);
 int32_t ep_abi_version(void);
@@ -175,6 +202,8 @@ ep_status ep_create(const ep_netlist *netlist, const ep_params *params, ep_engin
 void ep_destroy(ep_engine *e);
 const char *ep_last_error(const ep_engine *e);
 ep_status ep_get_info(const ep_engine *e, ep_info *info);
+ep_status ep_get_limits(const ep_engine *e, ep_limits *limits);
+ep_status ep_set_limits(ep_engine *e, const ep_limits *limits);
 /* Use this CUDA stream (cudaStream_t) for all later work; NULL = engine's own. */
 ep_status ep_set_stream(ep_engine *e, void *stream);
 ep_status ep_synchronize(ep_engine *e);
@@ -184,6 +213,8 @@ ep_status ep_synchronize(ep_engine *e);
  * PlaceDB/placedb.cpp:253-288).  xy has 2*count floats. */
 ep_status ep_get_positions(ep_engine *e, int32_t view, float *xy, int32_t count);
 ep_status ep_set_positions(ep_engine *e, int32_t view, const float *xy, int32_t count);
+/* ep_get_positions in double (an FP64 engine's centres without rounding). */
+ep_status ep_get_positions_f64(ep_engine *e, int32_t view, double *xy, int32_t count);
 /* PlaceDB::saveNodesLocation / loadNodesLocation (PlaceDB/placedb.cpp:1441-1465)
  * for every object, kept in device memory (no host copy). */
 ep_status ep_save_positions(ep_engine *e);
@@ -200,11 +231,17 @@ ep_status ep_get_gradient(ep_engine *e, int32_t view, float *xy, int32_t count);
 /* densityGradient / wirelengthGradient of the last evaluation, all objects
  * (keep_maps must be set). */
 ep_status ep_get_component_gradients(ep_engine *e, float *density_xy, float *wirelength_xy);
+/* The same in double: an FP64 engine's own values, an FP32 engine's widened.
+ * No counterpart in the reference (whose vectors are float). */
+ep_status ep_get_component_gradients_f64(ep_engine *e, double *density_xy, double *wirelength_xy);
 /* Bin maps of the last evaluation, x-major [bins_x][bins_y] (keep_maps must
  * be set for node/filler/field): nodeDensity, fillerDensity,
  * terminalDensity, baseDensity (areas), E.x, E.y, phi.  Any may be NULL. */
 ep_status ep_get_bin_maps(ep_engine *e, float *node, float *filler, float *terminal, float *base,
                           float *ex, float *ey, float *phi);
+/* E.x, E.y and phi of the last evaluation in double (keep_maps must be set);
+ * any may be NULL.  No counterpart in the reference. */
+ep_status ep_get_field_f64(ep_engine *e, double *ex, double *ey, double *phi);
 /* Raw fixed-point node / filler maps (int64, units of 1/density_scale). */
 ep_status ep_get_density_fixed(ep_engine *e, int64_t *node, int64_t *filler);
 

@@ -194,29 +194,40 @@ def record_variants():
 
 
 def record_bench_reference():
-    """The reference's whole mGP run on bench.py's 200k-cell design (about a
-    minute of CPU): iterations to overflow < 0.1, final overflow and HPWL.
-    bench.py scales its bounded CPU samples by this iteration count."""
+    """The reference's whole runs on bench.py's 200k-cell design (a few
+    minutes of CPU): from its own quadratic placement (QPPlacer, as its flow
+    starts) and from bench.design()'s seeded blob; iterations to overflow
+    < 0.1, final overflow and HPWL, and the stage times."""
     import json
     import time
     sys.path.insert(0, ROOT)
     import bench
-    nl = bench.design()
-    ref = R.RefPlacer(nl)
-    t0 = time.time()
-    ref.initialization(1.0)
-    t_init = time.time() - t0
-    t0 = time.time()
-    ref.opt_run()
-    t_mgp = time.time() - t0
-    i = ref.info()
-    out = {"stdcell_200k_mgp": dict(iterations=int(i["iter_count"]), overflow=float(i["overflow"]),
-                                    hpwl=float(ref.hpwl()), fillers=int(i["num_fillers"]),
-                                    bins=int(i["bins_x"]), init_seconds=t_init, mgp_seconds=t_mgp,
-                                    note="reference CPU path, 1 thread, build container")}
+    out = {}
+    for key, nl, qp in (("stdcell_200k_qp_mgp", bench.netlist(), True),
+                        ("stdcell_200k_blob_mgp", bench.design(), False)):
+        ref = R.RefPlacer(nl)
+        t_qp = 0.0
+        rec = {}
+        if qp:
+            t0 = time.time()
+            ref.qp()
+            t_qp = time.time() - t0
+            rec["qp_hpwl"] = float(ref.hpwl())
+        t0 = time.time()
+        ref.initialization(1.0)
+        t_init = time.time() - t0
+        t0 = time.time()
+        ref.opt_run()
+        t_mgp = time.time() - t0
+        i = ref.info()
+        rec.update(iterations=int(i["iter_count"]), overflow=float(i["overflow"]), hpwl=float(ref.hpwl()),
+                   fillers=int(i["num_fillers"]), bins=int(i["bins_x"]), qp_seconds=t_qp, init_seconds=t_init,
+                   mgp_seconds=t_mgp, note="reference CPU path, 1 thread")
+        out[key] = rec
+        ref.close()
+        print(key, rec, flush=True)
     with open(os.path.join(HERE, "reference_runs.json"), "w") as f:
         json.dump(out, f, indent=1)
-    print(out)
 
 
 if __name__ == "__main__":

@@ -27,12 +27,13 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults():
     L = placer.load()
-    assert L.ep_abi_version() == 1
+    assert L.ep_abi_version() == placer.ABI_VERSION == 2
     p = placer.default_params()
     assert p.target_density == pytest.approx(1.0)
     assert p.target_overflow == pytest.approx(0.10)
     assert p.max_iterations == 1000
     assert p.dct_mode == placer.DCT_AUTO and p.exp_mode == placer.EXP_FAST
+    assert p.precision == placer.PREC_MIXED
 
 
 def _bad_netlist(mutate):
