@@ -10,6 +10,7 @@
 // then laid out on the device as SoA arrays plus two CSRs (net -> pins,
 // object -> pins) and the loop of kernels.cu / dct.cu runs there.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -91,6 +92,12 @@ struct ep_engine {
     bool has_snap = false;
     // quadratic placement (qp.cu): net -> first device pin / pins, pin -> net
     std::vector<int32_t> h_net_first, h_net_deg, h_pin_net;
+    // owner of each pin in device order (object index, terminals n_obj + t) and
+    // the movable nodes' areas and pin counts, for the learned warm start
+    std::vector<int32_t> h_pin_owner;
+    std::vector<float> h_node_area, h_node_pins;
+    std::vector<float2> h_term_centre;
+    uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
     size_t qp_cap_x = 0, qp_cap_y = 0;
@@ -824,6 +831,10 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         }
     }
     // quadratic placement: nets in device order
+    e->h_pin_owner = dev_owner;
+    e->h_term_centre.assign(pos.begin() + no, pos.end());
+    e->h_node_area.assign(h_area.begin(), h_area.begin() + nn);
+    e->h_node_pins.assign(h_npins.begin(), h_npins.begin() + nn);
     e->h_net_first.assign(nnet, 0);
     e->h_net_deg.assign(nnet, 0);
     e->h_pin_net.assign(np, 0);
@@ -979,6 +990,8 @@ ep_status ep_create(const ep_netlist *nl, const ep_params *params, ep_engine **o
         return EP_ERR_NOMEM;
     }
     *out = e;
+    static std::atomic<uint64_t> next_uid{1};
+    e->uid = next_uid++;
     try {
         return create_engine(e, nl, params);
     } catch (const std::bad_alloc &) {
@@ -2011,3 +2024,48 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
 }
 
 }  // extern "C"
+
+// ---- views of an engine for other translation units (gnn.cu) ----------------
+namespace ep {
+
+int engine_graph(ep_engine *e, EngineGraph *g) {
+    if (!e || !g) return EP_ERR_ARG;
+    g->uid = e->uid;
+    g->nn = e->n_nodes;
+    g->n_obj = e->n_obj;
+    g->nt = e->n_terms;
+    g->nnet = e->n_nets;
+    g->np = e->n_pins;
+    g->pin_owner = e->h_pin_owner.data();
+    g->net_first = e->h_net_first.data();
+    g->net_deg = e->h_net_deg.data();
+    g->pin_net = e->h_pin_net.data();
+    g->node_area = e->h_node_area.data();
+    g->node_pins = e->h_node_pins.data();
+    g->term_centre = e->h_term_centre.data();
+    g->grid = e->grid;
+    g->st = e->st;
+    g->device = e->device;
+    return EP_OK;
+}
+
+// The movable nodes at these device-resident float2 centres (nn of them),
+// clamped into the core and stored in the engine's working precision.
+int engine_set_node_centres(ep_engine *e, const float2 *xy) {
+    const int n = e->n_nodes;
+    if (n == 0) return EP_OK;
+    if (e->fp64)
+        k_scatter_view<double><<<(n + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[EP_STAGE_MGP], n, xy, e->size,
+                                                                   (double2 *)e->pos);
+    else
+        k_scatter_view<float><<<(n + 255) / 256, 256, 0, e->st>>>(e->grid, e->view_idx[EP_STAGE_MGP], n, xy, e->size,
+                                                                  (float2 *)e->pos);
+    e->initialized = false;
+    return cudaGetLastError() == cudaSuccess ? EP_OK : EP_ERR_CUDA;
+}
+
+void engine_set_error(ep_engine *e, const char *msg) {
+    if (e) e->err.assign(msg);
+}
+
+}  // namespace ep

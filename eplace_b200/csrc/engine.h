@@ -173,6 +173,25 @@ void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, void *pos, const
 // updatePenaltyFactor rule, mode 2 applies it only if a lambda update is pending.
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S, cudaStream_t st);
 
+// ---- an engine's netlist for the learned warm start (gnn.cu) ------------------
+// Host arrays owned by the engine; valid while it lives.
+struct EngineGraph {
+    uint64_t uid;                        // distinct per engine in this process
+    int nn, n_obj, nt, nnet, np;         // movable nodes, objects, terminals, nets, pins
+    const int32_t *pin_owner;            // [np] device pin order: object index, or n_obj + terminal
+    const int32_t *net_first, *net_deg;  // [nnet] first device pin and pin count of each net
+    const int32_t *pin_net;              // [np] net of each device pin
+    const float *node_area, *node_pins;  // [nn]
+    const float2 *term_centre;           // [nt]
+    Grid grid;
+    cudaStream_t st;
+    int device;
+};
+int engine_graph(ep_engine *e, EngineGraph *g);
+// Movable-node centres from a device float2 array (clamped into the core).
+int engine_set_node_centres(ep_engine *e, const float2 *xy);
+void engine_set_error(ep_engine *e, const char *msg);
+
 // ---- quadratic placement (qp.cu) ---------------------------------------------
 // Device view of one engine's quadratic placement: the netlist in device pin
 // order (nets contiguous) plus the per-round systems and BiCGSTAB vectors,

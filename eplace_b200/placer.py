@@ -115,6 +115,9 @@ EXPORTS = (
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_positions_f64", "ep_get_field_f64", "ep_get_component_gradients_f64",
     "ep_get_limits", "ep_set_limits",
+    "ep_gnn_num_weights", "ep_gnn_create", "ep_gnn_destroy", "ep_gnn_last_error", "ep_gnn_get_weights",
+    "ep_gnn_set_weights", "ep_gnn_release", "ep_gnn_features", "ep_gnn_forward", "ep_gnn_loss_grad",
+    "ep_gnn_train_step", "ep_gnn_propose",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
@@ -191,6 +194,20 @@ def load():
     L.ep_get_component_gradients.argtypes = [vp, _f32p, _f32p]
     L.ep_get_component_gradients_f64.argtypes = [vp, _f64p, _f64p]
     L.ep_get_limits.argtypes = [vp, ctypes.POINTER(Limits)]
+    L.ep_gnn_num_weights.restype = ctypes.c_int32
+    L.ep_gnn_create.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.ep_gnn_destroy.argtypes = [vp]
+    L.ep_gnn_destroy.restype = None
+    L.ep_gnn_last_error.argtypes = [vp]
+    L.ep_gnn_last_error.restype = ctypes.c_char_p
+    L.ep_gnn_get_weights.argtypes = [vp, _f32p]
+    L.ep_gnn_set_weights.argtypes = [vp, _f32p]
+    L.ep_gnn_release.argtypes = [vp, vp]
+    L.ep_gnn_features.argtypes = [vp, vp, _f32p]
+    L.ep_gnn_forward.argtypes = [vp, vp, _f32p]
+    L.ep_gnn_loss_grad.argtypes = [vp, vp, _f32p, ctypes.POINTER(ctypes.c_double), _f32p]
+    L.ep_gnn_train_step.argtypes = [vp, vp, _f32p, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
+    L.ep_gnn_propose.argtypes = [vp, vp, ctypes.c_float]
     L.ep_set_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     L.ep_get_positions_f64.argtypes = [vp, ctypes.c_int32, _f64p, ctypes.c_int32]
     L.ep_get_field_f64.argtypes = [vp, _f64p, _f64p, _f64p]
@@ -643,3 +660,81 @@ class EplaceNesterovOpt:
     def opt(self, max_steps=0):
         self.last_run = self.placer.engine.nesterov_run(max_steps)
         return self.last_run
+
+
+class Gnn:
+    """The learned warm start (ep_gnn_*): a message-passing network that
+    proposes an initial placement for an Engine."""
+
+    FEATURES = 9
+
+    def __init__(self, device=0, seed=1, weights=None):
+        self._L = load()
+        self.h = ctypes.c_void_p()
+        rc = self._L.ep_gnn_create(int(device), int(seed), ctypes.byref(self.h))
+        if rc != EP_OK:
+            msg = self._L.ep_gnn_last_error(self.h).decode() if self.h.value else ""
+            self.close()
+            raise EPError(rc, f"ep_gnn_create: {msg}")
+        if weights is not None:
+            self.set_weights(weights)
+
+    def _check(self, rc):
+        if rc != EP_OK:
+            raise EPError(rc, self._L.ep_gnn_last_error(self.h).decode())
+
+    @property
+    def num_weights(self):
+        return int(self._L.ep_gnn_num_weights())
+
+    def get_weights(self):
+        w = np.zeros(self.num_weights, np.float32)
+        self._check(self._L.ep_gnn_get_weights(self.h, _p(w, _f32p)))
+        return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        if w.shape != (self.num_weights,):
+            raise ValueError(f"expected {self.num_weights} weights")
+        self._check(self._L.ep_gnn_set_weights(self.h, _p(w, _f32p)))
+
+    def release(self, engine):
+        self._check(self._L.ep_gnn_release(self.h, engine.h))
+
+    def features(self, engine):
+        i = engine.info
+        x = np.zeros((i.num_nodes + i.num_terminals, self.FEATURES), np.float32)
+        self._check(self._L.ep_gnn_features(self.h, engine.h, _p(x, _f32p)))
+        return x
+
+    def forward(self, engine):
+        xy = np.zeros((engine.info.num_nodes, 2), np.float32)
+        self._check(self._L.ep_gnn_forward(self.h, engine.h, _p(xy, _f32p)))
+        return xy
+
+    def loss_grad(self, engine, target_xy):
+        t = np.ascontiguousarray(target_xy, np.float32)
+        loss = ctypes.c_double()
+        g = np.zeros(self.num_weights, np.float32)
+        self._check(self._L.ep_gnn_loss_grad(self.h, engine.h, _p(t, _f32p), ctypes.byref(loss), _p(g, _f32p)))
+        return loss.value, g
+
+    def train_step(self, engine, target_xy, lr):
+        t = np.ascontiguousarray(target_xy, np.float32)
+        loss = ctypes.c_double()
+        self._check(self._L.ep_gnn_train_step(self.h, engine.h, _p(t, _f32p), float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def propose(self, engine, alpha=1.0):
+        self._check(self._L.ep_gnn_propose(self.h, engine.h, float(alpha)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self._L.ep_gnn_destroy(self.h)
+        self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
