@@ -97,6 +97,9 @@ struct ep_engine {
     std::vector<int32_t> h_pin_owner;
     std::vector<float> h_node_area, h_node_pins;
     std::vector<float2> h_term_centre;
+    // device copies of the net -> device pins and pin -> net maps (made at
+    // creation; the quadratic placement and the learned warm start read them)
+    int32_t *net_first = nullptr, *net_deg = nullptr, *pin_net = nullptr;
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
@@ -901,6 +904,9 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     CK(cudaGetLastError());
     for (int v = 0; v < 3; v++)
         if ((s = dupload(e, e->view_idx[v], e->h_view[v]))) return s;
+    if ((s = dupload(e, e->net_first, e->h_net_first)) || (s = dupload(e, e->net_deg, e->h_net_deg)) ||
+        (s = dupload(e, e->pin_net, e->h_pin_net)))
+        return s;
     if (P.step_rule == EP_STEP_BKTRK &&
         ((s = dalloc_bytes(e, e->bk_ysave, v2 * no)) || (s = dalloc_bytes(e, e->bk_gtrial, v2 * no)) ||
          (s = dalloc_bytes(e, e->bk_xtrial, v2 * no))))
@@ -1814,14 +1820,13 @@ ep_status qp_setup(ep_engine *e) {
     q.obj_pin_dev = e->obj_pin_dev;
     q.owner = e->pin_owner;
     q.off = e->pin_off;
-    int32_t *pin_net = nullptr, *net_first = nullptr, *net_deg = nullptr;
+
     // at most 4 entries per pin and axis: every counted pair of a net involves
     // one of its two bound pins (< 2 d pairs, two entries each)
     const size_t cap = 4 * (size_t)np + 16;
     const int pb = qp_partial_blocks(nn, nnet);
     ep_status s;
-    if ((s = dupload(e, pin_net, e->h_pin_net)) || (s = dupload(e, net_first, e->h_net_first)) ||
-        (s = dupload(e, net_deg, e->h_net_deg)) || (s = dalloc(e, q.bound, std::max(nnet, 1))) ||
+    if ((s = dalloc(e, q.bound, std::max(nnet, 1))) ||
         (s = dalloc(e, q.count, 2 * (size_t)nn)) || (s = dalloc(e, q.row_x, (size_t)nn + 1)) ||
         (s = dalloc(e, q.row_y, (size_t)nn + 1)) || (s = dalloc(e, q.col_x, cap)) || (s = dalloc(e, q.col_y, cap)) ||
         (s = dalloc(e, q.val_x, cap)) || (s = dalloc(e, q.val_y, cap)) || (s = dalloc(e, q.diag, nn)) ||
@@ -1830,9 +1835,9 @@ ep_status qp_setup(ep_engine *e) {
         (s = dalloc(e, q.s, nn)) || (s = dalloc(e, q.t, nn)) || (s = dalloc(e, q.partials, 4 * (size_t)pb)) ||
         (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)))
         return s;
-    q.pin_net = pin_net;
-    q.net_first = net_first;
-    q.net_deg = net_deg;
+    q.pin_net = e->pin_net;
+    q.net_first = e->net_first;
+    q.net_deg = e->net_deg;
     CK(cudaMemset(q.cnt, 0, sizeof(unsigned)));
     CK(cudaMallocHost((void **)&e->qp_out_h, 4 * sizeof(double)));
     e->qp_cap_x = e->qp_cap_y = cap;
@@ -2040,6 +2045,16 @@ int engine_graph(ep_engine *e, EngineGraph *g) {
     g->net_first = e->h_net_first.data();
     g->net_deg = e->h_net_deg.data();
     g->pin_net = e->h_pin_net.data();
+    g->d_pin_owner = e->pin_owner;
+    g->d_net_first = e->net_first;
+    g->d_net_deg = e->net_deg;
+    g->d_pin_net = e->pin_net;
+    g->d_obj_pin_start = e->obj_pin_start;
+    g->d_obj_pin_dev = e->obj_pin_dev;
+    g->d_area = e->area;
+    g->d_npins = e->npins;
+    g->d_pos = e->pos;
+    g->fp64 = e->fp64;
     g->node_area = e->h_node_area.data();
     g->node_pins = e->h_node_pins.data();
     g->term_centre = e->h_term_centre.data();

@@ -183,6 +183,12 @@ struct EngineGraph {
     const int32_t *pin_net;              // [np] net of each device pin
     const float *node_area, *node_pins;  // [nn]
     const float2 *term_centre;           // [nt]
+    // the same netlist on the device
+    const int32_t *d_pin_owner, *d_net_first, *d_net_deg, *d_pin_net;
+    const int32_t *d_obj_pin_start, *d_obj_pin_dev;  // object -> its device pins
+    const float *d_area, *d_npins;                   // [n_obj]
+    const void *d_pos;                               // [n_obj + nt] centres, vec2<R>
+    int fp64;
     Grid grid;
     cudaStream_t st;
     int device;

@@ -4,39 +4,41 @@
 // which stays the fallback and the judge.  No counterpart in the reference.
 //
 // Graph: the movable nodes (0..nn-1) and the terminals (nn..nn+nt-1) of an
-// engine; a net joins the nodes of its pins.  Two mean aggregations:
+// engine, read from the engine's device arrays (nets contiguous in device
+// pin order, each object's pins through its object -> pin map); a net joins
+// the nodes of its pins.  Two mean aggregations:
 //   net_mean   a[n] = mean over the pins of net n of h[node(pin)]
 //   node_mean  m[c] = mean over the pins of movable node c of a[net(pin)]
 //                     (terminals receive nothing: m = 0)
 //
-// Features (kF per node, from the netlist alone): log(1 + area) / 4,
-// log(1 + pins) / 3, terminal flag, and the node's coordinates (normalised
-// to the core) after 16, 64 and 256 steps of pad-anchored diffusion -- every
-// movable node starts at the core centre, terminals sit at their own
-// centres, and a step replaces each movable node by node_mean(net_mean(.)).
-// These are the fixed-pin distances the network reads: a node's diffused
-// coordinate says how its pads pull it, at three ranges.
+// Features (kF per node, from the netlist alone, computed on the device):
+// log(1 + area) / 4, log(1 + pins) / 3, terminal flag, and the node's
+// coordinates (normalised to the core) after 32, 128 and 512 steps of
+// pad-anchored diffusion: every movable node starts at the core centre,
+// terminals sit at their own centres, and a step replaces each movable node
+// by node_mean(net_mean(.)).  These are the fixed-pin distances the network
+// reads: a node's diffused coordinate says how its pads pull it, at three
+// ranges; d, the 512-step coordinates, is the base of the predictions.
 //
 // Network (hidden 64, weights stored BF16 for the forward pass, FP32
 // accumulate, FP32 master weights for training):
 //   h0 = relu(W0 x + b0)
 //   h_l = relu(W_l [h_{l-1} ; node_mean(net_mean(h_{l-1}))] + b_l),  l = 1..3
-//   pred = d256 + 0.25 tanh(W4 h3 + b4)       (normalised core coordinates)
-// so the network outputs a bounded correction to the 256-step diffusion.
-// Training: mean squared error to the engine's own final mGP placement
-// (normalised), Adam; every reduction (weight gradients, loss) is a per-block
+//   q = d + 0.25 tanh(W4[0:2] h3 + b4[0:2])   the engine's quadratic placement
+//   f = d + 0.25 tanh(W4[2:4] h3 + b4[2:4])   the engine's final mGP placement
+// (normalised core coordinates).  Training: the mean squared error of both
+// heads against the engine's own quadratic placement and final placement of
+// the design, Adam; every reduction (weight gradients, loss) is a per-block
 // partial summed in a fixed order, so a training step is bitwise repeatable.
-// A proposal moves the movable nodes to d256 + alpha * (pred - d256), mapped
-// to the core.
+// A proposal moves the movable nodes to q + alpha (f - q), mapped to the
+// core: the quadratic placement's compact layout moved part of the way to
+// where the optimizer ends.
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <memory>
-#include <mutex>
 #include <random>
-#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -44,18 +46,19 @@
 namespace ep {
 namespace {
 
-constexpr int kH = 64;        // hidden width
-constexpr int kF = 9;         // input features
-constexpr int kLayers = 3;    // message-passing layers
-constexpr int kDiffSteps[3] = {16, 64, 256};
-constexpr float kCorr = 0.25f;  // bound of the correction, in core sizes
+constexpr int kH = 64;      // hidden width
+constexpr int kF = 9;       // input features
+constexpr int kOut = 4;     // q (x, y), f (x, y)
+constexpr int kLayers = 3;  // message-passing layers
+constexpr int kDiffSteps[3] = {32, 128, 512};
+constexpr float kCorr = 0.25f;  // bound of a head's correction, in core sizes
 
 // Parameter layout (floats): W0[kH][kF], b0[kH], per layer W[kH][2kH], b[kH],
-// then W4[2][kH], b4[2].
+// then W4[kOut][kH], b4[kOut].
 constexpr int kOffW0 = 0, kOffB0 = kOffW0 + kH * kF, kOffL = kOffB0 + kH;
 constexpr int kLayerParams = kH * 2 * kH + kH;
-constexpr int kOffW4 = kOffL + kLayers * kLayerParams, kOffB4 = kOffW4 + 2 * kH;
-constexpr int kParams = kOffB4 + 2;
+constexpr int kOffW4 = kOffL + kLayers * kLayerParams, kOffB4 = kOffW4 + kOut * kH;
+constexpr int kParams = kOffB4 + kOut;
 inline int off_w(int l) { return kOffL + (l - 1) * kLayerParams; }
 inline int off_b(int l) { return off_w(l) + kH * 2 * kH; }
 
@@ -63,62 +66,77 @@ constexpr int kT = 256;
 constexpr int kRowsPerBlock = 512;  // rows of one partial weight gradient
 inline int nblk(long long n, int t = kT) { return (int)((n + t - 1) / t); }
 
-// ---------------------------------------------------------------- graph ----
-struct Graph {
-    uint64_t uid = 0;
-    int nn = 0, nt = 0, N = 0, nnet = 0, np = 0;
-    int32_t *net_first = nullptr, *net_deg = nullptr, *pin_node = nullptr;
-    int32_t *node_pin_start = nullptr, *node_pin_net = nullptr;
-    float *inv_deg = nullptr, *inv_pins = nullptr;
-    float *X = nullptr;      // [N][kF]
-    float2 *d256 = nullptr;  // [N] 256-step diffusion (base of the prediction)
-    float *h[kLayers + 1] = {};  // [N][kH]
-    float *a = nullptr;          // [nnet][kH] (recomputed in the backward pass)
-    float *m[kLayers + 1] = {};  // [N][kH], m[l] for layer l
-    float2 *raw = nullptr, *pred = nullptr, *dout = nullptr, *target = nullptr;  // [N]
-    float *dh = nullptr, *dx = nullptr, *dm = nullptr, *da = nullptr;
-    float *partial = nullptr;  // per-block partial weight gradients
-    size_t partial_floats = 0;
-    double *loss_part = nullptr;
-    std::vector<void *> allocs;
-    ~Graph() {
-        for (void *p : allocs) cudaFree(p);
-    }
-    template <typename T>
-    bool alloc(T *&p, size_t n) {
-        if (cudaMalloc((void **)&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
-            p = nullptr;
-            return false;
-        }
-        allocs.push_back(p);
-        return true;
-    }
+// Device view of the bound netlist.
+struct Net {
+    int nn, n_obj, N, nnet;
+    const int32_t *owner, *net_first, *net_deg, *pin_net, *obj_pin_start, *obj_pin_dev;
+    const int32_t *pad_start, *pad_net;  // terminals' pins (training only; may be null)
 };
 
+__device__ __forceinline__ int node_of(int o, int nn, int n_obj) { return o < nn ? o : nn + (o - n_obj); }
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
 
-// --------------------------------------------------------- diffusion ------
-__global__ void k_diff_net(int nnet, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
-                           const int32_t *__restrict__ pin_node, const float *__restrict__ inv_deg,
-                           const float2 *__restrict__ v, float2 *__restrict__ a) {
+// ------------------------------------------------------------ features ----
+template <typename R>
+__global__ void k_init(Net g, const float *__restrict__ area, const float *__restrict__ npins,
+                       const vec2<R> *__restrict__ pos, Grid gr, float *__restrict__ X, float2 *__restrict__ v,
+                       float *__restrict__ inv_pins) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.N) return;
+    float *x = X + (size_t)c * kF;
+#pragma unroll
+    for (int k = 0; k < kF; k++) x[k] = 0.f;
+    if (c < g.nn) {
+        x[0] = log1pf(area[c]) * 0.25f;
+        x[1] = log1pf(npins[c]) * (1.f / 3.f);
+        v[c] = make_float2(0.5f, 0.5f);
+        inv_pins[c] = npins[c] > 0.f ? 1.f / npins[c] : 0.f;
+    } else {
+        const vec2<R> t = pos[g.n_obj + (c - g.nn)];
+        x[2] = 1.f;
+        v[c] = make_float2((float)(((double)t.x - gr.llx) / ((double)gr.urx - gr.llx)),
+                           (float)(((double)t.y - gr.lly) / ((double)gr.ury - gr.lly)));
+        inv_pins[c] = 0.f;
+    }
+}
+
+__global__ void k_pad_pins(int np, Net g, int *__restrict__ cnt) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np && g.owner[p] >= g.n_obj) atomicAdd(&cnt[g.owner[p] - g.n_obj], 1);
+}
+
+__global__ void k_pad_feature(int nt, int nn, const int *__restrict__ cnt, float *__restrict__ X) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nt) X[(size_t)(nn + t) * kF + 1] = log1pf((float)cnt[t]) * (1.f / 3.f);
+}
+
+__global__ void k_inv_deg(int nnet, const int32_t *__restrict__ deg, float *__restrict__ inv) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= nnet) return;
+    if (n < nnet) inv[n] = deg[n] > 0 ? 1.f / deg[n] : 0.f;
+}
+
+__global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ v,
+                           float2 *__restrict__ a) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.nnet) return;
     float sx = 0.f, sy = 0.f;
-    for (int p = first[n], e = p + deg[n]; p < e; p++) {
-        const float2 q = v[pin_node[p]];
+    for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
+        const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
         sx += q.x;
         sy += q.y;
     }
     a[n] = make_float2(sx * inv_deg[n], sy * inv_deg[n]);
 }
 
-__global__ void k_diff_node(int nn, const int32_t *__restrict__ start, const int32_t *__restrict__ pin_net,
-                            const float *__restrict__ inv_pins, const float2 *__restrict__ a, float2 *__restrict__ v) {
+__global__ void k_diff_node(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ a,
+                            float2 *__restrict__ v) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nn || start[c + 1] == start[c]) return;
+    if (c >= g.nn) return;
+    const int q0 = g.obj_pin_start[c], q1 = g.obj_pin_start[c + 1];
+    if (q1 == q0) return;
     float sx = 0.f, sy = 0.f;
-    for (int q = start[c]; q < start[c + 1]; q++) {
-        const float2 t = a[pin_net[q]];
+    for (int q = q0; q < q1; q++) {
+        const float2 t = a[g.pin_net[g.obj_pin_dev[q]]];
         sx += t.x;
         sy += t.y;
     }
@@ -134,28 +152,27 @@ __global__ void k_store_feature(int N, const float2 *__restrict__ v, float *__re
 
 // ------------------------------------------------------ aggregations ------
 // One warp per row, a float2 of channels per lane.
-__global__ void k_net_mean(int nnet, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
-                           const int32_t *__restrict__ pin_node, const float *__restrict__ inv_deg,
-                           const float2 *__restrict__ h, float2 *__restrict__ a) {
+__global__ void k_net_mean(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ h,
+                           float2 *__restrict__ a) {
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (n >= nnet) return;
+    if (n >= g.nnet) return;
     float2 s = make_float2(0.f, 0.f);
-    for (int p = first[n], e = p + deg[n]; p < e; p++) {
-        const float2 q = h[(size_t)pin_node[p] * 32 + lane];
+    for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
+        const float2 q = h[(size_t)node_of(g.owner[p], g.nn, g.n_obj) * 32 + lane];
         s.x += q.x;
         s.y += q.y;
     }
     a[(size_t)n * 32 + lane] = make_float2(s.x * inv_deg[n], s.y * inv_deg[n]);
 }
 
-__global__ void k_node_mean(int N, int nn, const int32_t *__restrict__ start, const int32_t *__restrict__ pin_net,
-                            const float *__restrict__ inv_pins, const float2 *__restrict__ a, float2 *__restrict__ m) {
+__global__ void k_node_mean(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ a,
+                            float2 *__restrict__ m) {
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (c >= N) return;
+    if (c >= g.N) return;
     float2 s = make_float2(0.f, 0.f);
-    if (c < nn) {
-        for (int q = start[c]; q < start[c + 1]; q++) {
-            const float2 t = a[(size_t)pin_net[q] * 32 + lane];
+    if (c < g.nn) {
+        for (int q = g.obj_pin_start[c]; q < g.obj_pin_start[c + 1]; q++) {
+            const float2 t = a[(size_t)g.pin_net[g.obj_pin_dev[q]] * 32 + lane];
             s.x += t.x;
             s.y += t.y;
         }
@@ -166,15 +183,14 @@ __global__ void k_node_mean(int N, int nn, const int32_t *__restrict__ start, co
 }
 
 // transpose of node_mean: da[n] = sum over the pins of n on movable nodes c of dm[c] / pins(c)
-__global__ void k_node_mean_t(int nnet, int nn, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
-                              const int32_t *__restrict__ pin_node, const float *__restrict__ inv_pins,
-                              const float2 *__restrict__ dm, float2 *__restrict__ da) {
+__global__ void k_node_mean_t(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ dm,
+                              float2 *__restrict__ da) {
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (n >= nnet) return;
+    if (n >= g.nnet) return;
     float2 s = make_float2(0.f, 0.f);
-    for (int p = first[n], e = p + deg[n]; p < e; p++) {
-        const int c = pin_node[p];
-        if (c >= nn) continue;
+    for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
+        const int c = node_of(g.owner[p], g.nn, g.n_obj);
+        if (c >= g.nn) continue;
         const float2 t = dm[(size_t)c * 32 + lane];
         s.x += t.x * inv_pins[c];
         s.y += t.y * inv_pins[c];
@@ -183,17 +199,26 @@ __global__ void k_node_mean_t(int nnet, int nn, const int32_t *__restrict__ firs
 }
 
 // transpose of net_mean, added: dh[c] += sum over the pins of node c of da[net] / deg(net)
-__global__ void k_net_mean_t_add(int N, const int32_t *__restrict__ start, const int32_t *__restrict__ pin_net,
-                                 const float *__restrict__ inv_deg, const float2 *__restrict__ da,
+__global__ void k_net_mean_t_add(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ da,
                                  float2 *__restrict__ dh) {
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (c >= N) return;
+    if (c >= g.N) return;
     float2 s = make_float2(0.f, 0.f);
-    for (int q = start[c]; q < start[c + 1]; q++) {
-        const int n = pin_net[q];
-        const float2 t = da[(size_t)n * 32 + lane];
-        s.x += t.x * inv_deg[n];
-        s.y += t.y * inv_deg[n];
+    if (c < g.nn) {
+        for (int q = g.obj_pin_start[c]; q < g.obj_pin_start[c + 1]; q++) {
+            const int n = g.pin_net[g.obj_pin_dev[q]];
+            const float2 t = da[(size_t)n * 32 + lane];
+            s.x += t.x * inv_deg[n];
+            s.y += t.y * inv_deg[n];
+        }
+    } else {
+        const int t0 = c - g.nn;
+        for (int q = g.pad_start[t0]; q < g.pad_start[t0 + 1]; q++) {
+            const int n = g.pad_net[q];
+            const float2 t = da[(size_t)n * 32 + lane];
+            s.x += t.x * inv_deg[n];
+            s.y += t.y * inv_deg[n];
+        }
     }
     float2 &o = dh[(size_t)c * 32 + lane];
     o.x += s.x;
@@ -201,9 +226,10 @@ __global__ void k_net_mean_t_add(int N, const int32_t *__restrict__ start, const
 }
 
 // ------------------------------------------------------------ dense -------
-// Y[r][o] = act(b[o] + sum_k X[r][k] W[o][k]) with X = [XA (KA cols) | XB (KB
-// cols)], W BF16 [kH][KA+KB].  64 rows per 256-thread block, W (transposed)
-// and the rows staged in shared memory; a thread owns one row, 16 outputs.
+// Y[r][o] = relu(b[o] + sum_k X[r][k] W[o][k]) with X = [XA (KA cols) | XB
+// (KB cols)], W BF16 [kH][KA+KB].  64 rows per 256-thread block, W
+// (transposed) and the rows staged in shared memory; a thread owns one row,
+// 16 outputs.
 template <int KA, int KB>
 __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ XA, const float *__restrict__ XB,
                                               const __nv_bfloat16 *__restrict__ W, const float *__restrict__ b,
@@ -239,15 +265,15 @@ __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ X
     }
 }
 
-// dX = (dY .* (Y > 0)) W, split into dXA (KA cols, stored) and dXB (KB cols, stored).
+// dX = (dY .* (Y > 0)) W, split into dXA (KA cols) and dXB (KB cols).
 template <int KA, int KB>
 __global__ void __launch_bounds__(kT) k_dense_dx(int N, const float *__restrict__ dY, const float *__restrict__ Y,
                                                  const __nv_bfloat16 *__restrict__ W, float *__restrict__ dXA,
                                                  float *__restrict__ dXB) {
     constexpr int K = KA + KB, PER = (K + 3) / 4;
     extern __shared__ float sm[];
-    float *Ws = sm;            // [kH][K]
-    float *Zs = sm + kH * K;   // [64][kH + 1]
+    float *Ws = sm;           // [kH][K]
+    float *Zs = sm + kH * K;  // [64][kH + 1]
     for (int i = threadIdx.x; i < kH * K; i += kT) Ws[i] = bf(W[i]);
     const int r0 = blockIdx.x * 64;
     for (int i = threadIdx.x; i < 64 * kH; i += kT) {
@@ -349,39 +375,50 @@ __global__ void k_reduce_partials(int blocks, int OK, int O, const float *__rest
 }
 
 // ------------------------------------------------------------ output ------
+// raw = W4 h + b4; pred = d + 0.25 tanh(raw) for both heads.
 __global__ void k_output(int N, const float *__restrict__ h, const __nv_bfloat16 *__restrict__ W4,
-                         const float *__restrict__ b4, const float2 *__restrict__ base, float2 *__restrict__ raw,
-                         float2 *__restrict__ pred) {
+                         const float *__restrict__ b4, const float2 *__restrict__ base, float4 *__restrict__ raw,
+                         float4 *__restrict__ pred) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
-    float rx = b4[0], ry = b4[1];
+    float r[kOut];
+#pragma unroll
+    for (int j = 0; j < kOut; j++) r[j] = b4[j];
     const float *hc = h + (size_t)c * kH;
 #pragma unroll 8
     for (int k = 0; k < kH; k++) {
-        rx = fmaf(hc[k], bf(W4[k]), rx);
-        ry = fmaf(hc[k], bf(W4[kH + k]), ry);
+        const float x = hc[k];
+#pragma unroll
+        for (int j = 0; j < kOut; j++) r[j] = fmaf(x, bf(W4[j * kH + k]), r[j]);
     }
-    raw[c] = make_float2(rx, ry);
+    raw[c] = make_float4(r[0], r[1], r[2], r[3]);
     const float2 b = base[c];
-    pred[c] = make_float2(b.x + kCorr * tanhf(rx), b.y + kCorr * tanhf(ry));
+    pred[c] = make_float4(b.x + kCorr * tanhf(r[0]), b.y + kCorr * tanhf(r[1]), b.x + kCorr * tanhf(r[2]),
+                          b.y + kCorr * tanhf(r[3]));
 }
 
-// Loss (squared error summed over the movable nodes, per-block partial) and
-// d loss / d raw for the mean over nodes and coordinates.
-__global__ void k_loss(int N, int nn, const float2 *__restrict__ raw, const float2 *__restrict__ pred,
-                       const float2 *__restrict__ target, float2 *__restrict__ dout, double *__restrict__ part) {
+// Loss: the squared errors of both heads over the movable nodes, divided by
+// 2 nn (per-block partials), and d loss / d raw.
+__global__ void k_loss(int N, int nn, const float4 *__restrict__ raw, const float4 *__restrict__ pred,
+                       const float4 *__restrict__ target, float4 *__restrict__ dout, double *__restrict__ part) {
     __shared__ double sh[kT / 32];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double l = 0.0;
     if (c < N) {
-        float2 d = make_float2(0.f, 0.f);
+        float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c < nn) {
-            const float2 p = pred[c], t = target[c], r = raw[c];
-            const float ex = p.x - t.x, ey = p.y - t.y;
-            l = (double)ex * ex + (double)ey * ey;
-            const float s = 2.f / (2.f * nn);
-            const float tx = tanhf(r.x), ty = tanhf(r.y);
-            d = make_float2(s * ex * kCorr * (1.f - tx * tx), s * ey * kCorr * (1.f - ty * ty));
+            const float4 p = pred[c], t = target[c], r = raw[c];
+            const float e[4] = {p.x - t.x, p.y - t.y, p.z - t.z, p.w - t.w};
+            const float rr[4] = {r.x, r.y, r.z, r.w};
+            float dd[4];
+            const float s = 1.f / (float)nn;  // d/dp of e^2 / (2 nn)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                l += (double)e[j] * e[j];
+                const float th = tanhf(rr[j]);
+                dd[j] = s * e[j] * kCorr * (1.f - th * th);
+            }
+            d = make_float4(dd[0], dd[1], dd[2], dd[3]);
         }
         dout[c] = d;
     }
@@ -402,14 +439,14 @@ __global__ void k_sum_loss(int n, const double *__restrict__ part, int nn, doubl
     out[0] = s / (2.0 * nn);
 }
 
-// dh[c][k] = dout[c] . W4[:, k]
-__global__ void k_output_dh(int N, const float2 *__restrict__ dout, const __nv_bfloat16 *__restrict__ W4,
+// dh[c][k] = sum_j dout[c][j] W4[j][k]
+__global__ void k_output_dh(int N, const float4 *__restrict__ dout, const __nv_bfloat16 *__restrict__ W4,
                             float *__restrict__ dh) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)N * kH) return;
     const int c = (int)(i / kH), k = (int)(i % kH);
-    const float2 d = dout[c];
-    dh[i] = d.x * bf(W4[k]) + d.y * bf(W4[kH + k]);
+    const float4 d = dout[c];
+    dh[i] = d.x * bf(W4[k]) + d.y * bf(W4[kH + k]) + d.z * bf(W4[2 * kH + k]) + d.w * bf(W4[3 * kH + k]);
 }
 
 // -------------------------------------------------------------- adam ------
@@ -431,14 +468,14 @@ __global__ void k_to_bf16(int n, const float *__restrict__ w, __nv_bfloat16 *__r
     if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
-// proposal: the movable nodes at d256 + alpha (pred - d256), in core units
-__global__ void k_propose(int nn, const float2 *__restrict__ base, const float2 *__restrict__ pred, float alpha,
-                          float llx, float lly, float w, float h, float2 *__restrict__ xy) {
+// proposal: the movable nodes at q + alpha (f - q), in core units
+__global__ void k_propose(int nn, const float4 *__restrict__ pred, float alpha, float llx, float lly, float w,
+                          float h, float2 *__restrict__ xy) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nn) return;
-    const float2 b = base[c], p = pred[c];
-    const float x = fminf(fmaxf(b.x + alpha * (p.x - b.x), 0.f), 1.f);
-    const float y = fminf(fmaxf(b.y + alpha * (p.y - b.y), 0.f), 1.f);
+    const float4 p = pred[c];
+    const float x = fminf(fmaxf(p.x + alpha * (p.z - p.x), 0.f), 1.f);
+    const float y = fminf(fmaxf(p.y + alpha * (p.w - p.y), 0.f), 1.f);
     xy[c] = make_float2(llx + x * w, lly + y * h);
 }
 
@@ -447,16 +484,32 @@ __global__ void k_propose(int nn, const float2 *__restrict__ base, const float2 
 
 using namespace ep;
 
+// Workspace of the network, grown to the largest netlist bound so far, and
+// the netlist it currently holds features of.
 struct ep_gnn {
     int device = 0;
     std::string err;
     float *w = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *wb = nullptr;
     double *loss = nullptr;
-    float2 *xy = nullptr;
-    size_t xy_cap = 0;
     int64_t step = 0;
-    std::unordered_map<uint64_t, std::unique_ptr<Graph>> graphs;
+    // bound netlist
+    uint64_t uid = 0;         // 0: none
+    bool pads_ready = false;  // terminal pin lists uploaded (training)
+    Net net{};
+    EngineGraph eg{};
+    // capacities and buffers
+    size_t capN = 0, capNet = 0, capPad = 0, capT = 0;
+    float *X = nullptr, *inv_pins = nullptr, *inv_deg = nullptr;
+    float2 *v = nullptr, *netv = nullptr;
+    int *padcnt = nullptr;
+    int32_t *pad_start = nullptr, *pad_net = nullptr;
+    float *h[kLayers + 1] = {}, *m[kLayers + 1] = {};
+    float *a = nullptr, *dh = nullptr, *dx = nullptr, *dm = nullptr, *da = nullptr, *partial = nullptr;
+    float4 *raw = nullptr, *pred = nullptr, *dout = nullptr, *target = nullptr;
+    float2 *xy = nullptr;
+    double *loss_part = nullptr;
+    std::vector<void *> ws;  // workspace allocations (freed on growth)
     ep_gnn() { err.reserve(256); }
 };
 
@@ -475,11 +528,9 @@ size_t smem_dense(int K) { return sizeof(float) * ((size_t)K * kH + 64 * (size_t
 size_t smem_dx(int K) { return sizeof(float) * ((size_t)kH * K + 64 * (size_t)(kH + 1)); }
 
 void set_smem_attrs() {
-    static std::mutex mu;
     static std::vector<int> done;
     int dev = 0;
     cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lock(mu);
     if (std::find(done.begin(), done.end(), dev) != done.end()) return;
     done.push_back(dev);
     cudaFuncSetAttribute(k_dense<kF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dense(kF));
@@ -487,169 +538,223 @@ void set_smem_attrs() {
     cudaFuncSetAttribute(k_dense_dx<kH, kH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dx(2 * kH));
 }
 
-// The graph of an engine (built on first use, cached by the engine's id):
-// device pins in net order, each node's pins, the mean weights, the features.
-ep_status bind(ep_gnn *g, ep_engine *e, Graph *&out) {
+template <typename T>
+bool walloc(ep_gnn *g, T *&p, size_t n) {
+    if (cudaMalloc((void **)&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+        p = nullptr;
+        return false;
+    }
+    g->ws.push_back(p);
+    return true;
+}
+
+// Grow the workspace to hold N nodes, nnet nets and nt terminals.
+ep_status reserve(ep_gnn *g, size_t N, size_t nnet, size_t nt) {
+    if (N <= g->capN && nnet <= g->capNet && nt <= g->capT) return EP_OK;
+    cudaDeviceSynchronize();
+    for (void *p : g->ws) cudaFree(p);
+    g->ws.clear();
+    g->uid = 0;
+    g->pads_ready = false;
+    g->capPad = 0;
+    g->pad_net = nullptr;
+    N = std::max(N, g->capN);
+    nnet = std::max(nnet, g->capNet);
+    nt = std::max(nt, g->capT);
+    bool ok = walloc(g, g->X, N * kF) && walloc(g, g->inv_pins, N) && walloc(g, g->inv_deg, nnet) &&
+              walloc(g, g->v, N) && walloc(g, g->netv, nnet) && walloc(g, g->padcnt, nt) &&
+              walloc(g, g->pad_start, nt + 1) && walloc(g, g->a, nnet * kH) && walloc(g, g->dh, N * kH) &&
+              walloc(g, g->dx, N * kH) && walloc(g, g->dm, N * kH) && walloc(g, g->da, nnet * kH) &&
+              walloc(g, g->partial, (size_t)nblk((long long)N, kRowsPerBlock) * (kH * 2 * kH + kH)) &&
+              walloc(g, g->raw, N) && walloc(g, g->pred, N) && walloc(g, g->dout, N) && walloc(g, g->target, N) &&
+              walloc(g, g->xy, N) && walloc(g, g->loss_part, nblk((long long)N));
+    for (int l = 0; l <= kLayers && ok; l++) ok = walloc(g, g->h[l], N * kH) && walloc(g, g->m[l], N * kH);
+    if (!ok) {
+        g->capN = g->capNet = g->capT = 0;
+        g->err = "cudaMalloc failed for the network's workspace";
+        return EP_ERR_NOMEM;
+    }
+    g->capN = N;
+    g->capNet = nnet;
+    g->capT = nt;
+    return EP_OK;
+}
+
+// Bind an engine's netlist: its device arrays, the features (computed on the
+// engine's stream) -- skipped when the workspace already holds them.
+ep_status bind(ep_gnn *g, ep_engine *e) {
     EngineGraph eg{};
     if (engine_graph(e, &eg)) return EP_ERR_ARG;
-    auto it = g->graphs.find(eg.uid);
-    if (it != g->graphs.end()) {
-        out = it->second.get();
-        return EP_OK;
-    }
     if (eg.nn <= 0 || eg.nnet <= 0) {
         g->err = "the network needs movable nodes and nets";
         return EP_ERR_ARG;
     }
-    std::unique_ptr<Graph> G(new Graph());
-    G->uid = eg.uid;
-    G->nn = eg.nn;
-    G->nt = eg.nt;
-    G->N = eg.nn + eg.nt;
-    G->nnet = eg.nnet;
-    G->np = eg.np;
-    const int N = G->N, nn = eg.nn, np = eg.np, nnet = eg.nnet;
-    // graph node of each device pin; nodes' pins grouped (counting sort)
-    std::vector<int32_t> pin_node(np), start(N + 1, 0), pin_net_of_node(np);
-    for (int p = 0; p < np; p++) {
-        const int o = eg.pin_owner[p];
-        pin_node[p] = o < eg.nn ? o : (o >= eg.n_obj ? nn + (o - eg.n_obj) : -1);
-        if (pin_node[p] < 0) {
-            g->err = "a pin on a filler";
-            return EP_ERR_STATE;
-        }
-        start[pin_node[p] + 1]++;
+    if (eg.device != g->device) {
+        g->err = "the engine lives on another device than the network";
+        return EP_ERR_ARG;
     }
-    for (int c = 0; c < N; c++) start[c + 1] += start[c];
-    {
-        std::vector<int32_t> fill(start.begin(), start.end() - 1);
-        for (int p = 0; p < np; p++) pin_net_of_node[fill[pin_node[p]]++] = eg.pin_net[p];
+    if (g->uid == eg.uid) {
+        g->eg = eg;
+        return EP_OK;
     }
-    std::vector<float> inv_deg(nnet), inv_pins(N, 0.f), X((size_t)N * kF, 0.f);
-    for (int n = 0; n < nnet; n++) inv_deg[n] = eg.net_deg[n] > 0 ? 1.f / eg.net_deg[n] : 0.f;
-    for (int c = 0; c < N; c++) {
-        const int k = start[c + 1] - start[c];
-        inv_pins[c] = k > 0 ? 1.f / k : 0.f;
-    }
-    const Grid &gr = eg.grid;
-    const float W = gr.urx - gr.llx, H = gr.ury - gr.lly;
-    std::vector<float2> v0(N);
-    for (int c = 0; c < N; c++) {
-        const int pins = start[c + 1] - start[c];
-        X[(size_t)c * kF + 1] = std::log1p((float)pins) / 3.f;
-        if (c < nn) {
-            X[(size_t)c * kF + 0] = std::log1p(eg.node_area[c]) / 4.f;
-            v0[c] = make_float2(0.5f, 0.5f);
-        } else {
-            const float2 t = eg.term_centre[c - nn];
-            X[(size_t)c * kF + 2] = 1.f;
-            v0[c] = make_float2((t.x - gr.llx) / W, (t.y - gr.lly) / H);
-        }
-    }
-    if (!G->alloc(G->net_first, nnet) || !G->alloc(G->net_deg, nnet) || !G->alloc(G->pin_node, np) ||
-        !G->alloc(G->node_pin_start, N + 1) || !G->alloc(G->node_pin_net, np) || !G->alloc(G->inv_deg, nnet) ||
-        !G->alloc(G->inv_pins, N) || !G->alloc(G->X, (size_t)N * kF) || !G->alloc(G->d256, N) ||
-        !G->alloc(G->a, (size_t)nnet * kH) || !G->alloc(G->raw, N) || !G->alloc(G->pred, N) ||
-        !G->alloc(G->dout, N) || !G->alloc(G->target, N) || !G->alloc(G->dh, (size_t)N * kH) ||
-        !G->alloc(G->dx, (size_t)N * kH) || !G->alloc(G->dm, (size_t)N * kH) || !G->alloc(G->da, (size_t)nnet * kH) ||
-        !G->alloc(G->loss_part, nblk(N)))
-        return EP_ERR_NOMEM;
-    for (int l = 0; l <= kLayers; l++)
-        if (!G->alloc(G->h[l], (size_t)N * kH) || !G->alloc(G->m[l], (size_t)N * kH)) return EP_ERR_NOMEM;
-    G->partial_floats = (size_t)nblk(N, kRowsPerBlock) * (kH * 2 * kH + kH);
-    if (!G->alloc(G->partial, G->partial_floats)) return EP_ERR_NOMEM;
+    set_smem_attrs();
+    const int N = eg.nn + eg.nt;
+    ep_status s = reserve(g, N, eg.nnet, eg.nt);
+    if (s) return s;
+    g->eg = eg;
+    g->pads_ready = false;
+    Net &n = g->net;
+    n.nn = eg.nn;
+    n.n_obj = eg.n_obj;
+    n.N = N;
+    n.nnet = eg.nnet;
+    n.owner = eg.d_pin_owner;
+    n.net_first = eg.d_net_first;
+    n.net_deg = eg.d_net_deg;
+    n.pin_net = eg.d_pin_net;
+    n.obj_pin_start = eg.d_obj_pin_start;
+    n.obj_pin_dev = eg.d_obj_pin_dev;
+    n.pad_start = g->pad_start;
+    n.pad_net = g->pad_net;
     cudaStream_t st = eg.st;
-    GK(cudaMemcpyAsync(G->net_first, eg.net_first, sizeof(int32_t) * nnet, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->net_deg, eg.net_deg, sizeof(int32_t) * nnet, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->pin_node, pin_node.data(), sizeof(int32_t) * np, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->node_pin_start, start.data(), sizeof(int32_t) * (N + 1), cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->node_pin_net, pin_net_of_node.data(), sizeof(int32_t) * np, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->inv_deg, inv_deg.data(), sizeof(float) * nnet, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->inv_pins, inv_pins.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->X, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice, st));
-    GK(cudaMemcpyAsync(G->d256, v0.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
-    // pad-anchored diffusion: the movable nodes' coordinates after 16, 64 and
-    // 256 steps into feature columns 3-8 (terminals keep their centres);
-    // G->a serves as the per-net buffer
-    float2 *netv = (float2 *)G->a;
+    if (eg.fp64)
+        k_init<double><<<nblk(N), kT, 0, st>>>(n, eg.d_area, eg.d_npins, (const double2 *)eg.d_pos, eg.grid, g->X,
+                                                g->v, g->inv_pins);
+    else
+        k_init<float><<<nblk(N), kT, 0, st>>>(n, eg.d_area, eg.d_npins, (const float2 *)eg.d_pos, eg.grid, g->X,
+                                               g->v, g->inv_pins);
+    if (eg.nt > 0) {
+        GK(cudaMemsetAsync(g->padcnt, 0, sizeof(int) * eg.nt, st));
+        k_pad_pins<<<nblk(eg.np), kT, 0, st>>>(eg.np, n, g->padcnt);
+        k_pad_feature<<<nblk(eg.nt), kT, 0, st>>>(eg.nt, eg.nn, g->padcnt, g->X);
+    }
+    k_inv_deg<<<nblk(eg.nnet), kT, 0, st>>>(eg.nnet, eg.d_net_deg, g->inv_deg);
     int col = 3;
     for (int k = 1; k <= kDiffSteps[2]; k++) {
-        k_diff_net<<<nblk(nnet), kT, 0, st>>>(nnet, G->net_first, G->net_deg, G->pin_node, G->inv_deg, G->d256, netv);
-        k_diff_node<<<nblk(nn), kT, 0, st>>>(nn, G->node_pin_start, G->node_pin_net, G->inv_pins, netv, G->d256);
+        k_diff_net<<<nblk(eg.nnet), kT, 0, st>>>(n, g->inv_deg, g->v, g->netv);
+        k_diff_node<<<nblk(eg.nn), kT, 0, st>>>(n, g->inv_pins, g->netv, g->v);
         if (k == kDiffSteps[0] || k == kDiffSteps[1] || k == kDiffSteps[2]) {
-            k_store_feature<<<nblk(N), kT, 0, st>>>(N, G->d256, G->X, col);
+            k_store_feature<<<nblk(N), kT, 0, st>>>(N, g->v, g->X, col);
             col += 2;
         }
     }
     GK(cudaGetLastError());
-    GK(cudaStreamSynchronize(st));  // the host vectors go out of scope
-    out = G.get();
-    g->graphs[eg.uid] = std::move(G);
+    g->uid = eg.uid;
     return EP_OK;
 }
 
-// Forward pass on a bound graph (activations kept for the backward pass).
-ep_status forward(ep_gnn *g, Graph &G, cudaStream_t st) {
-    const int N = G.N, nn = G.nn, nnet = G.nnet;
+// The terminals' pin lists (the transposed aggregation into terminals needs
+// them; training only), built on the host from the engine's pin owners.
+ep_status bind_pads(ep_gnn *g) {
+    if (g->pads_ready) return EP_OK;
+    const EngineGraph &eg = g->eg;
+    std::vector<int32_t> start(eg.nt + 1, 0), nets;
+    for (int p = 0; p < eg.np; p++)
+        if (eg.pin_owner[p] >= eg.n_obj) start[eg.pin_owner[p] - eg.n_obj + 1]++;
+    for (int t = 0; t < eg.nt; t++) start[t + 1] += start[t];
+    nets.resize(std::max(start[eg.nt], 1));
+    {
+        std::vector<int32_t> fill(start.begin(), start.end() - 1);
+        for (int p = 0; p < eg.np; p++)
+            if (eg.pin_owner[p] >= eg.n_obj) nets[fill[eg.pin_owner[p] - eg.n_obj]++] = eg.pin_net[p];
+    }
+    if (nets.size() > g->capPad) {
+        if (g->pad_net) {
+            cudaStreamSynchronize(eg.st);
+            cudaFree(g->pad_net);
+            g->ws.erase(std::find(g->ws.begin(), g->ws.end(), (void *)g->pad_net));
+            g->pad_net = nullptr;
+        }
+        if (!walloc(g, g->pad_net, nets.size())) {
+            g->capPad = 0;
+            g->err = "cudaMalloc failed for the terminals' pin lists";
+            return EP_ERR_NOMEM;
+        }
+        g->capPad = nets.size();
+    }
+    GK(cudaMemcpyAsync(g->pad_start, start.data(), sizeof(int32_t) * start.size(), cudaMemcpyHostToDevice, eg.st));
+    GK(cudaMemcpyAsync(g->pad_net, nets.data(), sizeof(int32_t) * nets.size(), cudaMemcpyHostToDevice, eg.st));
+    GK(cudaStreamSynchronize(eg.st));  // the host vectors go out of scope
+    g->net.pad_start = g->pad_start;
+    g->net.pad_net = g->pad_net;
+    g->pads_ready = true;
+    return EP_OK;
+}
+
+// Forward pass on the bound netlist (activations kept for the backward pass).
+ep_status forward(ep_gnn *g) {
+    const Net &n = g->net;
+    const int N = n.N;
+    cudaStream_t st = g->eg.st;
     const float *w = g->w;
     const __nv_bfloat16 *wb = g->wb;
-    k_dense<kF, 0><<<nblk(N, 64), kT, smem_dense(kF), st>>>(N, G.X, nullptr, wb + kOffW0, w + kOffB0, G.h[0]);
+    k_dense<kF, 0><<<nblk(N, 64), kT, smem_dense(kF), st>>>(N, g->X, nullptr, wb + kOffW0, w + kOffB0, g->h[0]);
     for (int l = 1; l <= kLayers; l++) {
-        k_net_mean<<<nblk((long long)nnet * 32), kT, 0, st>>>(nnet, G.net_first, G.net_deg, G.pin_node, G.inv_deg,
-                                                              (const float2 *)G.h[l - 1], (float2 *)G.a);
-        k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(N, nn, G.node_pin_start, G.node_pin_net, G.inv_pins,
-                                                            (const float2 *)G.a, (float2 *)G.m[l]);
-        k_dense<kH, kH><<<nblk(N, 64), kT, smem_dense(2 * kH), st>>>(N, G.h[l - 1], G.m[l], wb + off_w(l),
-                                                                     w + off_b(l), G.h[l]);
+        k_net_mean<<<nblk((long long)n.nnet * 32), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
+                                                                (float2 *)g->a);
+        k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
+        k_dense<kH, kH><<<nblk(N, 64), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], wb + off_w(l),
+                                                                     w + off_b(l), g->h[l]);
     }
-    k_output<<<nblk(N), kT, 0, st>>>(N, G.h[kLayers], wb + kOffW4, w + kOffB4, G.d256, G.raw, G.pred);
+    k_output<<<nblk(N), kT, 0, st>>>(N, g->h[kLayers], wb + kOffW4, w + kOffB4, g->v, g->raw, g->pred);
     GK(cudaGetLastError());
     return EP_OK;
 }
 
-// Loss against G.target and the gradient of every parameter into g->grad.
-ep_status backward(ep_gnn *g, Graph &G, cudaStream_t st) {
-    const int N = G.N, nn = G.nn, nnet = G.nnet;
+// Loss against g->target and the gradient of every parameter into g->grad.
+ep_status backward(ep_gnn *g) {
+    const Net &n = g->net;
+    const int N = n.N;
+    cudaStream_t st = g->eg.st;
     const __nv_bfloat16 *wb = g->wb;
     const int lb = nblk(N);
-    k_loss<<<lb, kT, 0, st>>>(N, nn, G.raw, G.pred, G.target, G.dout, G.loss_part);
-    k_sum_loss<<<1, 32, 0, st>>>(lb, G.loss_part, nn, g->loss);
+    k_loss<<<lb, kT, 0, st>>>(N, n.nn, g->raw, g->pred, g->target, g->dout, g->loss_part);
+    k_sum_loss<<<1, 32, 0, st>>>(lb, g->loss_part, n.nn, g->loss);
     const int pb = nblk(N, kRowsPerBlock);
     // output layer
-    k_dweight<2, kH, 0><<<pb, kT, 0, st>>>(N, kRowsPerBlock, (const float *)G.dout, nullptr, G.h[kLayers], nullptr,
-                                          G.partial);
-    k_reduce_partials<<<nblk(2 * kH + 2), kT, 0, st>>>(pb, 2 * kH, 2, G.partial, g->grad, kOffW4, kOffB4);
-    k_output_dh<<<nblk((long long)N * kH), kT, 0, st>>>(N, G.dout, wb + kOffW4, G.dh);
-    // message-passing layers, last to first; G.dh holds d loss / d h_l
+    k_dweight<kOut, kH, 0><<<pb, kT, 0, st>>>(N, kRowsPerBlock, (const float *)g->dout, nullptr, g->h[kLayers],
+                                             nullptr, g->partial);
+    k_reduce_partials<<<nblk(kOut * kH + kOut), kT, 0, st>>>(pb, kOut * kH, kOut, g->partial, g->grad, kOffW4,
+                                                             kOffB4);
+    k_output_dh<<<nblk((long long)N * kH), kT, 0, st>>>(N, g->dout, wb + kOffW4, g->dh);
+    // message-passing layers, last to first; dh holds d loss / d h_l
+    float *dh = g->dh, *dx = g->dx;
     for (int l = kLayers; l >= 1; l--) {
-        k_dweight<kH, kH, kH><<<pb, kT, 0, st>>>(N, kRowsPerBlock, G.dh, G.h[l], G.h[l - 1], G.m[l], G.partial);
-        k_reduce_partials<<<nblk(kH * 2 * kH + kH), kT, 0, st>>>(pb, kH * 2 * kH, kH, G.partial, g->grad, off_w(l),
+        k_dweight<kH, kH, kH><<<pb, kT, 0, st>>>(N, kRowsPerBlock, dh, g->h[l], g->h[l - 1], g->m[l], g->partial);
+        k_reduce_partials<<<nblk(kH * 2 * kH + kH), kT, 0, st>>>(pb, kH * 2 * kH, kH, g->partial, g->grad, off_w(l),
                                                                  off_b(l));
-        // d h_{l-1} (direct part) into G.dx, d m_l into G.dm
-        k_dense_dx<kH, kH><<<nblk(N, 64), kT, smem_dx(2 * kH), st>>>(N, G.dh, G.h[l], wb + off_w(l), G.dx, G.dm);
-        k_node_mean_t<<<nblk((long long)nnet * 32), kT, 0, st>>>(nnet, nn, G.net_first, G.net_deg, G.pin_node,
-                                                                 G.inv_pins, (const float2 *)G.dm, (float2 *)G.da);
-        k_net_mean_t_add<<<nblk((long long)N * 32), kT, 0, st>>>(N, G.node_pin_start, G.node_pin_net, G.inv_deg,
-                                                                 (const float2 *)G.da, (float2 *)G.dx);
-        std::swap(G.dh, G.dx);
+        // d h_{l-1} (direct part) into dx, d m_l into g->dm
+        k_dense_dx<kH, kH><<<nblk(N, 64), kT, smem_dx(2 * kH), st>>>(N, dh, g->h[l], wb + off_w(l), dx, g->dm);
+        k_node_mean_t<<<nblk((long long)n.nnet * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->dm,
+                                                                   (float2 *)g->da);
+        k_net_mean_t_add<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->da,
+                                                                 (float2 *)dx);
+        std::swap(dh, dx);
     }
     // input layer
-    k_dweight<kH, kF, 0><<<pb, kT, 0, st>>>(N, kRowsPerBlock, G.dh, G.h[0], G.X, nullptr, G.partial);
-    k_reduce_partials<<<nblk(kH * kF + kH), kT, 0, st>>>(pb, kH * kF, kH, G.partial, g->grad, kOffW0, kOffB0);
+    k_dweight<kH, kF, 0><<<pb, kT, 0, st>>>(N, kRowsPerBlock, dh, g->h[0], g->X, nullptr, g->partial);
+    k_reduce_partials<<<nblk(kH * kF + kH), kT, 0, st>>>(pb, kH * kF, kH, g->partial, g->grad, kOffW0, kOffB0);
     GK(cudaGetLastError());
     return EP_OK;
 }
 
-ep_status upload_target(ep_gnn *g, Graph &G, const float *target_xy, const EngineGraph &eg, cudaStream_t st) {
-    // the movable nodes' targets (core coordinates) normalised to the core
-    const Grid &gr = eg.grid;
+// Targets of the movable nodes: [nn][4] core coordinates (quadratic
+// placement x, y, final x, y), normalised to the core.
+ep_status upload_target(ep_gnn *g, const float *t4) {
+    const Grid &gr = g->eg.grid;
     const float W = gr.urx - gr.llx, H = gr.ury - gr.lly;
-    std::vector<float2> t(G.N, make_float2(0.f, 0.f));
-    for (int c = 0; c < G.nn; c++)
-        t[c] = make_float2((target_xy[2 * c] - gr.llx) / W, (target_xy[2 * c + 1] - gr.lly) / H);
-    GK(cudaMemcpyAsync(G.target, t.data(), sizeof(float2) * G.N, cudaMemcpyHostToDevice, st));
-    GK(cudaStreamSynchronize(st));
+    std::vector<float4> t(g->net.N, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int c = 0; c < g->net.nn; c++)
+        t[c] = make_float4((t4[4 * c] - gr.llx) / W, (t4[4 * c + 1] - gr.lly) / H, (t4[4 * c + 2] - gr.llx) / W,
+                           (t4[4 * c + 3] - gr.lly) / H);
+    GK(cudaMemcpyAsync(g->target, t.data(), sizeof(float4) * t.size(), cudaMemcpyHostToDevice, g->eg.st));
+    GK(cudaStreamSynchronize(g->eg.st));
     return EP_OK;
+}
+
+ep_status oom(ep_gnn *g) {
+    g->err.assign("out of host memory");
+    return EP_ERR_NOMEM;
 }
 
 }  // namespace
@@ -660,15 +765,10 @@ int32_t ep_gnn_num_weights(void) { return kParams; }
 
 const char *ep_gnn_last_error(const ep_gnn *g) { return g ? g->err.c_str() : "null network"; }
 
-ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) {
+ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) try {
     if (!out) return EP_ERR_ARG;
     *out = nullptr;
-    ep_gnn *g = nullptr;
-    try {
-        g = new ep_gnn();
-    } catch (const std::bad_alloc &) {
-        return EP_ERR_NOMEM;
-    }
+    ep_gnn *g = new ep_gnn();
     *out = g;
     g->device = device;
     GK(cudaSetDevice(device));
@@ -682,7 +782,7 @@ ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) {
         return EP_ERR_NOMEM;
     }
     // Glorot-uniform weights, zero biases; the output layer starts small so
-    // the first proposals stay near the diffusion coordinates
+    // the first predictions stay near the diffusion coordinates
     std::vector<float> w(kParams, 0.f);
     std::mt19937_64 rng(seed);
     auto fill = [&](int off, int rows, int cols, float gain) {
@@ -692,15 +792,18 @@ ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) {
     };
     fill(kOffW0, kH, kF, 1.f);
     for (int l = 1; l <= kLayers; l++) fill(off_w(l), kH, 2 * kH, 1.f);
-    fill(kOffW4, 2, kH, 0.1f);
+    fill(kOffW4, kOut, kH, 0.1f);
     return ep_gnn_set_weights(g, w.data());
+} catch (const std::bad_alloc &) {
+    return EP_ERR_NOMEM;
 }
 
 void ep_gnn_destroy(ep_gnn *g) {
     if (!g) return;
-    g->graphs.clear();
+    cudaDeviceSynchronize();
+    for (void *p : g->ws) cudaFree(p);
     for (void *p : {(void *)g->w, (void *)g->grad, (void *)g->adam_m, (void *)g->adam_v, (void *)g->wb,
-                    (void *)g->loss, (void *)g->xy})
+                    (void *)g->loss})
         if (p) cudaFree(p);
     delete g;
 }
@@ -727,117 +830,82 @@ ep_status ep_gnn_release(ep_gnn *g, ep_engine *e) {
     if (!g || !e) return EP_ERR_ARG;
     EngineGraph eg{};
     if (engine_graph(e, &eg)) return EP_ERR_ARG;
-    g->graphs.erase(eg.uid);
+    if (g->uid == eg.uid) g->uid = 0;
     return EP_OK;
 }
 
-ep_status ep_gnn_features(ep_gnn *g, ep_engine *e, float *X) try {
+ep_status ep_gnn_features(ep_gnn *g, ep_engine *e, float *X) {
     if (!g || !e || !X) return EP_ERR_ARG;
-    set_smem_attrs();
-    Graph *G = nullptr;
-    ep_status s = bind(g, e, G);
+    ep_status s = bind(g, e);
     if (s) return s;
-    GK(cudaMemcpy(X, G->X, sizeof(float) * (size_t)G->N * kF, cudaMemcpyDeviceToHost));
+    GK(cudaMemcpyAsync(X, g->X, sizeof(float) * (size_t)g->net.N * kF, cudaMemcpyDeviceToHost, g->eg.st));
+    GK(cudaStreamSynchronize(g->eg.st));
     return EP_OK;
-} catch (const std::bad_alloc &) {
-    g->err.assign("out of host memory");
-    return EP_ERR_NOMEM;
 }
 
-ep_status ep_gnn_forward(ep_gnn *g, ep_engine *e, float *pred_xy) try {
-    if (!g || !e || !pred_xy) return EP_ERR_ARG;
-    set_smem_attrs();
-    Graph *G = nullptr;
-    ep_status s = bind(g, e, G);
-    if (s) return s;
-    EngineGraph eg{};
-    engine_graph(e, &eg);
-    if ((s = forward(g, *G, eg.st))) return s;
-    std::vector<float2> p(G->nn);
-    GK(cudaMemcpyAsync(p.data(), G->pred, sizeof(float2) * G->nn, cudaMemcpyDeviceToHost, eg.st));
-    GK(cudaStreamSynchronize(eg.st));
-    const Grid &gr = eg.grid;
-    for (int c = 0; c < G->nn; c++) {
-        pred_xy[2 * c] = gr.llx + p[c].x * (gr.urx - gr.llx);
-        pred_xy[2 * c + 1] = gr.lly + p[c].y * (gr.ury - gr.lly);
+ep_status ep_gnn_forward(ep_gnn *g, ep_engine *e, float *xy4) try {
+    if (!g || !e || !xy4) return EP_ERR_ARG;
+    ep_status s = bind(g, e);
+    if (s || (s = forward(g))) return s;
+    const int nn = g->net.nn;
+    std::vector<float4> p(nn);
+    GK(cudaMemcpyAsync(p.data(), g->pred, sizeof(float4) * nn, cudaMemcpyDeviceToHost, g->eg.st));
+    GK(cudaStreamSynchronize(g->eg.st));
+    const Grid &gr = g->eg.grid;
+    const float W = gr.urx - gr.llx, H = gr.ury - gr.lly;
+    for (int c = 0; c < nn; c++) {
+        xy4[4 * c] = gr.llx + p[c].x * W;
+        xy4[4 * c + 1] = gr.lly + p[c].y * H;
+        xy4[4 * c + 2] = gr.llx + p[c].z * W;
+        xy4[4 * c + 3] = gr.lly + p[c].w * H;
     }
     return EP_OK;
 } catch (const std::bad_alloc &) {
-    g->err.assign("out of host memory");
-    return EP_ERR_NOMEM;
+    return oom(g);
 }
 
-ep_status ep_gnn_loss_grad(ep_gnn *g, ep_engine *e, const float *target_xy, double *loss, float *grad) try {
-    if (!g || !e || !target_xy) return EP_ERR_ARG;
-    set_smem_attrs();
-    Graph *G = nullptr;
-    ep_status s = bind(g, e, G);
-    if (s) return s;
-    EngineGraph eg{};
-    engine_graph(e, &eg);
-    if ((s = upload_target(g, *G, target_xy, eg, eg.st)) || (s = forward(g, *G, eg.st)) ||
-        (s = backward(g, *G, eg.st)))
+ep_status ep_gnn_loss_grad(ep_gnn *g, ep_engine *e, const float *target4, double *loss, float *grad) try {
+    if (!g || !e || !target4) return EP_ERR_ARG;
+    ep_status s = bind(g, e);
+    if (s || (s = bind_pads(g)) || (s = upload_target(g, target4)) || (s = forward(g)) || (s = backward(g)))
         return s;
-    if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, eg.st));
-    if (grad) GK(cudaMemcpyAsync(grad, g->grad, sizeof(float) * kParams, cudaMemcpyDeviceToHost, eg.st));
-    GK(cudaStreamSynchronize(eg.st));
+    if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, g->eg.st));
+    if (grad) GK(cudaMemcpyAsync(grad, g->grad, sizeof(float) * kParams, cudaMemcpyDeviceToHost, g->eg.st));
+    GK(cudaStreamSynchronize(g->eg.st));
     return EP_OK;
 } catch (const std::bad_alloc &) {
-    g->err.assign("out of host memory");
-    return EP_ERR_NOMEM;
+    return oom(g);
 }
 
-ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target_xy, float lr, double *loss) try {
-    if (!g || !e || !target_xy || !(lr > 0)) return EP_ERR_ARG;
-    set_smem_attrs();
-    Graph *G = nullptr;
-    ep_status s = bind(g, e, G);
-    if (s) return s;
-    EngineGraph eg{};
-    engine_graph(e, &eg);
-    if ((s = upload_target(g, *G, target_xy, eg, eg.st)) || (s = forward(g, *G, eg.st)) ||
-        (s = backward(g, *G, eg.st)))
+ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target4, float lr, double *loss) try {
+    if (!g || !e || !target4 || !(lr > 0)) return EP_ERR_ARG;
+    ep_status s = bind(g, e);
+    if (s || (s = bind_pads(g)) || (s = upload_target(g, target4)) || (s = forward(g)) || (s = backward(g)))
         return s;
     g->step++;
     const float c1 = 1.f / (1.f - std::pow(0.9f, (float)g->step)), c2 = 1.f / (1.f - std::pow(0.999f, (float)g->step));
-    k_adam<<<nblk(kParams), kT, 0, eg.st>>>(kParams, g->w, g->grad, g->adam_m, g->adam_v, lr, c1, c2, g->wb);
+    k_adam<<<nblk(kParams), kT, 0, g->eg.st>>>(kParams, g->w, g->grad, g->adam_m, g->adam_v, lr, c1, c2, g->wb);
     GK(cudaGetLastError());
-    if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, eg.st));
-    GK(cudaStreamSynchronize(eg.st));
+    if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, g->eg.st));
+    GK(cudaStreamSynchronize(g->eg.st));
     return EP_OK;
 } catch (const std::bad_alloc &) {
-    g->err.assign("out of host memory");
-    return EP_ERR_NOMEM;
+    return oom(g);
 }
 
-ep_status ep_gnn_propose(ep_gnn *g, ep_engine *e, float alpha) try {
+ep_status ep_gnn_propose(ep_gnn *g, ep_engine *e, float alpha) {
     if (!g || !e || !(alpha >= 0.f) || alpha > 1.f) return EP_ERR_ARG;
-    set_smem_attrs();
-    Graph *G = nullptr;
-    ep_status s = bind(g, e, G);
-    if (s) return s;
-    EngineGraph eg{};
-    engine_graph(e, &eg);
-    if ((s = forward(g, *G, eg.st))) return s;
-    if (g->xy_cap < (size_t)G->nn) {
-        if (g->xy) cudaFree(g->xy);
-        g->xy = nullptr;
-        GK(cudaMalloc(&g->xy, sizeof(float2) * std::max(G->nn, 1)));
-        g->xy_cap = G->nn;
-    }
-    const Grid &gr = eg.grid;
-    k_propose<<<nblk(G->nn), kT, 0, eg.st>>>(G->nn, G->d256, G->pred, alpha, gr.llx, gr.lly, gr.urx - gr.llx,
-                                              gr.ury - gr.lly, g->xy);
+    ep_status s = bind(g, e);
+    if (s || (s = forward(g))) return s;
+    const Grid &gr = g->eg.grid;
+    k_propose<<<nblk(g->net.nn), kT, 0, g->eg.st>>>(g->net.nn, g->pred, alpha, gr.llx, gr.lly, gr.urx - gr.llx,
+                                                    gr.ury - gr.lly, g->xy);
     GK(cudaGetLastError());
     if (engine_set_node_centres(e, g->xy)) {
         g->err = "setting the proposed positions failed";
         return EP_ERR_CUDA;
     }
-    GK(cudaStreamSynchronize(eg.st));
     return EP_OK;
-} catch (const std::bad_alloc &) {
-    g->err.assign("out of host memory");
-    return EP_ERR_NOMEM;
 }
 
 }  // extern "C"

@@ -708,19 +708,25 @@ class Gnn:
         return x
 
     def forward(self, engine):
-        xy = np.zeros((engine.info.num_nodes, 2), np.float32)
+        """[num_nodes, 4]: the predicted quadratic-placement centre (x, y)
+        and final centre (x, y) of each movable node."""
+        xy = np.zeros((engine.info.num_nodes, 4), np.float32)
         self._check(self._L.ep_gnn_forward(self.h, engine.h, _p(xy, _f32p)))
         return xy
 
-    def loss_grad(self, engine, target_xy):
-        t = np.ascontiguousarray(target_xy, np.float32)
+    def loss_grad(self, engine, target4):
+        t = np.ascontiguousarray(target4, np.float32)
+        if t.shape != (engine.info.num_nodes, 4):
+            raise ValueError("targets: [num_nodes, 4] (QP x, y, final x, y)")
         loss = ctypes.c_double()
         g = np.zeros(self.num_weights, np.float32)
         self._check(self._L.ep_gnn_loss_grad(self.h, engine.h, _p(t, _f32p), ctypes.byref(loss), _p(g, _f32p)))
         return loss.value, g
 
-    def train_step(self, engine, target_xy, lr):
-        t = np.ascontiguousarray(target_xy, np.float32)
+    def train_step(self, engine, target4, lr):
+        t = np.ascontiguousarray(target4, np.float32)
+        if t.shape != (engine.info.num_nodes, 4):
+            raise ValueError("targets: [num_nodes, 4] (QP x, y, final x, y)")
         loss = ctypes.c_double()
         self._check(self._L.ep_gnn_train_step(self.h, engine.h, _p(t, _f32p), float(lr), ctypes.byref(loss)))
         return loss.value

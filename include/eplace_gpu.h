@@ -392,19 +392,21 @@ ep_status ep_density_scatter_noalloc(const ep_scatter_grid *grid, int32_t num_ob
  * caller keeps a proposal when its mGP run reaches the same overflow at an
  * HPWL within its tolerance of the QP-started run).
  *
- * Graph: an engine's movable nodes and terminals joined by its nets; mean
- * aggregations node -> net -> node.  Input features per node: log(1 + area)/4,
- * log(1 + pins)/3, terminal flag, and its core-normalised coordinates after
- * 16, 64 and 256 steps of pad-anchored diffusion (movable nodes start at the
- * core centre, terminals stay at their centres, a step is node <- mean of
- * its nets <- mean of their pins).  Network: h0 = relu(W0 x + b0); three
- * layers h = relu(W [h ; mean of the nets' mean of h] + b), hidden 64;
- * prediction = 256-step coordinates + 0.25 tanh(W4 h + b4).  Weights are
- * FP32 masters with BF16 copies used by the forward pass (FP32 accumulate);
- * training minimises the mean squared error to a target placement
+ * Graph: an engine's movable nodes and terminals joined by its nets (read
+ * from the engine's device arrays); mean aggregations node -> net -> node.
+ * Input features per node: log(1 + area)/4, log(1 + pins)/3, terminal flag,
+ * and its core-normalised coordinates after 32, 128 and 512 steps of
+ * pad-anchored diffusion (movable nodes start at the core centre, terminals
+ * stay at their centres, a step is node <- mean of its nets <- mean of their
+ * pins).  Network: h0 = relu(W0 x + b0); three layers h = relu(W [h ; mean
+ * of the nets' mean of h] + b), hidden 64; two heads q, f = d + 0.25
+ * tanh(W4 h + b4), d the 512-step coordinates: q predicts the engine's
+ * quadratic placement of the design, f its final mGP placement.  Weights
+ * are FP32 masters with BF16 copies used by the forward pass (FP32
+ * accumulate); training minimises the mean squared error of both heads
  * (normalised to the core) with Adam.  All work runs on the engine's
- * stream; the network caches each engine's graph until ep_gnn_release or
- * ep_gnn_destroy. */
+ * stream, in a workspace the network keeps (grown to the largest netlist;
+ * the features of the last engine used are kept until ep_gnn_release). */
 typedef struct ep_gnn ep_gnn;
 int32_t ep_gnn_num_weights(void);
 ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out);
@@ -416,16 +418,19 @@ ep_status ep_gnn_set_weights(ep_gnn *g, const float *w);
 ep_status ep_gnn_release(ep_gnn *g, ep_engine *e);
 /* Input features, [num_nodes + num_terminals][9] floats. */
 ep_status ep_gnn_features(ep_gnn *g, ep_engine *e, float *x);
-/* Predicted centres of the movable nodes (core coordinates), [num_nodes][2]. */
-ep_status ep_gnn_forward(ep_gnn *g, ep_engine *e, float *xy);
-/* Loss against target centres ([num_nodes][2], core coordinates) and its
- * gradient with respect to every weight (may be NULL). */
-ep_status ep_gnn_loss_grad(ep_gnn *g, ep_engine *e, const float *target_xy, double *loss, float *grad);
+/* Predictions for the movable nodes (core coordinates), [num_nodes][4]:
+ * q.x, q.y, f.x, f.y. */
+ep_status ep_gnn_forward(ep_gnn *g, ep_engine *e, float *xy4);
+/* Loss against targets [num_nodes][4] (core coordinates: the quadratic
+ * placement's centre, then the final centre, of each movable node), the sum
+ * of both heads' squared errors over 2 num_nodes, and its gradient with
+ * respect to every weight (may be NULL). */
+ep_status ep_gnn_loss_grad(ep_gnn *g, ep_engine *e, const float *target4, double *loss, float *grad);
 /* One Adam step (learning rate lr) on that loss; *loss (may be NULL) is the
  * loss before the step. */
-ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target_xy, float lr, double *loss);
-/* Move the engine's movable nodes to d + alpha (prediction - d), d the
- * 256-step coordinates, alpha in [0, 1], clamped into the core; fillers stay.
+ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target4, float lr, double *loss);
+/* Move the engine's movable nodes to q + alpha (f - q), alpha in [0, 1],
+ * clamped into the core; fillers stay.  Enqueued on the engine's stream;
  * ep_initialize must run again afterwards. */
 ep_status ep_gnn_propose(ep_gnn *g, ep_engine *e, float alpha);
 

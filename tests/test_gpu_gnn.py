@@ -4,14 +4,15 @@ the network -- test-side only).
 
 Tolerances:
   * diffusion features: 1e-5 absolute (core-normalised coordinates) against
-    the same 16/64/256 mean-aggregation steps in float64;
-  * forward prediction and loss: 1e-5 relative; every weight gradient: 1e-4
-    of the largest gradient entry, against autograd on the BF16-rounded
-    weights (the forward pass uses BF16 weights, FP32 accumulation);
+    the same 32/128/512 mean-aggregation steps in float64;
+  * both heads' predictions and the loss: 1e-5 relative; every weight
+    gradient: 1e-4 of the largest gradient entry, against autograd on the
+    BF16-rounded weights (the forward pass uses BF16 weights, FP32
+    accumulation);
   * a training step is bitwise repeatable, and 60 Adam steps on one design
     lower its loss by at least a fifth;
-  * a proposal with alpha = 0 puts the movable nodes at the 256-step
-    diffusion coordinates (to float rounding of the core mapping).
+  * a proposal puts the movable nodes at q + alpha (f - q) of the forward
+    pass (to float rounding of the core mapping, and the core clamp).
 """
 import numpy as np
 import pytest
@@ -52,10 +53,10 @@ def features_ref(nl):
     v = np.concatenate([np.full((nn, 2), 0.5), np.stack([tcx, tcy], 1)]).astype(np.float64)
     has = pins[:nn] > 0
     cols = []
-    for k in range(1, 257):
+    for k in range(1, 513):
         new = node_mean @ (net_mean @ v)
         v[:nn][has] = new[:nn][has]
-        if k in (16, 64, 256):
+        if k in (32, 128, 512):
             cols.append(v.copy())
     return cols
 
@@ -99,14 +100,15 @@ def torch_loss(x, w, nl, target, nn):
     for l in (1, 2, 3):
         take(f"W{l}", H, 2 * H, True)
         take(f"b{l}", 1, H, False)
-    take("W4", 2, H, True)
-    take("b4", 1, 2, False)
+    take("W4", 4, H, True)
+    take("b4", 1, 4, False)
     h = torch.relu(X @ p["W0"].T + p["b0"])
     for l in (1, 2, 3):
         m = M @ (A @ h)
         h = torch.relu(torch.cat([h, m], 1) @ p[f"W{l}"].T + p[f"b{l}"])
     raw = h @ p["W4"].T + p["b4"]
-    pred = X[:, 7:9] + 0.25 * torch.tanh(raw)
+    d = X[:, 7:9]
+    pred = torch.cat([d, d], 1) + 0.25 * torch.tanh(raw)
     t = torch.tensor(target, dtype=torch.float64)
     loss = ((pred[:nn] - t) ** 2).sum() / (2 * nn)
     loss.backward()
@@ -121,25 +123,27 @@ def test_forward_loss_and_gradients_match_autograd():
     g = placer.Gnn(seed=4)
     w = g.get_weights()
     # larger output weights so every layer carries gradient
-    w[-(2 * H + 2):] = np.random.default_rng(1).uniform(-0.5, 0.5, 2 * H + 2).astype(np.float32)
+    w[-(4 * H + 4):] = np.random.default_rng(1).uniform(-0.5, 0.5, 4 * H + 4).astype(np.float32)
     g.set_weights(w)
     x = g.features(e)
     i = e.info
     rng = np.random.default_rng(7)
     nn = nl.num_nodes
-    tgt = rng.uniform(0.05, 0.95, (nn, 2))
+    tgt = rng.uniform(0.05, 0.95, (nn, 4))
     core_w, core_h = i.core_urx - i.core_llx, i.core_ury - i.core_lly
-    target_xy = np.stack([i.core_llx + tgt[:, 0] * core_w, i.core_lly + tgt[:, 1] * core_h], 1).astype(np.float32)
-    tgt_norm = np.stack([(target_xy[:, 0] - i.core_llx) / core_w, (target_xy[:, 1] - i.core_lly) / core_h], 1)
-    loss, grad = g.loss_grad(e, target_xy)
+    lo = np.array([i.core_llx, i.core_lly] * 2)
+    size = np.array([core_w, core_h] * 2)
+    target4 = (lo + tgt * size).astype(np.float32)
+    tgt_norm = (target4.astype(np.float64) - lo) / size
+    loss, grad = g.loss_grad(e, target4)
     rl, rpred, rgrad = torch_loss(x, w, nl, tgt_norm, nn)
     assert loss == pytest.approx(rl, rel=1e-5)
     pred = g.forward(e)
-    ref_xy = np.stack([i.core_llx + rpred[:nn, 0] * core_w, i.core_lly + rpred[:nn, 1] * core_h], 1)
-    assert np.abs(pred - ref_xy).max() < 1e-5 * max(core_w, core_h)
+    ref = lo + rpred[:nn] * size
+    assert np.abs(pred - ref).max() < 1e-5 * max(core_w, core_h)
     assert np.abs(grad - rgrad).max() < 1e-4 * np.abs(rgrad).max()
     # every block of weights receives gradient
-    assert np.abs(grad[:H * F]).max() > 0 and np.abs(grad[-(2 * H + 2):]).max() > 0
+    assert np.abs(grad[:H * F]).max() > 0 and np.abs(grad[-(4 * H + 4):]).max() > 0
     g.close()
     e.close()
 
@@ -148,9 +152,10 @@ def test_training_is_repeatable_and_learns():
     nl = small_design(2000, 9)
     e = placer.Engine(nl, placer.default_params(target_density=1.0))
     e.quadratic_placement()
+    qp = e.get_positions()[:nl.num_nodes]
     e.initialize()
     e.nesterov_run()
-    target = e.get_positions()[:nl.num_nodes]
+    target = np.concatenate([qp, e.get_positions()[:nl.num_nodes]], 1)
     runs = []
     for _ in range(2):
         g = placer.Gnn(seed=11)
@@ -163,21 +168,21 @@ def test_training_is_repeatable_and_learns():
     e.close()
 
 
-def test_proposal_at_alpha_zero_is_the_diffusion():
+@pytest.mark.parametrize("alpha", [0.0, 0.4, 1.0])
+def test_proposal_blends_the_two_heads(alpha):
     nl = small_design(3000, 5)
     e = placer.Engine(nl, placer.default_params(target_density=1.0))
     g = placer.Gnn(seed=2)
-    x = g.features(e)
-    g.propose(e, 0.0)
+    p = g.forward(e).astype(np.float64)
+    g.propose(e, alpha)
     i = e.info
     xy = e.get_positions()[:nl.num_nodes]
-    ref = np.stack([i.core_llx + x[:nl.num_nodes, 7] * (i.core_urx - i.core_llx),
-                    i.core_lly + x[:nl.num_nodes, 8] * (i.core_ury - i.core_lly)], 1)
-    # clamping keeps a node's box inside the core
-    w = nl.node_w[:, None].astype(np.float64)
-    assert np.abs(xy - ref).max() <= w.max() / 2 + 1e-3
-    inside = (ref[:, 0] - w[:, 0] / 2 > i.core_llx + 1e-3) & (ref[:, 0] + w[:, 0] / 2 < i.core_urx - 1e-3) & \
+    ref = p[:, :2] + alpha * (p[:, 2:] - p[:, :2])
+    # the core clamp keeps a node's box inside the core
+    hw = nl.node_w.astype(np.float64) / 2
+    inside = (ref[:, 0] - hw > i.core_llx + 1e-3) & (ref[:, 0] + hw < i.core_urx - 1e-3) & \
              (ref[:, 1] - 0.5 > i.core_lly + 1e-3) & (ref[:, 1] + 0.5 < i.core_ury - 1e-3)
+    assert inside.mean() > 0.9
     assert np.abs(xy[inside] - ref[inside]).max() < 1e-3
     g.close()
     e.close()
