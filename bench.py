@@ -6,9 +6,11 @@ precision against the plain FP64 form, HPWL within 0.5%; one B200 per rank.
 
 A "step" is one placement of the design from its netlist, resident on the
 device, to overflow < 0.1:
-  learned+mixed (the product; `value`)  the network's proposal (graph build,
+  learned+mixed (the product; `value`)  the network's proposal (graph,
          pad-anchored diffusion features, forward pass; ep_gnn_propose with
-         the committed weights) then mGP in the mixed-precision form;
+         the committed weights and alpha), the committed number of rounds of
+         the quadratic model from it (ep_quadratic_refine), then mGP in the
+         mixed-precision form;
   plain  the device quadratic placement (the reference flow's start) then
          mGP with every vector, map and wirelength term in FP64.
 Both are timed with CUDA events on the engines' stream around the whole
@@ -48,11 +50,11 @@ DESIGN = dict(cells=200_000, seed=7, start_seed=3, start_sigma=0.05)
 REF_RUNS = os.path.join(ROOT, "tests", "golden", "reference_runs.json")
 SAMPLE_ITERS = 8  # reference optimizer steps of the cpu_baseline sample
 # kernels one ep_gnn_propose launches on a netlist it has not bound: the
-# features (initial values, terminal pin counts and feature, 1/degree, 512
+# features (initial values, terminal pin counts and feature, 1/degree, 128
 # diffusion steps of 2 kernels, 3 feature stores), the forward pass (input
 # layer, 3 x (net mean, node mean, dense), output), the proposal and the
 # position store
-GNN_LAUNCHES = 4 + 2 * 512 + 3 + 1 + 3 * 3 + 1 + 2
+GNN_LAUNCHES = 4 + 2 * 128 + 3 + 1 + 3 * 3 + 1 + 2
 
 
 def netlist():
@@ -282,6 +284,9 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    # the engines, the network and the timing events share this stream (the
+    # legacy default stream does not order against the engines' own streams)
+    torch.cuda.set_stream(torch.cuda.Stream())
     dist = None
     if world > 1:
         import datetime
@@ -291,7 +296,7 @@ def main():
     from eplace_b200 import placer, warmstart
     nl = netlist()
     stream = torch.cuda.current_stream()
-    weights, alpha = warmstart.load_weights()
+    weights, alpha, rounds = warmstart.load_weights()
     gnn = placer.Gnn(device=local, weights=weights)
 
     def engine(precision):
@@ -320,7 +325,7 @@ def main():
         gnn.release(mixed)  # the proposal builds the graph and features afresh
         t0 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        gnn.propose(mixed, alpha)
+        warmstart.propose(gnn, mixed, alpha, rounds)
         t1 = torch.cuda.Event(enable_timing=True)
         t1.record(stream)
         mixed.initialize()
@@ -378,7 +383,7 @@ def main():
         t0 = time.perf_counter()
         e = placer.Engine(nl, placer.default_params(target_density=1.0, precision=precision, device=local))
         if start == "gnn":
-            gnn.propose(e, alpha)
+            warmstart.propose(gnn, e, alpha, rounds)
         else:
             e.quadratic_placement()
         e.initialize()
@@ -415,7 +420,8 @@ def main():
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": workload_config(nl, dict(
                    fillers=info.num_fillers, parallelism=f"replicas x{world}" if world > 1 else "1 GPU",
-                   product="learned warm start (ep_gnn_propose, alpha %.2f) + mixed-precision mGP" % alpha,
+                   product=("learned warm start (ep_gnn_propose, alpha %.2f, then %d rounds of ep_quadratic_refine)"
+                            " + mixed-precision mGP" % (alpha, rounds)),
                    plain="device quadratic placement + FP64 mGP",
                    mixed_precision="FP32 positions, FFT Poisson, gather and WA; int64 fixed-point density; "
                                    "FP64 reductions; network BF16 weights, FP32 accumulate",

@@ -1966,7 +1966,10 @@ ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, double err[2], 
 extern "C" {
 
 // ep_quadratic_placement's body (its set-up builds host arrays).
-static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
+// from_centre: the reference's flow (every node to the core centre first,
+// rounds until converged or max_iterations + 1); otherwise exactly
+// max_iterations rounds from the current centres.
+static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool from_centre, ep_qp_stats *stats) {
     if (e->in_run) {
         e->err = "ep_quadratic_placement cannot run inside an optimizer run";
         return EP_ERR_STATE;
@@ -1984,7 +1987,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp
     const int max_outer = max_iterations > 0 ? max_iterations : 20;  // IPiteCount, default 20
     const double target_error = 0.000001;                           // qplace.cpp:47
     CK(cudaEventRecord(e->ev0, st));
-    qp_center(q, e->grid, e->size, qpos, st);  // moveNodesCenterToCenter
+    if (from_centre) qp_center(q, e->grid, e->size, qpos, st);  // moveNodesCenterToCenter
     qp_bounds(q, qpos, q.out, st);
     if ((s = qp_read(e, 1))) return s;
     double hpwl = e->qp_out_h[0], err[2] = {0, 0};
@@ -1999,6 +2002,10 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp
         if ((s = qp_read(e, 1))) return s;
         hpwl = e->qp_out_h[0];
         outer = i + 1;
+        if (!from_centre) {
+            if (outer >= max_iterations) break;
+            continue;
+        }
         if (std::fabs(err[0]) < target_error && std::fabs(err[1]) < target_error && i > 4) break;
         if (i >= max_outer) break;
     }
@@ -2022,7 +2029,16 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp
 ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
     if (!e) return EP_ERR_ARG;
     try {
-        return quadratic_placement(e, max_iterations, stats);
+        return quadratic_placement(e, max_iterations, true, stats);
+    } catch (const std::bad_alloc &) {
+        return host_oom(e);
+    }
+}
+
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, ep_qp_stats *stats) {
+    if (!e || rounds < 1) return EP_ERR_ARG;
+    try {
+        return quadratic_placement(e, rounds, false, stats);
     } catch (const std::bad_alloc &) {
         return host_oom(e);
     }

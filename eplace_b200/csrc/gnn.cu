@@ -13,12 +13,12 @@
 //
 // Features (kF per node, from the netlist alone, computed on the device):
 // log(1 + area) / 4, log(1 + pins) / 3, terminal flag, and the node's
-// coordinates (normalised to the core) after 32, 128 and 512 steps of
+// coordinates (normalised to the core) after 8, 32 and 128 steps of
 // pad-anchored diffusion: every movable node starts at the core centre,
 // terminals sit at their own centres, and a step replaces each movable node
 // by node_mean(net_mean(.)).  These are the fixed-pin distances the network
 // reads: a node's diffused coordinate says how its pads pull it, at three
-// ranges; d, the 512-step coordinates, is the base of the predictions.
+// ranges; d, the 128-step coordinates, is the base of the predictions.
 //
 // Network (hidden 64, weights stored BF16 for the forward pass, FP32
 // accumulate, FP32 master weights for training):
@@ -50,7 +50,7 @@ constexpr int kH = 64;      // hidden width
 constexpr int kF = 9;       // input features
 constexpr int kOut = 4;     // q (x, y), f (x, y)
 constexpr int kLayers = 3;  // message-passing layers
-constexpr int kDiffSteps[3] = {32, 128, 512};
+constexpr int kDiffSteps[3] = {8, 32, 128};
 constexpr float kCorr = 0.25f;  // bound of a head's correction, in core sizes
 
 // Parameter layout (floats): W0[kH][kF], b0[kH], per layer W[kH][2kH], b[kH],

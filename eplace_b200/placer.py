@@ -114,7 +114,7 @@ EXPORTS = (
     "ep_set_stream", "ep_synchronize", "ep_get_positions", "ep_set_positions", "ep_initialize",
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_positions_f64", "ep_get_field_f64", "ep_get_component_gradients_f64",
-    "ep_get_limits", "ep_set_limits",
+    "ep_get_limits", "ep_set_limits", "ep_quadratic_refine",
     "ep_gnn_num_weights", "ep_gnn_create", "ep_gnn_destroy", "ep_gnn_last_error", "ep_gnn_get_weights",
     "ep_gnn_set_weights", "ep_gnn_release", "ep_gnn_features", "ep_gnn_forward", "ep_gnn_loss_grad",
     "ep_gnn_train_step", "ep_gnn_propose",
@@ -176,6 +176,7 @@ def load():
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
+    L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_run_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(RunStats)]
     L.ep_netbin_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.c_float, ctypes.c_int32]
     L.ep_netbin_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_float),
@@ -532,6 +533,12 @@ class Engine:
         """QPPlacer::quadraticPlacement on the device; returns its stats."""
         st = QpStats()
         self._check(self._L.ep_quadratic_placement(self.h, int(max_iterations), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in QpStats._fields_}
+
+    def quadratic_refine(self, rounds):
+        """ep_quadratic_refine: rounds of the quadratic model from the current centres."""
+        st = QpStats()
+        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
     def switch_stage(self, stage, filler_ll=None):

@@ -12,10 +12,12 @@ that proposes the initial placement in place of the quadratic placement
   * training: Adam on the mean squared error of the network's two heads
     against the engine's quadratic placement and final mGP centres of each
     design (normalised to the core), one design per step in a seeded order;
-  * proposal strength alpha: the start is q + alpha (f - q), q and f the two
-    heads; alpha is picked on validation designs (not the held-out ones):
-    the largest alpha whose runs end with a mean HPWL within 0.3% of the
-    QP-started runs, else the one with the lowest mean HPWL;
+  * the start: the network's proposal q + alpha (f - q), q and f the two
+    heads, then `rounds` rounds of the quadratic model from there
+    (ep_quadratic_refine; 0 = none).  (alpha, rounds) are picked on
+    validation designs (not the held-out ones): the fewest rounds, then the
+    largest alpha, whose runs end with a mean HPWL within 0.3% of the
+    QP-started runs, else the pair with the lowest mean HPWL;
   * evaluation: on held-out designs, the QP-started run against the
     proposal-started run (iterations and device seconds to overflow < 0.1,
     final HPWL), and the judge: a proposal is kept when its run reaches the
@@ -51,13 +53,22 @@ def training_sizes(count, seed, lo=2_000, hi=50_000):
 
 
 def load_weights(path=WEIGHTS):
+    """(weights, alpha, rounds) of a trained network."""
     z = np.load(path)
-    return z["weights"], float(z["alpha"])
+    return z["weights"], float(z["alpha"]), int(z["rounds"])
 
 
-def save_weights(path, weights, alpha, meta):
-    np.savez(path, weights=np.asarray(weights, np.float32), alpha=np.float32(alpha),
+def save_weights(path, weights, alpha, rounds, meta):
+    np.savez(path, weights=np.asarray(weights, np.float32), alpha=np.float32(alpha), rounds=np.int32(rounds),
              meta=np.array(json.dumps(meta)))
+
+
+def propose(gnn, engine, alpha, rounds):
+    """The learned start: the network's proposal, then `rounds` rounds of
+    the quadratic model from it."""
+    gnn.propose(engine, alpha)
+    if rounds > 0:
+        engine.quadratic_refine(rounds)
 
 
 def log_pair(directory, name, nl, final_xy):
@@ -116,7 +127,7 @@ def run_from(engine, start):
     return st
 
 
-def compare(gnn, nl, alpha, precision=placer.PREC_MIXED, tolerance=0.005):
+def compare(gnn, nl, alpha, rounds, precision=placer.PREC_MIXED, tolerance=0.005):
     """The QP-started run against the proposal-started run on one design.
     Device seconds of each start (quadratic placement; graph build, features
     and forward pass of the network) and of each mGP run."""
@@ -130,7 +141,7 @@ def compare(gnn, nl, alpha, precision=placer.PREC_MIXED, tolerance=0.005):
     e.load_positions()
     e.synchronize()
     t0 = time.perf_counter()
-    gnn.propose(e, alpha)
+    propose(gnn, e, alpha, rounds)
     e.synchronize()
     t_gnn = time.perf_counter() - t0
     r = run_from(e, "gnn")
@@ -144,25 +155,32 @@ def compare(gnn, nl, alpha, precision=placer.PREC_MIXED, tolerance=0.005):
     return out
 
 
-def pick_alpha(gnn, netlists, alphas=(0.0, 0.125, 0.25, 0.375, 0.5, 0.75, 1.0), within=0.003):
-    """On these (validation) netlists: the largest alpha whose
-    proposal-started runs end with a mean HPWL ratio to the QP-started runs
-    of at most 1 + within, else the alpha with the lowest mean ratio."""
-    table = {a: [] for a in alphas}
+def pick_start(gnn, netlists, alphas=(0.0, 0.25, 0.5), rounds=(0, 1, 2, 3, 5), within=0.003):
+    """On these (validation) netlists: the fewest refinement rounds, then the
+    largest alpha, whose runs end with a mean HPWL ratio to the QP-started
+    runs of at most 1 + within, else the pair with the lowest mean ratio.
+    Returns (alpha, rounds) and the table of mean ratios and iterations."""
+    keys = [(a, r) for r in rounds for a in alphas]
+    ratio = {k: [] for k in keys}
+    iters = {k: [] for k in keys}
     for nl in netlists:
         e = placer.Engine(nl, placer.default_params(target_density=1.0))
         e.save_positions()
         e.quadratic_placement()
         ref = run_from(e, "qp")["hpwl"]
-        for a in alphas:
+        for a, r in keys:
             e.load_positions()
-            gnn.propose(e, a)
-            table[a].append(run_from(e, f"gnn{a}")["hpwl"] / ref)
+            propose(gnn, e, a, r)
+            st = run_from(e, f"gnn{a}/{r}")
+            ratio[(a, r)].append(st["hpwl"] / ref)
+            iters[(a, r)].append(st["iterations"])
         gnn.release(e)
         e.close()
-    mean = {a: float(np.mean(v)) for a, v in table.items()}
-    ok = [a for a in alphas if mean[a] <= 1.0 + within]
-    return (max(ok) if ok else min(mean, key=mean.get)), mean
+    mean = {k: float(np.mean(v)) for k, v in ratio.items()}
+    ok = [k for k in keys if mean[k] <= 1.0 + within]
+    best = min(ok, key=lambda k: (k[1], -k[0])) if ok else min(mean, key=mean.get)
+    table = {f"{a}/{r}": dict(hpwl_ratio=mean[(a, r)], iterations=float(np.mean(iters[(a, r)]))) for a, r in keys}
+    return best, table
 
 
 def _seeds(spec):
@@ -203,18 +221,18 @@ def main():
             gnn.release(e)
             e.close()
         valid = [design(n, 900_000 + i) for i, n in enumerate(training_sizes(a.valid, a.seed + 7, 40_000, 120_000))]
-        alpha, table = pick_alpha(gnn, valid)
+        (alpha, rounds), table = pick_start(gnn, valid)
         meta = dict(designs=a.designs, steps=a.steps, lr=a.lr, seed=a.seed, final_loss=float(np.mean(losses[-100:])),
-                    first_loss=float(np.mean(losses[:50])), alpha_table=table, generate_s=t_gen, place_s=t_place,
+                    first_loss=float(np.mean(losses[:50])), start_table=table, generate_s=t_gen, place_s=t_place,
                     iterations=[int(s["iterations"]) for s in stats])
-        save_weights(a.out, gnn.get_weights(), alpha, meta)
-        print(json.dumps(dict(alpha=alpha, **meta)))
+        save_weights(a.out, gnn.get_weights(), alpha, rounds, meta)
+        print(json.dumps(dict(alpha=alpha, rounds=rounds, **meta)))
     else:
-        w, alpha = load_weights(a.weights)
+        w, alpha, rounds = load_weights(a.weights)
         gnn = placer.Gnn(weights=w)
         rows = []
         for s in _seeds(a.seeds):
-            r = compare(gnn, design(a.cells, s), alpha)
+            r = compare(gnn, design(a.cells, s), alpha, rounds)
             r["seed"] = s
             rows.append(r)
             print(json.dumps({k: r[k] for k in ("seed", "hpwl_ratio", "kept")} |
@@ -222,7 +240,7 @@ def main():
                               for f in ("iterations", "seconds", "start_seconds", "hpwl")}), flush=True)
         if a.out:
             with open(a.out, "w") as f:
-                json.dump(dict(alpha=alpha, rows=rows), f, indent=1)
+                json.dump(dict(alpha=alpha, rounds=rounds, rows=rows), f, indent=1)
 
 
 if __name__ == "__main__":

@@ -270,6 +270,11 @@ ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy);
  * the fifth, or after max_iterations + 1 rounds (0 = the reference's 20).
  * Fillers are not moved.  ep_initialize must run again afterwards. */
 ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats);
+/* `rounds` rounds of the same quadratic model starting from the current
+ * centres instead of the core centre (no convergence test): a short
+ * refinement of a start from elsewhere, e.g. ep_gnn_propose.  No
+ * counterpart in the reference. */
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, ep_qp_stats *stats);
 
 /* FirstOrderOptimizer::opt (Optimization/opt.hpp:30-36) with
  * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:
@@ -395,12 +400,12 @@ ep_status ep_density_scatter_noalloc(const ep_scatter_grid *grid, int32_t num_ob
  * Graph: an engine's movable nodes and terminals joined by its nets (read
  * from the engine's device arrays); mean aggregations node -> net -> node.
  * Input features per node: log(1 + area)/4, log(1 + pins)/3, terminal flag,
- * and its core-normalised coordinates after 32, 128 and 512 steps of
+ * and its core-normalised coordinates after 8, 32 and 128 steps of
  * pad-anchored diffusion (movable nodes start at the core centre, terminals
  * stay at their centres, a step is node <- mean of its nets <- mean of their
  * pins).  Network: h0 = relu(W0 x + b0); three layers h = relu(W [h ; mean
  * of the nets' mean of h] + b), hidden 64; two heads q, f = d + 0.25
- * tanh(W4 h + b4), d the 512-step coordinates: q predicts the engine's
+ * tanh(W4 h + b4), d the 128-step coordinates: q predicts the engine's
  * quadratic placement of the design, f its final mGP placement.  Weights
  * are FP32 masters with BF16 copies used by the forward pass (FP32
  * accumulate); training minimises the mean squared error of both heads

@@ -4,7 +4,7 @@ the network -- test-side only).
 
 Tolerances:
   * diffusion features: 1e-5 absolute (core-normalised coordinates) against
-    the same 32/128/512 mean-aggregation steps in float64;
+    the same 8/32/128 mean-aggregation steps in float64;
   * both heads' predictions and the loss: 1e-5 relative; every weight
     gradient: 1e-4 of the largest gradient entry, against autograd on the
     BF16-rounded weights (the forward pass uses BF16 weights, FP32
@@ -53,10 +53,10 @@ def features_ref(nl):
     v = np.concatenate([np.full((nn, 2), 0.5), np.stack([tcx, tcy], 1)]).astype(np.float64)
     has = pins[:nn] > 0
     cols = []
-    for k in range(1, 513):
+    for k in range(1, 129):
         new = node_mean @ (net_mean @ v)
         v[:nn][has] = new[:nn][has]
-        if k in (32, 128, 512):
+        if k in (8, 32, 128):
             cols.append(v.copy())
     return cols
 

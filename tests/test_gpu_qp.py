@@ -65,3 +65,22 @@ def test_qp_then_mgp_matches_reference_flow():
     st = e.nesterov_run()
     assert st["overflow"] < 0.1
     assert abs(st["hpwl"] / float(g["run_hpwl"]) - 1) < 0.02
+
+
+def test_quadratic_refine_keeps_a_converged_placement_and_improves_a_blob():
+    nl = synth.standard_cell(5_000, seed=3, every_cell_pinned=True, local_pads=True)
+    e = placer.Engine(nl, placer.default_params(target_density=1.0))
+    full = e.quadratic_placement()
+    ref = e.get_positions()
+    st = e.quadratic_refine(2)
+    assert st["rounds"] == 2
+    assert st["hpwl"] == pytest.approx(full["hpwl"], rel=0.005)
+    core = max(e.info.core_urx - e.info.core_llx, e.info.core_ury - e.info.core_lly)
+    assert np.abs(e.get_positions() - ref).mean() < 0.01 * core
+    b = placer.Engine(synth.blob_start(nl, sigma_frac=0.2), placer.default_params(target_density=1.0))
+    h0 = b.hpwl()
+    assert b.quadratic_refine(3)["hpwl"] < 0.5 * h0
+    with pytest.raises(placer.EPError):
+        b.quadratic_refine(0)
+    e.close()
+    b.close()
