@@ -14,7 +14,7 @@ mGP) on its smoke example ending within 2% of the reference's HPWL.
 import numpy as np
 import pytest
 
-from eplace_b200 import placer
+from eplace_b200 import placer, synth
 from tests.helpers import golden_netlist, load_golden
 
 pytestmark = pytest.mark.gpu
