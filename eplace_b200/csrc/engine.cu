@@ -100,11 +100,13 @@ struct ep_engine {
     // device copies of the net -> device pins and pin -> net maps (made at
     // creation; the quadratic placement and the learned warm start read them)
     int32_t *net_first = nullptr, *net_deg = nullptr, *pin_net = nullptr;
+    int32_t *net_dev_order = nullptr;  // nets in device pin order (grouped by degree)
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
     size_t qp_cap_x = 0, qp_cap_y = 0;
     double *qp_out_h = nullptr;  // pinned mirror of qp.out
+    QpSolve *qp_state_h = nullptr;  // pinned mirror of the device solver state
     int bk_trials = 64;       // backtracking trials per step before EP_ERR_TIMEOUT (ep_limits)
     int64_t launches = 0;     // engine kernels launched so far
     int64_t graph_kernels = 0;  // kernels in one replay of the step graph
@@ -904,9 +906,15 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     CK(cudaGetLastError());
     for (int v = 0; v < 3; v++)
         if ((s = dupload(e, e->view_idx[v], e->h_view[v]))) return s;
-    if ((s = dupload(e, e->net_first, e->h_net_first)) || (s = dupload(e, e->net_deg, e->h_net_deg)) ||
-        (s = dupload(e, e->pin_net, e->h_pin_net)))
-        return s;
+    {
+        std::vector<int32_t> order;
+        order.reserve(nnet);
+        for (int p = 0; p < np; p++)
+            if (p == 0 || e->h_pin_net[p] != e->h_pin_net[p - 1]) order.push_back(e->h_pin_net[p]);
+        if ((s = dupload(e, e->net_first, e->h_net_first)) || (s = dupload(e, e->net_deg, e->h_net_deg)) ||
+            (s = dupload(e, e->pin_net, e->h_pin_net)) || (s = dupload(e, e->net_dev_order, order)))
+            return s;
+    }
     if (P.step_rule == EP_STEP_BKTRK &&
         ((s = dalloc_bytes(e, e->bk_ysave, v2 * no)) || (s = dalloc_bytes(e, e->bk_gtrial, v2 * no)) ||
          (s = dalloc_bytes(e, e->bk_xtrial, v2 * no))))
@@ -1012,6 +1020,7 @@ void ep_destroy(ep_engine *e) {
     for (void *p : e->allocs) cudaFree(p);
     if (e->hS) cudaFreeHost(e->hS);
     if (e->qp_out_h) cudaFreeHost(e->qp_out_h);
+    if (e->qp_state_h) cudaFreeHost(e->qp_state_h);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -1833,13 +1842,14 @@ ep_status qp_setup(ep_engine *e) {
         (s = dalloc(e, q.rhs, nn)) || (s = dalloc(e, q.x, nn)) || (s = dalloc(e, q.r, nn)) ||
         (s = dalloc(e, q.r0, nn)) || (s = dalloc(e, q.p, nn)) || (s = dalloc(e, q.v, nn)) ||
         (s = dalloc(e, q.s, nn)) || (s = dalloc(e, q.t, nn)) || (s = dalloc(e, q.partials, 4 * (size_t)pb)) ||
-        (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)))
+        (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)) || (s = dalloc(e, q.solve, 1)))
         return s;
     q.pin_net = e->pin_net;
     q.net_first = e->net_first;
     q.net_deg = e->net_deg;
     CK(cudaMemset(q.cnt, 0, sizeof(unsigned)));
     CK(cudaMallocHost((void **)&e->qp_out_h, 4 * sizeof(double)));
+    CK(cudaMallocHost((void **)&e->qp_state_h, sizeof(QpSolve)));
     e->qp_cap_x = e->qp_cap_y = cap;
     e->qp_ready = true;
     return EP_OK;
@@ -1878,86 +1888,31 @@ ep_status qp_build(ep_engine *e, const float2 *qpos) {
 }
 
 // BiCGSTAB as Eigen implements it (van der Vorst's method with a restart
-// when r0.r vanishes; identity preconditioner), both axes at once: stop when
-// |r|^2 <= (eps |b|)^2 with eps the float epsilon, or after max_it
-// iterations; the current centres are the initial guess.  err[c] = |r|/|b|
-// at the end, the value QPPlacer reads as solver.error().
+// when r0.r vanishes; identity preconditioner), both axes at once, on the
+// device (qp.cu): stop when |r|^2 <= (eps |b|)^2 with eps the float epsilon,
+// or after max_it iterations; the current centres are the initial guess.
+// The host enqueues iterations in chunks and reads the solver state once per
+// chunk.  err[c] = |r|/|b| at the end, the value QPPlacer reads as
+// solver.error().
 ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, double err[2], int &iters) {
     QpDev &q = e->qp;
     cudaStream_t st = e->st;
-    const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
+    constexpr int kChunk = 10;
     qp_to_x(q, qpos, st);
-    qp_init(q, st);
-    ep_status s = qp_read(e, 4);
-    if (s) return s;
-    double rr[2] = {e->qp_out_h[0], e->qp_out_h[1]}, bb[2] = {e->qp_out_h[2], e->qp_out_h[3]};
-    double r0sq[2] = {rr[0], rr[1]};
-    double rho[2] = {1, 1}, alpha[2] = {1, 1}, w[2] = {1, 1};
-    double r0r[2] = {rr[0], rr[1]};  // r0.r of the current residual (r0 = r at the start)
-    double tol2[2];
-    int it[2] = {0, 0}, restarts[2] = {0, 0};
-    bool active[2];
-    for (int c = 0; c < 2; c++) {
-        tol2[c] = eps2 * bb[c];
-        if (bb[c] == 0.0) {  // x = 0 (Eigen returns at once)
-            qp_zero_axis(q, c, st);
-            rr[c] = 0.0;
-            active[c] = false;
-        } else {
-            active[c] = rr[c] > tol2[c] && max_it > 0;
-        }
+    qp_init(q, max_it, st);
+    QpSolve h{};
+    for (int done = 0; done < max_it;) {
+        const int n = std::min(kChunk, max_it - done);
+        qp_iterations(q, n, st);
+        done += n;
+        CK(cudaMemcpyAsync(e->qp_state_h, q.solve, sizeof(QpSolve), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        h = *e->qp_state_h;
+        if (!h.active[0] && !h.active[1]) break;
     }
-    iters = 0;
-    while (active[0] || active[1]) {
-        double rho_old[2] = {rho[0], rho[1]};
-        int restart = 0;
-        for (int c = 0; c < 2; c++) {
-            if (!active[c]) continue;
-            rho[c] = r0r[c];
-            if (std::fabs(rho[c]) < eps2 * r0sq[c]) restart |= 1 << c;
-        }
-        if (restart) {
-            // r = b - A x, r0 = r, rho = r0sq = |r|^2
-            qp_restart(q, restart, st);
-            if ((s = qp_read(e, 2))) return s;
-            for (int c = 0; c < 2; c++)
-                if (restart & (1 << c)) {
-                    rho[c] = r0sq[c] = e->qp_out_h[c];
-                    if (restarts[c]++ == 0) it[c] = 0;
-                }
-        }
-        float2 fb = make_float2(0.f, 0.f), fw = make_float2(0.f, 0.f), fa = make_float2(0.f, 0.f);
-        double beta[2] = {0, 0};
-        for (int c = 0; c < 2; c++)
-            if (active[c]) beta[c] = (rho[c] / rho_old[c]) * (alpha[c] / w[c]);
-        fb = make_float2((float)beta[0], (float)beta[1]);
-        fw = make_float2(active[0] ? (float)w[0] : 0.f, active[1] ? (float)w[1] : 0.f);
-        qp_dir(q, fb, fw, st);  // p = r + beta (p - w v)
-        qp_av(q, st);           // v = A p, r0.v
-        if ((s = qp_read(e, 2))) return s;
-        for (int c = 0; c < 2; c++) alpha[c] = active[c] ? rho[c] / e->qp_out_h[c] : 0.0;
-        fa = make_float2((float)alpha[0], (float)alpha[1]);
-        qp_s(q, fa, st);  // s = r - alpha v
-        qp_at(q, st);     // t = A s, t.t, t.s
-        if ((s = qp_read(e, 4))) return s;
-        for (int c = 0; c < 2; c++) {
-            if (!active[c]) continue;
-            const double tt = e->qp_out_h[c], ts = e->qp_out_h[2 + c];
-            w[c] = tt > 0.0 ? ts / tt : 0.0;
-        }
-        fw = make_float2(active[0] ? (float)w[0] : 0.f, active[1] ? (float)w[1] : 0.f);
-        qp_step(q, fa, fw, st);  // x += alpha p + w s, r = s - w t, |r|^2, r0.r
-        if ((s = qp_read(e, 4))) return s;
-        iters++;
-        for (int c = 0; c < 2; c++) {
-            if (!active[c]) continue;
-            rr[c] = e->qp_out_h[c];
-            r0r[c] = e->qp_out_h[2 + c];
-            it[c]++;
-            active[c] = rr[c] > tol2[c] && it[c] < max_it;
-        }
-    }
-    for (int c = 0; c < 2; c++) err[c] = bb[c] > 0.0 ? std::sqrt(rr[c] / bb[c]) : 0.0;
+    CK(cudaGetLastError());
+    iters = h.iters;
+    for (int c = 0; c < 2; c++) err[c] = h.bb[c] > 0.0 ? std::sqrt(h.rr[c] / h.bb[c]) : 0.0;
     return EP_OK;
 }
 
@@ -2065,6 +2020,7 @@ int engine_graph(ep_engine *e, EngineGraph *g) {
     g->d_net_first = e->net_first;
     g->d_net_deg = e->net_deg;
     g->d_pin_net = e->pin_net;
+    g->d_net_dev_order = e->net_dev_order;
     g->d_obj_pin_start = e->obj_pin_start;
     g->d_obj_pin_dev = e->obj_pin_dev;
     g->d_area = e->area;

@@ -185,6 +185,7 @@ struct EngineGraph {
     const float2 *term_centre;           // [nt]
     // the same netlist on the device
     const int32_t *d_pin_owner, *d_net_first, *d_net_deg, *d_pin_net;
+    const int32_t *d_net_dev_order;  // [nnet] nets in device pin order (grouped by degree)
     const int32_t *d_obj_pin_start, *d_obj_pin_dev;  // object -> its device pins
     const float *d_area, *d_npins;                   // [n_obj]
     const void *d_pos;                               // [n_obj + nt] centres, vec2<R>
@@ -199,6 +200,12 @@ int engine_set_node_centres(ep_engine *e, const float2 *xy);
 void engine_set_error(ep_engine *e, const char *msg);
 
 // ---- quadratic placement (qp.cu) ---------------------------------------------
+// Scalars of the device BiCGSTAB (per axis: X, Y), see qp.cu.
+struct QpSolve {
+    double rho[2], rho_old[2], alpha[2], w[2], r0sq[2], rr[2], bb[2], tol2[2], r0r[2];
+    int it[2], restarts[2], active[2];
+    int restart_mask, zero_mask, iters, max_it;
+};
 // Device view of one engine's quadratic placement: the netlist in device pin
 // order (nets contiguous) plus the per-round systems and BiCGSTAB vectors,
 // both axes side by side in float2 (x for the X system, y for the Y system).
@@ -218,18 +225,15 @@ struct QpDev {
     float2 *x, *r, *r0, *p, *v, *s, *t;
     double *partials;
     unsigned *cnt;
-    double *out;  // [4] sums of the last reduction
+    double *out;      // [4] sums of the last reduction (bounds: HPWL)
+    QpSolve *solve;   // device BiCGSTAB state
 };
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st);
 void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st);
-void qp_init(const QpDev &q, cudaStream_t st);
-void qp_dir(const QpDev &q, float2 beta, float2 w, cudaStream_t st);
-void qp_av(const QpDev &q, cudaStream_t st);
-void qp_s(const QpDev &q, float2 alpha, cudaStream_t st);
-void qp_at(const QpDev &q, cudaStream_t st);
-void qp_step(const QpDev &q, float2 alpha, float2 w, cudaStream_t st);
-void qp_restart(const QpDev &q, int mask, cudaStream_t st);
-void qp_zero_axis(const QpDev &q, int axis, cudaStream_t st);
+// r = b - A x and the solver's initial state (zero right-hand sides give x = 0)
+void qp_init(const QpDev &q, int max_it, cudaStream_t st);
+// enqueue `count` BiCGSTAB iterations (no-ops once both axes have stopped)
+void qp_iterations(const QpDev &q, int count, cudaStream_t st);
 void qp_to_x(const QpDev &q, const float2 *pos, cudaStream_t st);
 void qp_from_x(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);
 void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);

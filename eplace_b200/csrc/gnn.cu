@@ -70,6 +70,7 @@ inline int nblk(long long n, int t = kT) { return (int)((n + t - 1) / t); }
 struct Net {
     int nn, n_obj, N, nnet;
     const int32_t *owner, *net_first, *net_deg, *pin_net, *obj_pin_start, *obj_pin_dev;
+    const int32_t *net_order;            // nets in device pin order (neighbouring nets of equal degree)
     const int32_t *pad_start, *pad_net;  // terminals' pins (training only; may be null)
 };
 
@@ -115,10 +116,13 @@ __global__ void k_inv_deg(int nnet, const int32_t *__restrict__ deg, float *__re
     if (n < nnet) inv[n] = deg[n] > 0 ? 1.f / deg[n] : 0.f;
 }
 
+// thread k takes the k-th net in device pin order, so a warp's nets have
+// (nearly) the same degree
 __global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ v,
                            float2 *__restrict__ a) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= g.nnet) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.nnet) return;
+    const int n = g.net_order[k];
     float sx = 0.f, sy = 0.f;
     for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
         const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
@@ -614,6 +618,7 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     n.pin_net = eg.d_pin_net;
     n.obj_pin_start = eg.d_obj_pin_start;
     n.obj_pin_dev = eg.d_obj_pin_dev;
+    n.net_order = eg.d_net_dev_order;
     n.pad_start = g->pad_start;
     n.pad_net = g->pad_net;
     cudaStream_t st = eg.st;

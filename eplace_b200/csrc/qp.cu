@@ -186,15 +186,33 @@ __device__ __forceinline__ float2 spmv_row(const QpMat &m, const float2 *__restr
     return make_float2(ax, ay);
 }
 
-__device__ __forceinline__ void qp_finish(double *acc, int nv, double *out) {
-    for (int k = 0; k < nv; k++) out[k] = acc[k];
-}
+// ---- BiCGSTAB on the device -----------------------------------------------------
+// Eigen's BiCGSTAB (van der Vorst's method, restart when r0.r vanishes,
+// identity preconditioner) for both systems at once, every scalar of the
+// recurrence kept in device memory (QpSolve) and updated by the finalising
+// block of the grid reduction that produces its inputs; vector kernels read
+// alpha, beta and omega from there.  Per axis c:
+//   pre      rho_old = rho; rho = r0.r; restart when |rho| < eps^2 r0sq
+//   restart  (only when flagged) r = b - A x, r0 = r; rho = r0sq = |r|^2,
+//            the iteration count reset at the first restart
+//   dir      p = r + beta (p - omega v), beta = (rho / rho_old)(alpha / omega)
+//   av       v = A p; alpha = rho / (r0.v)
+//   s        s = r - alpha v
+//   at       t = A s; omega = t.s / t.t (0 when t.t = 0)
+//   step     x += alpha p + omega s; r = s - omega t; |r|^2, r0.r; count;
+//            the axis stays active while |r|^2 > (eps |b|)^2 and the count
+//            is below the limit
+// An inactive axis uses alpha = beta = omega = 0 (its x and r stay), and
+// every kernel returns at once when neither axis is active, so iterations
+// can be enqueued ahead of the convergence test.
+__device__ __forceinline__ bool any_active(const QpSolve *S) { return S->active[0] || S->active[1]; }
 
-// r = b - A x, r0 = r, p = v = 0; sums (r.r per system, b.b per system).
+// r = b - A x, r0 = r, p = v = 0; |r|^2 and |b|^2 per system, then the
+// solver's initial state.
 __global__ void __launch_bounds__(kQT)
 k_qp_init(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restrict__ x, float2 *__restrict__ r,
           float2 *__restrict__ r0, float2 *__restrict__ p, float2 *__restrict__ v, double *__restrict__ partials,
-          unsigned *__restrict__ cnt, double *__restrict__ out) {
+          unsigned *__restrict__ cnt, int max_it, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -210,91 +228,61 @@ k_qp_init(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restr
         acc[2] = (double)bi.x * bi.x;
         acc[3] = (double)bi.y * bi.y;
     }
-    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) qp_finish(acc, 4, out);
+    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
+        const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
+        S->zero_mask = 0;
+        S->restart_mask = 0;
+        S->iters = 0;
+        for (int c = 0; c < 2; c++) {
+            S->rr[c] = acc[c];
+            S->bb[c] = acc[2 + c];
+            S->r0sq[c] = acc[c];
+            S->r0r[c] = acc[c];
+            S->rho[c] = S->alpha[c] = S->w[c] = 1.0;
+            S->it[c] = 0;
+            S->restarts[c] = 0;
+            S->tol2[c] = eps2 * S->bb[c];
+            if (S->bb[c] == 0.0) {  // x = 0 (Eigen returns at once)
+                S->zero_mask |= 1 << c;
+                S->rr[c] = 0.0;
+                S->active[c] = 0;
+            } else {
+                S->active[c] = S->rr[c] > S->tol2[c] && max_it > 0;
+            }
+        }
+        S->max_it = max_it;
+    }
 }
 
-// p = r + beta (p - w v)
-__global__ void __launch_bounds__(kQT)
-k_qp_dir(int nn, float2 beta, float2 w, const float2 *__restrict__ r, const float2 *__restrict__ v,
-         float2 *__restrict__ p) {
+// A zero right-hand side gives x = 0.
+__global__ void k_qp_zero(int nn, const QpSolve *__restrict__ S, float2 *__restrict__ x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nn) return;
-    const float2 ri = r[i], vi = v[i], pi = p[i];
-    p[i] = make_float2(ri.x + beta.x * (pi.x - w.x * vi.x), ri.y + beta.y * (pi.y - w.y * vi.y));
+    if (i >= nn || !S->zero_mask) return;
+    if (S->zero_mask & 1) x[i].x = 0.f;
+    if (S->zero_mask & 2) x[i].y = 0.f;
 }
 
-// v = A p; sums r0.v per system.
+__global__ void k_qp_pre(QpSolve *__restrict__ S) {
+    if (threadIdx.x != 0 || !any_active(S)) return;
+    const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
+    int restart = 0;
+    for (int c = 0; c < 2; c++) {
+        S->rho_old[c] = S->rho[c];
+        if (!S->active[c]) continue;
+        S->rho[c] = S->r0r[c];
+        if (fabs(S->rho[c]) < eps2 * S->r0sq[c]) restart |= 1 << c;
+    }
+    S->restart_mask = restart;
+}
+
+// Restart of the flagged systems: r = b - A x, r0 = r; rho = r0sq = |r|^2.
 __global__ void __launch_bounds__(kQT)
-k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict__ r0, float2 *__restrict__ v,
-        double *__restrict__ partials, unsigned *__restrict__ cnt, double *__restrict__ out) {
+k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restrict__ x, float2 *__restrict__ r,
+             float2 *__restrict__ r0, double *__restrict__ partials, unsigned *__restrict__ cnt,
+             QpSolve *__restrict__ S) {
     __shared__ double sh[2 * 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[2] = {0.0, 0.0};
-    if (i < nn) {
-        const float2 vi = spmv_row(m, p, i), z = r0[i];
-        v[i] = vi;
-        acc[0] = (double)z.x * vi.x;
-        acc[1] = (double)z.y * vi.y;
-    }
-    if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) qp_finish(acc, 2, out);
-}
-
-// s = r - alpha v
-__global__ void __launch_bounds__(kQT)
-k_qp_s(int nn, float2 alpha, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nn) return;
-    const float2 ri = r[i], vi = v[i];
-    s[i] = make_float2(ri.x - alpha.x * vi.x, ri.y - alpha.y * vi.y);
-}
-
-// t = A s; sums t.t and t.s per system.
-__global__ void __launch_bounds__(kQT)
-k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, double *__restrict__ partials,
-        unsigned *__restrict__ cnt, double *__restrict__ out) {
-    __shared__ double sh[4 * 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < nn) {
-        const float2 ti = spmv_row(m, s, i), si = s[i];
-        t[i] = ti;
-        acc[0] = (double)ti.x * ti.x;
-        acc[1] = (double)ti.y * ti.y;
-        acc[2] = (double)ti.x * si.x;
-        acc[3] = (double)ti.y * si.y;
-    }
-    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) qp_finish(acc, 4, out);
-}
-
-// x += alpha p + w s; r = s - w t; sums r.r and r0.r per system.
-__global__ void __launch_bounds__(kQT)
-k_qp_step(int nn, float2 alpha, float2 w, const float2 *__restrict__ p, const float2 *__restrict__ s,
-          const float2 *__restrict__ t, const float2 *__restrict__ r0, float2 *__restrict__ x,
-          float2 *__restrict__ r, double *__restrict__ partials, unsigned *__restrict__ cnt,
-          double *__restrict__ out) {
-    __shared__ double sh[4 * 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < nn) {
-        const float2 pi = p[i], si = s[i], ti = t[i], xi = x[i], z = r0[i];
-        x[i] = make_float2(xi.x + alpha.x * pi.x + w.x * si.x, xi.y + alpha.y * pi.y + w.y * si.y);
-        const float2 ri = make_float2(si.x - w.x * ti.x, si.y - w.y * ti.y);
-        r[i] = ri;
-        acc[0] = (double)ri.x * ri.x;
-        acc[1] = (double)ri.y * ri.y;
-        acc[2] = (double)z.x * ri.x;
-        acc[3] = (double)z.y * ri.y;
-    }
-    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) qp_finish(acc, 4, out);
-}
-
-// BiCGSTAB restart of the systems in `mask` (bit 0 X, bit 1 Y): r = b - A x,
-// r0 = r; sums r.r per system.
-__global__ void __launch_bounds__(kQT)
-k_qp_restart(int nn, int mask, QpMat m, const float2 *__restrict__ rhs, const float2 *__restrict__ x,
-             float2 *__restrict__ r, float2 *__restrict__ r0, double *__restrict__ partials,
-             unsigned *__restrict__ cnt, double *__restrict__ out) {
-    __shared__ double sh[2 * 32];
+    const int mask = S->restart_mask;
+    if (!mask || !any_active(S)) return;  // uniform over the grid
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[2] = {0.0, 0.0};
     if (i < nn) {
@@ -307,17 +295,117 @@ k_qp_restart(int nn, int mask, QpMat m, const float2 *__restrict__ rhs, const fl
         acc[0] = (double)ri.x * ri.x;
         acc[1] = (double)ri.y * ri.y;
     }
-    if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) qp_finish(acc, 2, out);
+    if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
+        for (int c = 0; c < 2; c++)
+            if (mask & (1 << c)) {
+                S->rho[c] = S->r0sq[c] = acc[c];
+                if (S->restarts[c]++ == 0) S->it[c] = 0;
+            }
+        S->restart_mask = 0;
+    }
 }
 
-// A zero right-hand side gives x = 0 (Eigen's BiCGSTAB returns at once).
-__global__ void k_qp_zero_axis(int nn, int axis, float2 *__restrict__ x) {
+// p = r + beta (p - omega v)
+__global__ void __launch_bounds__(kQT)
+k_qp_dir(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ p,
+         const QpSolve *__restrict__ S) {
+    if (!any_active(S)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
-    if (axis == 0)
-        x[i].x = 0.f;
-    else
-        x[i].y = 0.f;
+    float b[2], w[2];
+    for (int c = 0; c < 2; c++) {
+        b[c] = S->active[c] ? (float)((S->rho[c] / S->rho_old[c]) * (S->alpha[c] / S->w[c])) : 0.f;
+        w[c] = S->active[c] ? (float)S->w[c] : 0.f;
+    }
+    const float2 ri = r[i], vi = v[i], pi = p[i];
+    p[i] = make_float2(ri.x + b[0] * (pi.x - w[0] * vi.x), ri.y + b[1] * (pi.y - w[1] * vi.y));
+}
+
+// v = A p; alpha = rho / (r0.v)
+__global__ void __launch_bounds__(kQT)
+k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict__ r0, float2 *__restrict__ v,
+        double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
+    __shared__ double sh[2 * 32];
+    if (!any_active(S)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    if (i < nn) {
+        const float2 vi = spmv_row(m, p, i), z = r0[i];
+        v[i] = vi;
+        acc[0] = (double)z.x * vi.x;
+        acc[1] = (double)z.y * vi.y;
+    }
+    if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0)
+        for (int c = 0; c < 2; c++) S->alpha[c] = S->active[c] ? S->rho[c] / acc[c] : 0.0;
+}
+
+// s = r - alpha v
+__global__ void __launch_bounds__(kQT)
+k_qp_s(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ s,
+       const QpSolve *__restrict__ S) {
+    if (!any_active(S)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const float ax = (float)S->alpha[0], ay = (float)S->alpha[1];
+    const float2 ri = r[i], vi = v[i];
+    s[i] = make_float2(ri.x - ax * vi.x, ri.y - ay * vi.y);
+}
+
+// t = A s; omega = t.s / t.t
+__global__ void __launch_bounds__(kQT)
+k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, double *__restrict__ partials,
+        unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
+    __shared__ double sh[4 * 32];
+    if (!any_active(S)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < nn) {
+        const float2 ti = spmv_row(m, s, i), si = s[i];
+        t[i] = ti;
+        acc[0] = (double)ti.x * ti.x;
+        acc[1] = (double)ti.y * ti.y;
+        acc[2] = (double)ti.x * si.x;
+        acc[3] = (double)ti.y * si.y;
+    }
+    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0)
+        for (int c = 0; c < 2; c++)
+            if (S->active[c]) S->w[c] = acc[c] > 0.0 ? acc[2 + c] / acc[c] : 0.0;
+}
+
+// x += alpha p + omega s; r = s - omega t; |r|^2, r0.r; convergence per axis.
+__global__ void __launch_bounds__(kQT)
+k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, const float2 *__restrict__ t,
+          const float2 *__restrict__ r0, float2 *__restrict__ x, float2 *__restrict__ r, double *__restrict__ partials,
+          unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
+    __shared__ double sh[4 * 32];
+    if (!any_active(S)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float a[2], w[2];
+    for (int c = 0; c < 2; c++) {
+        a[c] = S->active[c] ? (float)S->alpha[c] : 0.f;
+        w[c] = S->active[c] ? (float)S->w[c] : 0.f;
+    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < nn) {
+        const float2 pi = p[i], si = s[i], ti = t[i], xi = x[i], z = r0[i];
+        x[i] = make_float2(xi.x + a[0] * pi.x + w[0] * si.x, xi.y + a[1] * pi.y + w[1] * si.y);
+        const float2 ri = make_float2(si.x - w[0] * ti.x, si.y - w[1] * ti.y);
+        r[i] = ri;
+        acc[0] = (double)ri.x * ri.x;
+        acc[1] = (double)ri.y * ri.y;
+        acc[2] = (double)z.x * ri.x;
+        acc[3] = (double)z.y * ri.y;
+    }
+    if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
+        S->iters++;
+        for (int c = 0; c < 2; c++) {
+            if (!S->active[c]) continue;
+            S->rr[c] = acc[c];
+            S->r0r[c] = acc[2 + c];
+            S->it[c]++;
+            S->active[c] = S->rr[c] > S->tol2[c] && S->it[c] < S->max_it;
+        }
+    }
 }
 
 // Node centres <-> solution vector (setModuleCenter_2D clamp on the way back).
@@ -357,39 +445,23 @@ void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
 
 static QpMat mat(const QpDev &q) { return QpMat{q.row_x, q.col_x, q.row_y, q.col_y, q.val_x, q.val_y, q.diag}; }
 
-void qp_init(const QpDev &q, cudaStream_t st) {
-    k_qp_init<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials, q.cnt,
-                                             q.out);
+void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
+    k_qp_init<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials, q.cnt, max_it,
+                                             q.solve);
+    k_qp_zero<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.solve, q.x);
 }
 
-void qp_dir(const QpDev &q, float2 beta, float2 w, cudaStream_t st) {
-    k_qp_dir<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, beta, w, q.r, q.v, q.p);
-}
-
-void qp_av(const QpDev &q, cudaStream_t st) {
-    k_qp_av<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.out);
-}
-
-void qp_s(const QpDev &q, float2 alpha, cudaStream_t st) {
-    k_qp_s<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, alpha, q.r, q.v, q.s);
-}
-
-void qp_at(const QpDev &q, cudaStream_t st) {
-    k_qp_at<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.out);
-}
-
-void qp_step(const QpDev &q, float2 alpha, float2 w, cudaStream_t st) {
-    k_qp_step<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, alpha, w, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt,
-                                             q.out);
-}
-
-void qp_restart(const QpDev &q, int mask, cudaStream_t st) {
-    k_qp_restart<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mask, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt,
-                                                q.out);
-}
-
-void qp_zero_axis(const QpDev &q, int axis, cudaStream_t st) {
-    k_qp_zero_axis<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, axis, q.x);
+void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
+    const int b = qblocks(q.nn);
+    for (int k = 0; k < count; k++) {
+        k_qp_pre<<<1, 32, 0, st>>>(q.solve);
+        k_qp_restart<<<b, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
+        k_qp_dir<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.p, q.solve);
+        k_qp_av<<<b, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
+        k_qp_s<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.s, q.solve);
+        k_qp_at<<<b, kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
+        k_qp_step<<<b, kQT, 0, st>>>(q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
+    }
 }
 
 void qp_to_x(const QpDev &q, const float2 *pos, cudaStream_t st) {
