@@ -296,7 +296,7 @@ def main():
     from eplace_b200 import placer, warmstart
     nl = netlist()
     stream = torch.cuda.current_stream()
-    weights, alpha, rounds = warmstart.load_weights()
+    weights, start = warmstart.load_weights()
     gnn = placer.Gnn(device=local, weights=weights)
 
     def engine(precision):
@@ -325,7 +325,7 @@ def main():
         gnn.release(mixed)  # the proposal builds the graph and features afresh
         t0 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        warmstart.propose(gnn, mixed, alpha, rounds)
+        warmstart.propose(gnn, mixed, start)
         t1 = torch.cuda.Event(enable_timing=True)
         t1.record(stream)
         mixed.initialize()
@@ -383,7 +383,7 @@ def main():
         t0 = time.perf_counter()
         e = placer.Engine(nl, placer.default_params(target_density=1.0, precision=precision, device=local))
         if start == "gnn":
-            warmstart.propose(gnn, e, alpha, rounds)
+            warmstart.propose(gnn, e, start)
         else:
             e.quadratic_placement()
         e.initialize()
@@ -420,8 +420,9 @@ def main():
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": workload_config(nl, dict(
                    fillers=info.num_fillers, parallelism=f"replicas x{world}" if world > 1 else "1 GPU",
-                   product=("learned warm start (ep_gnn_propose, alpha %.2f, then %d rounds of ep_quadratic_refine)"
-                            " + mixed-precision mGP" % (alpha, rounds)),
+                   product=("learned warm start (ep_gnn_propose, alpha %.2f, then %d rounds of ep_quadratic_refine"
+                            " of at most %d solver iterations) + mixed-precision mGP"
+                            % (start["alpha"], start["rounds"], start["iters"])),
                    plain="device quadratic placement + FP64 mGP",
                    mixed_precision="FP32 positions, FFT Poisson, gather and WA; int64 fixed-point density; "
                                    "FP64 reductions; network BF16 weights, FP32 accumulate",

@@ -1923,8 +1923,10 @@ extern "C" {
 // ep_quadratic_placement's body (its set-up builds host arrays).
 // from_centre: the reference's flow (every node to the core centre first,
 // rounds until converged or max_iterations + 1); otherwise exactly
-// max_iterations rounds from the current centres.
-static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool from_centre, ep_qp_stats *stats) {
+// max_iterations rounds from the current centres.  solver_its: BiCGSTAB
+// iterations per round (the reference's 100).
+static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool from_centre, int solver_its,
+                                     ep_qp_stats *stats) {
     if (e->in_run) {
         e->err = "ep_quadratic_placement cannot run inside an optimizer run";
         return EP_ERR_STATE;
@@ -1950,7 +1952,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
     for (int i = 0;; i++) {
         if ((s = qp_build(e, qpos))) return s;
         int it = 0;
-        if ((s = qp_solve(e, qpos, 100, err, it))) return s;  // solver.setMaxIterations(100)
+        if ((s = qp_solve(e, qpos, solver_its, err, it))) return s;  // solver.setMaxIterations(100)
         solver_iters += it;
         qp_from_x(q, e->grid, e->size, qpos, st);  // updateModuleLocation
         qp_bounds(q, qpos, q.out, st);             // calcNetBoundPins
@@ -1984,16 +1986,16 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
 ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
     if (!e) return EP_ERR_ARG;
     try {
-        return quadratic_placement(e, max_iterations, true, stats);
+        return quadratic_placement(e, max_iterations, true, 100, stats);
     } catch (const std::bad_alloc &) {
         return host_oom(e);
     }
 }
 
-ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, ep_qp_stats *stats) {
-    if (!e || rounds < 1) return EP_ERR_ARG;
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, ep_qp_stats *stats) {
+    if (!e || rounds < 1 || solver_iterations < 0) return EP_ERR_ARG;
     try {
-        return quadratic_placement(e, rounds, false, stats);
+        return quadratic_placement(e, rounds, false, solver_iterations > 0 ? solver_iterations : 100, stats);
     } catch (const std::bad_alloc &) {
         return host_oom(e);
     }

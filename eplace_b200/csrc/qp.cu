@@ -177,12 +177,30 @@ struct QpMat {
     const float2 *diag;
 };
 
-// (A_x v.x, A_y v.y) for row i.
-__device__ __forceinline__ float2 spmv_row(const QpMat &m, const float2 *__restrict__ v, int i) {
-    const float2 d = m.diag[i], vi = v[i];
-    float ax = d.x * vi.x, ay = d.y * vi.y;
-    for (int e = m.row_x[i]; e < m.row_x[i + 1]; e++) ax = fmaf(m.val_x[e], v[m.col_x[e]].x, ax);
-    for (int e = m.row_y[i]; e < m.row_y[i + 1]; e++) ay = fmaf(m.val_y[e], v[m.col_y[e]].y, ay);
+// (A_x v.x, A_y v.y) for row i, computed by the 8 lanes of an aligned lane
+// group (sub = lane index in the group): lane k sums entries k, k + 8, ...
+// of the row in order, a fixed xor tree adds the 8 partial sums, and the
+// diagonal term comes last, so the result is the same on every run.  Rows
+// of bound pins of large nets hold hundreds of entries; eight lanes per row
+// keep those from holding up a warp.  Every lane of the warp must call it
+// (valid = false for lanes past the last row); all 8 lanes get the result.
+constexpr int kRowLanes = 8;
+__device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__restrict__ v, int i, int sub, bool valid) {
+    float ax = 0.f, ay = 0.f;
+    if (valid) {
+        for (int e = m.row_x[i] + sub; e < m.row_x[i + 1]; e += kRowLanes) ax = fmaf(m.val_x[e], v[m.col_x[e]].x, ax);
+        for (int e = m.row_y[i] + sub; e < m.row_y[i + 1]; e += kRowLanes) ay = fmaf(m.val_y[e], v[m.col_y[e]].y, ay);
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    if (valid) {
+        const float2 d = m.diag[i], vi = v[i];
+        ax = fmaf(d.x, vi.x, ax);
+        ay = fmaf(d.y, vi.y, ay);
+    }
     return make_float2(ax, ay);
 }
 
@@ -214,10 +232,11 @@ k_qp_init(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restr
           float2 *__restrict__ r0, float2 *__restrict__ p, float2 *__restrict__ v, double *__restrict__ partials,
           unsigned *__restrict__ cnt, int max_it, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < nn) {
-        const float2 ax = spmv_row(m, x, i), bi = rhs[i];
+    const float2 ax = spmv_row8(m, x, i, sub, i < nn);
+    if (i < nn && sub == 0) {
+        const float2 bi = rhs[i];
         const float2 ri = make_float2(bi.x - ax.x, bi.y - ax.y);
         r[i] = ri;
         r0[i] = ri;
@@ -283,10 +302,11 @@ k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__re
     __shared__ double sh[2 * 32];
     const int mask = S->restart_mask;
     if (!mask || !any_active(S)) return;  // uniform over the grid
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[2] = {0.0, 0.0};
-    if (i < nn) {
-        const float2 ax = spmv_row(m, x, i), bi = rhs[i];
+    const float2 ax = spmv_row8(m, x, i, sub, i < nn);
+    if (i < nn && sub == 0) {
+        const float2 bi = rhs[i];
         float2 ri = r[i], zi = r0[i];
         if (mask & 1) ri.x = zi.x = bi.x - ax.x;
         if (mask & 2) ri.y = zi.y = bi.y - ax.y;
@@ -327,10 +347,11 @@ k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict_
         double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[2 * 32];
     if (!any_active(S)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[2] = {0.0, 0.0};
-    if (i < nn) {
-        const float2 vi = spmv_row(m, p, i), z = r0[i];
+    const float2 vi = spmv_row8(m, p, i, sub, i < nn);
+    if (i < nn && sub == 0) {
+        const float2 z = r0[i];
         v[i] = vi;
         acc[0] = (double)z.x * vi.x;
         acc[1] = (double)z.y * vi.y;
@@ -357,10 +378,11 @@ k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, d
         unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     if (!any_active(S)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < nn) {
-        const float2 ti = spmv_row(m, s, i), si = s[i];
+    const float2 ti = spmv_row8(m, s, i, sub, i < nn);
+    if (i < nn && sub == 0) {
+        const float2 si = s[i];
         t[i] = ti;
         acc[0] = (double)ti.x * ti.x;
         acc[1] = (double)ti.y * ti.y;
@@ -446,20 +468,20 @@ void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
 static QpMat mat(const QpDev &q) { return QpMat{q.row_x, q.col_x, q.row_y, q.col_y, q.val_x, q.val_y, q.diag}; }
 
 void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
-    k_qp_init<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials, q.cnt, max_it,
-                                             q.solve);
+    k_qp_init<<<qblocks(kRowLanes * q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials,
+                                                         q.cnt, max_it, q.solve);
     k_qp_zero<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.solve, q.x);
 }
 
 void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
-    const int b = qblocks(q.nn);
+    const int b = qblocks(q.nn), bm = qblocks(kRowLanes * q.nn);
     for (int k = 0; k < count; k++) {
         k_qp_pre<<<1, 32, 0, st>>>(q.solve);
-        k_qp_restart<<<b, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
+        k_qp_restart<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
         k_qp_dir<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.p, q.solve);
-        k_qp_av<<<b, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
+        k_qp_av<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
         k_qp_s<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.s, q.solve);
-        k_qp_at<<<b, kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
+        k_qp_at<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
         k_qp_step<<<b, kQT, 0, st>>>(q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
     }
 }
@@ -476,6 +498,6 @@ void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, c
     k_qp_center<<<qblocks(q.nn), kQT, 0, st>>>(g, q.nn, size, pos);
 }
 
-int qp_partial_blocks(int nn, int nnet) { return std::max(qblocks(nn), qblocks(nnet)); }
+int qp_partial_blocks(int nn, int nnet) { return std::max(qblocks(kRowLanes * nn), qblocks(nnet)); }
 
 }  // namespace ep

@@ -176,7 +176,7 @@ def load():
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
-    L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
+    L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_run_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(RunStats)]
     L.ep_netbin_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.c_float, ctypes.c_int32]
     L.ep_netbin_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_float),
@@ -535,10 +535,10 @@ class Engine:
         self._check(self._L.ep_quadratic_placement(self.h, int(max_iterations), ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
-    def quadratic_refine(self, rounds):
+    def quadratic_refine(self, rounds, solver_iterations=0):
         """ep_quadratic_refine: rounds of the quadratic model from the current centres."""
         st = QpStats()
-        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), ctypes.byref(st)))
+        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), int(solver_iterations), ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
     def switch_stage(self, stage, filler_ll=None):

@@ -13,11 +13,12 @@ that proposes the initial placement in place of the quadratic placement
     against the engine's quadratic placement and final mGP centres of each
     design (normalised to the core), one design per step in a seeded order;
   * the start: the network's proposal q + alpha (f - q), q and f the two
-    heads, then `rounds` rounds of the quadratic model from there
-    (ep_quadratic_refine; 0 = none).  (alpha, rounds) are picked on
-    validation designs (not the held-out ones): the fewest rounds, then the
-    largest alpha, whose runs end with a mean HPWL within 0.3% of the
-    QP-started runs, else the pair with the lowest mean HPWL;
+    heads, then `rounds` rounds of the quadratic model from there with at
+    most `iters` BiCGSTAB iterations each (ep_quadratic_refine; rounds 0 =
+    none).  (alpha, rounds, iters) are picked on validation designs (not the
+    held-out ones): the least solver work (rounds x iters), then the largest
+    alpha, whose runs end with a mean HPWL within 0.3% of the QP-started
+    runs, else the choice with the lowest mean HPWL;
   * evaluation: on held-out designs, the QP-started run against the
     proposal-started run (iterations and device seconds to overflow < 0.1,
     final HPWL), and the judge: a proposal is kept when its run reaches the
@@ -27,6 +28,7 @@ that proposes the initial placement in place of the quadratic placement
     use, diffusion features, forward pass, positions set; it synchronises).
 
     python -m eplace_b200.warmstart train --designs 256 --steps 6000 --out W.npz
+    python -m eplace_b200.warmstart pick --weights W.npz --out W2.npz   # re-pick the start only
     python -m eplace_b200.warmstart eval --weights W.npz --cells 200000 --seeds 100-119
 """
 import argparse
@@ -53,22 +55,24 @@ def training_sizes(count, seed, lo=2_000, hi=50_000):
 
 
 def load_weights(path=WEIGHTS):
-    """(weights, alpha, rounds) of a trained network."""
+    """(weights, start) of a trained network; start = dict(alpha, rounds, iters)."""
     z = np.load(path)
-    return z["weights"], float(z["alpha"]), int(z["rounds"])
+    iters = int(z["iters"]) if "iters" in z.files else 100
+    return z["weights"], dict(alpha=float(z["alpha"]), rounds=int(z["rounds"]), iters=iters)
 
 
-def save_weights(path, weights, alpha, rounds, meta):
-    np.savez(path, weights=np.asarray(weights, np.float32), alpha=np.float32(alpha), rounds=np.int32(rounds),
-             meta=np.array(json.dumps(meta)))
+def save_weights(path, weights, start, meta):
+    np.savez(path, weights=np.asarray(weights, np.float32), alpha=np.float32(start["alpha"]),
+             rounds=np.int32(start["rounds"]), iters=np.int32(start["iters"]), meta=np.array(json.dumps(meta)))
 
 
-def propose(gnn, engine, alpha, rounds):
-    """The learned start: the network's proposal, then `rounds` rounds of
-    the quadratic model from it."""
-    gnn.propose(engine, alpha)
-    if rounds > 0:
-        engine.quadratic_refine(rounds)
+def propose(gnn, engine, start):
+    """The learned start: the network's proposal, then start["rounds"]
+    rounds of the quadratic model from it (start["iters"] solver iterations
+    each)."""
+    gnn.propose(engine, start["alpha"])
+    if start["rounds"] > 0:
+        engine.quadratic_refine(start["rounds"], start["iters"])
 
 
 def log_pair(directory, name, nl, final_xy):
@@ -127,7 +131,7 @@ def run_from(engine, start):
     return st
 
 
-def compare(gnn, nl, alpha, rounds, precision=placer.PREC_MIXED, tolerance=0.005):
+def compare(gnn, nl, start, precision=placer.PREC_MIXED, tolerance=0.005):
     """The QP-started run against the proposal-started run on one design.
     Device seconds of each start (quadratic placement; graph build, features
     and forward pass of the network) and of each mGP run."""
@@ -141,7 +145,7 @@ def compare(gnn, nl, alpha, rounds, precision=placer.PREC_MIXED, tolerance=0.005
     e.load_positions()
     e.synchronize()
     t0 = time.perf_counter()
-    propose(gnn, e, alpha, rounds)
+    propose(gnn, e, start)
     e.synchronize()
     t_gnn = time.perf_counter() - t0
     r = run_from(e, "gnn")
@@ -155,12 +159,14 @@ def compare(gnn, nl, alpha, rounds, precision=placer.PREC_MIXED, tolerance=0.005
     return out
 
 
-def pick_start(gnn, netlists, alphas=(0.0, 0.25, 0.5), rounds=(0, 1, 2, 3, 5), within=0.003):
-    """On these (validation) netlists: the fewest refinement rounds, then the
-    largest alpha, whose runs end with a mean HPWL ratio to the QP-started
-    runs of at most 1 + within, else the pair with the lowest mean ratio.
-    Returns (alpha, rounds) and the table of mean ratios and iterations."""
-    keys = [(a, r) for r in rounds for a in alphas]
+def pick_start(gnn, netlists, alphas=(0.0, 0.5), refinements=((0, 0), (1, 20), (1, 40), (1, 100), (2, 40)),
+               within=0.003):
+    """On these (validation) netlists: the start (alpha, rounds, iters) with
+    the least solver work (rounds x iters), then the largest alpha, whose
+    runs end with a mean HPWL ratio to the QP-started runs of at most
+    1 + within, else the one with the lowest mean ratio.  Returns it and the
+    table of mean ratios and iterations."""
+    keys = [(a, r, it) for r, it in refinements for a in alphas]
     ratio = {k: [] for k in keys}
     iters = {k: [] for k in keys}
     for nl in netlists:
@@ -168,19 +174,20 @@ def pick_start(gnn, netlists, alphas=(0.0, 0.25, 0.5), rounds=(0, 1, 2, 3, 5), w
         e.save_positions()
         e.quadratic_placement()
         ref = run_from(e, "qp")["hpwl"]
-        for a, r in keys:
+        for a, r, it in keys:
             e.load_positions()
-            propose(gnn, e, a, r)
-            st = run_from(e, f"gnn{a}/{r}")
-            ratio[(a, r)].append(st["hpwl"] / ref)
-            iters[(a, r)].append(st["iterations"])
+            propose(gnn, e, dict(alpha=a, rounds=r, iters=it))
+            st = run_from(e, f"gnn{a}/{r}x{it}")
+            ratio[(a, r, it)].append(st["hpwl"] / ref)
+            iters[(a, r, it)].append(st["iterations"])
         gnn.release(e)
         e.close()
     mean = {k: float(np.mean(v)) for k, v in ratio.items()}
     ok = [k for k in keys if mean[k] <= 1.0 + within]
-    best = min(ok, key=lambda k: (k[1], -k[0])) if ok else min(mean, key=mean.get)
-    table = {f"{a}/{r}": dict(hpwl_ratio=mean[(a, r)], iterations=float(np.mean(iters[(a, r)]))) for a, r in keys}
-    return best, table
+    best = min(ok, key=lambda k: (k[1] * k[2], -k[0])) if ok else min(mean, key=mean.get)
+    table = {f"{a}/{r}x{it}": dict(hpwl_ratio=mean[(a, r, it)], iterations=float(np.mean(iters[(a, r, it)])))
+             for a, r, it in keys}
+    return dict(alpha=best[0], rounds=best[1], iters=best[2]), table
 
 
 def _seeds(spec):
@@ -199,13 +206,27 @@ def main():
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--pairs", default="")
     t.add_argument("--out", required=True)
+    pk = sub.add_parser("pick")
+    pk.add_argument("--weights", default=WEIGHTS)
+    pk.add_argument("--valid", type=int, default=6)
+    pk.add_argument("--seed", type=int, default=1)
+    pk.add_argument("--out", required=True)
     ev = sub.add_parser("eval")
     ev.add_argument("--weights", default=WEIGHTS)
     ev.add_argument("--cells", type=int, default=200_000)
     ev.add_argument("--seeds", default="100-119")
     ev.add_argument("--out", default="")
     a = ap.parse_args()
-    if a.cmd == "train":
+    if a.cmd in ("train", "pick"):
+        valid = [design(n, 900_000 + i) for i, n in enumerate(training_sizes(a.valid, a.seed + 7, 40_000, 120_000))]
+    if a.cmd == "pick":
+        w, _ = load_weights(a.weights)
+        meta = json.loads(str(np.load(a.weights)["meta"]))
+        gnn = placer.Gnn(weights=w)
+        start, meta["start_table"] = pick_start(gnn, valid)
+        save_weights(a.out, w, start, meta)
+        print(json.dumps(dict(start=start, start_table=meta["start_table"])))
+    elif a.cmd == "train":
         t0 = time.time()
         sizes = training_sizes(a.designs, a.seed)
         nls = [design(n, 1000 + a.seed * 10_000 + i) for i, n in enumerate(sizes)]
@@ -220,19 +241,18 @@ def main():
         for e in engines:
             gnn.release(e)
             e.close()
-        valid = [design(n, 900_000 + i) for i, n in enumerate(training_sizes(a.valid, a.seed + 7, 40_000, 120_000))]
-        (alpha, rounds), table = pick_start(gnn, valid)
+        start, table = pick_start(gnn, valid)
         meta = dict(designs=a.designs, steps=a.steps, lr=a.lr, seed=a.seed, final_loss=float(np.mean(losses[-100:])),
                     first_loss=float(np.mean(losses[:50])), start_table=table, generate_s=t_gen, place_s=t_place,
                     iterations=[int(s["iterations"]) for s in stats])
-        save_weights(a.out, gnn.get_weights(), alpha, rounds, meta)
-        print(json.dumps(dict(alpha=alpha, rounds=rounds, **meta)))
+        save_weights(a.out, gnn.get_weights(), start, meta)
+        print(json.dumps(dict(start=start, **meta)))
     else:
-        w, alpha, rounds = load_weights(a.weights)
+        w, start = load_weights(a.weights)
         gnn = placer.Gnn(weights=w)
         rows = []
         for s in _seeds(a.seeds):
-            r = compare(gnn, design(a.cells, s), alpha, rounds)
+            r = compare(gnn, design(a.cells, s), start)
             r["seed"] = s
             rows.append(r)
             print(json.dumps({k: r[k] for k in ("seed", "hpwl_ratio", "kept")} |
@@ -240,7 +260,7 @@ def main():
                               for f in ("iterations", "seconds", "start_seconds", "hpwl")}), flush=True)
         if a.out:
             with open(a.out, "w") as f:
-                json.dump(dict(alpha=alpha, rounds=rounds, rows=rows), f, indent=1)
+                json.dump(dict(start=start, rows=rows), f, indent=1)
 
 
 if __name__ == "__main__":

@@ -271,10 +271,11 @@ ep_status ep_switch_stage(ep_engine *e, int32_t stage, const float *filler_xy);
  * Fillers are not moved.  ep_initialize must run again afterwards. */
 ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats);
 /* `rounds` rounds of the same quadratic model starting from the current
- * centres instead of the core centre (no convergence test): a short
- * refinement of a start from elsewhere, e.g. ep_gnn_propose.  No
+ * centres instead of the core centre (no convergence test), each with at
+ * most solver_iterations BiCGSTAB iterations (0 = the reference's 100): a
+ * short refinement of a start from elsewhere, e.g. ep_gnn_propose.  No
  * counterpart in the reference. */
-ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, ep_qp_stats *stats);
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, ep_qp_stats *stats);
 
 /* FirstOrderOptimizer::opt (Optimization/opt.hpp:30-36) with
  * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:

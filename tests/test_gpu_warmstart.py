@@ -21,11 +21,11 @@ pytestmark = pytest.mark.gpu
 SEEDS = (5001, 5002, 5003)
 
 
-def _learned_run(gnn, nl, alpha, rounds):
+def _learned_run(gnn, nl, start):
     e = placer.Engine(nl, placer.default_params(target_density=1.0))
     e.synchronize()
     t0 = time.perf_counter()
-    warmstart.propose(gnn, e, alpha, rounds)
+    warmstart.propose(gnn, e, start)
     e.synchronize()
     t_start = time.perf_counter() - t0
     e.initialize()
@@ -49,16 +49,17 @@ def _qp_run(nl):
 
 
 def test_trained_start_against_qp_and_an_untrained_network():
-    w, alpha, rounds = warmstart.load_weights()
+    w, start = warmstart.load_weights()
+    bare = dict(start, rounds=0)
     trained = placer.Gnn(weights=w)
     untrained = placer.Gnn(seed=123)
     ratios, ratios_untrained, t_learned, t_qp = [], [], [], []
     for s in SEEDS:
         nl = warmstart.design(60_000, s)
         tq, q = _qp_run(nl)
-        tl, l = _learned_run(trained, nl, alpha, rounds)
-        _, u = _learned_run(untrained, nl, alpha, 0)
-        _, l0 = _learned_run(trained, nl, alpha, 0)
+        tl, l = _learned_run(trained, nl, start)
+        _, u = _learned_run(untrained, nl, bare)
+        _, l0 = _learned_run(trained, nl, bare)
         assert l["overflow"] < 0.1
         ratios.append(l["hpwl"] / q["hpwl"])
         ratios_untrained.append((l0["hpwl"] / q["hpwl"], u["hpwl"] / q["hpwl"]))
