@@ -378,11 +378,11 @@ def main():
                                                    "pin_owner", "pin_dx", "pin_dy", "row_llx", "row_lly",
                                                    "row_urx", "row_h"))
 
-    def e2e(precision, start):
+    def e2e(precision, how):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e = placer.Engine(nl, placer.default_params(target_density=1.0, precision=precision, device=local))
-        if start == "gnn":
+        if how == "gnn":
             warmstart.propose(gnn, e, start)
         else:
             e.quadratic_placement()
@@ -391,7 +391,7 @@ def main():
         n = e.info.num_objects
         e.get_positions_ptr(host_out.data_ptr(), n)
         t1 = time.perf_counter()
-        if start == "gnn":
+        if how == "gnn":
             gnn.release(e)
         e.close()
         return (t1 - t0) * 1e3, st, n

@@ -311,7 +311,9 @@ __device__ __forceinline__ bool last_block(unsigned int *cnt, unsigned int total
 // Deterministic grid-wide sum of NV doubles.  Every block writes its block
 // total to partials[k * total + block_id]; the block that arrives last sums
 // the partials in a fixed order (thread-strided, then a fixed tree), so the
-// result does not depend on block scheduling.  Must be called by all threads
+// result does not depend on block scheduling.  The finalising block loads
+// the NV partials of four blocks before it adds any of them (the additions
+// keep the block order), so its L2 round trips overlap.  Must be called by all threads
 // of every participating block.  Returns true in all threads of the last
 // block; its thread 0 then holds the totals in v.
 // Arrival count with acquire-release semantics at GPU scope: the partials this
@@ -341,11 +343,23 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *sh, double *pa
     __threadfence_block();
     double s[NV];
 #pragma unroll
-    for (int k = 0; k < NV; k++) {
-        s[k] = 0.0;
-        for (unsigned int i = threadIdx.x; i < total; i += blockDim.x)
-            s[k] += __ldcg(&partials[(size_t)k * total + i]);
+    for (int k = 0; k < NV; k++) s[k] = 0.0;
+    constexpr int U = 4;
+    unsigned int i = threadIdx.x;
+    for (; i + (U - 1) * blockDim.x < total; i += U * blockDim.x) {
+        double t[U][NV];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int k = 0; k < NV; k++) t[u][k] = __ldcg(&partials[(size_t)k * total + i + u * blockDim.x]);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int k = 0; k < NV; k++) s[k] += t[u][k];
     }
+    for (; i < total; i += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; k++) s[k] += __ldcg(&partials[(size_t)k * total + i]);
     block_sum<NV>(s, sh);
     if (threadIdx.x == 0) {
         *cnt = 0;

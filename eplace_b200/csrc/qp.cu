@@ -37,6 +37,11 @@ constexpr int kQT = 256;
 constexpr float kMinDistance = 25.0f;  // MIN_DISTANCE, QPlace/qplace.h
 
 inline int qblocks(int n) { return (n + kQT - 1) / kQT; }
+// Kernels that end in a grid reduction run on at most 8 blocks per SM and
+// loop over their rows, so the finalising block adds few partials; the grid
+// depends only on the sizes, so the sums are the same on every run.
+constexpr int kQpMaxBlocks = 148 * 8;
+inline int qgrid(int n) { return std::min(qblocks(n), kQpMaxBlocks); }
 
 __device__ __forceinline__ float2 abs_pin(const float2 *__restrict__ pos, const float2 *__restrict__ off,
                                           int owner, int q) {
@@ -52,9 +57,8 @@ k_qp_bounds(int nnet, const int32_t *__restrict__ first, const int32_t *__restri
             const float2 *__restrict__ pos, int4 *__restrict__ bound, double *__restrict__ partials,
             unsigned *__restrict__ cnt, double *__restrict__ hpwl) {
     __shared__ double sh[32];
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[1] = {0.0};
-    if (n < nnet) {
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nnet; n += gridDim.x * blockDim.x) {
         const int f = first[n], d = deg[n];
         double mnx = 1.79769e308, mxx = -1.79769e308, mny = 1.79769e308, mxy = -1.79769e308;
         int4 b = make_int4(0, 0, 0, 0);
@@ -66,7 +70,7 @@ k_qp_bounds(int nnet, const int32_t *__restrict__ first, const int32_t *__restri
             if ((double)a.y > mxy) { mxy = a.y; b.w = k; }
         }
         bound[n] = b;
-        if (d > 0) acc[0] = (mxx - mnx) + (mxy - mny);
+        if (d > 0) acc[0] += (mxx - mnx) + (mxy - mny);
     }
     if (grid_sum<1>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) *hpwl = acc[0];
 }
@@ -184,7 +188,7 @@ struct QpMat {
 // of bound pins of large nets hold hundreds of entries; eight lanes per row
 // keep those from holding up a warp.  Every lane of the warp must call it
 // (valid = false for lanes past the last row); all 8 lanes get the result.
-constexpr int kRowLanes = 8;
+constexpr int kRowLanes = 8, kRowsPerWarp = 32 / kRowLanes;
 __device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__restrict__ v, int i, int sub, bool valid) {
     float ax = 0.f, ay = 0.f;
     if (valid) {
@@ -203,6 +207,17 @@ __device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__rest
     }
     return make_float2(ax, ay);
 }
+
+// Grid-stride loop over the rows of a matrix kernel, kRowsPerWarp rows per
+// warp and pass; the loop bound is uniform over a warp (spmv_row8 shuffles),
+// and row i, lane sub of its group, are declared for the body.
+__device__ __forceinline__ int row_group_first() {
+    return ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kRowsPerWarp;
+}
+__device__ __forceinline__ int row_group_stride() { return ((gridDim.x * blockDim.x) >> 5) * kRowsPerWarp; }
+#define ROW_GROUPS(nn)                                                                                        \
+    for (int base_ = row_group_first(), sub = threadIdx.x % kRowLanes, i = base_ + (threadIdx.x & 31) / kRowLanes; \
+         base_ < (nn); base_ += row_group_stride(), i = base_ + (threadIdx.x & 31) / kRowLanes)
 
 // ---- BiCGSTAB on the device -----------------------------------------------------
 // Eigen's BiCGSTAB (van der Vorst's method, restart when r0.r vanishes,
@@ -232,20 +247,21 @@ k_qp_init(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restr
           float2 *__restrict__ r0, float2 *__restrict__ p, float2 *__restrict__ v, double *__restrict__ partials,
           unsigned *__restrict__ cnt, int max_it, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const float2 ax = spmv_row8(m, x, i, sub, i < nn);
-    if (i < nn && sub == 0) {
-        const float2 bi = rhs[i];
-        const float2 ri = make_float2(bi.x - ax.x, bi.y - ax.y);
-        r[i] = ri;
-        r0[i] = ri;
-        p[i] = make_float2(0.f, 0.f);
-        v[i] = make_float2(0.f, 0.f);
-        acc[0] = (double)ri.x * ri.x;
-        acc[1] = (double)ri.y * ri.y;
-        acc[2] = (double)bi.x * bi.x;
-        acc[3] = (double)bi.y * bi.y;
+    ROW_GROUPS(nn) {
+        const float2 ax = spmv_row8(m, x, i, sub, i < nn);
+        if (i < nn && sub == 0) {
+            const float2 bi = rhs[i];
+            const float2 ri = make_float2(bi.x - ax.x, bi.y - ax.y);
+            r[i] = ri;
+            r0[i] = ri;
+            p[i] = make_float2(0.f, 0.f);
+            v[i] = make_float2(0.f, 0.f);
+            acc[0] += (double)ri.x * ri.x;
+            acc[1] += (double)ri.y * ri.y;
+            acc[2] += (double)bi.x * bi.x;
+            acc[3] += (double)bi.y * bi.y;
+        }
     }
     if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
         const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
@@ -302,18 +318,19 @@ k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__re
     __shared__ double sh[2 * 32];
     const int mask = S->restart_mask;
     if (!mask || !any_active(S)) return;  // uniform over the grid
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[2] = {0.0, 0.0};
-    const float2 ax = spmv_row8(m, x, i, sub, i < nn);
-    if (i < nn && sub == 0) {
-        const float2 bi = rhs[i];
-        float2 ri = r[i], zi = r0[i];
-        if (mask & 1) ri.x = zi.x = bi.x - ax.x;
-        if (mask & 2) ri.y = zi.y = bi.y - ax.y;
-        r[i] = ri;
-        r0[i] = zi;
-        acc[0] = (double)ri.x * ri.x;
-        acc[1] = (double)ri.y * ri.y;
+    ROW_GROUPS(nn) {
+        const float2 ax = spmv_row8(m, x, i, sub, i < nn);
+        if (i < nn && sub == 0) {
+            const float2 bi = rhs[i];
+            float2 ri = r[i], zi = r0[i];
+            if (mask & 1) ri.x = zi.x = bi.x - ax.x;
+            if (mask & 2) ri.y = zi.y = bi.y - ax.y;
+            r[i] = ri;
+            r0[i] = zi;
+            acc[0] += (double)ri.x * ri.x;
+            acc[1] += (double)ri.y * ri.y;
+        }
     }
     if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
         for (int c = 0; c < 2; c++)
@@ -347,14 +364,15 @@ k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict_
         double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[2 * 32];
     if (!any_active(S)) return;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[2] = {0.0, 0.0};
-    const float2 vi = spmv_row8(m, p, i, sub, i < nn);
-    if (i < nn && sub == 0) {
-        const float2 z = r0[i];
-        v[i] = vi;
-        acc[0] = (double)z.x * vi.x;
-        acc[1] = (double)z.y * vi.y;
+    ROW_GROUPS(nn) {
+        const float2 vi = spmv_row8(m, p, i, sub, i < nn);
+        if (i < nn && sub == 0) {
+            const float2 z = r0[i];
+            v[i] = vi;
+            acc[0] += (double)z.x * vi.x;
+            acc[1] += (double)z.y * vi.y;
+        }
     }
     if (grid_sum<2>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0)
         for (int c = 0; c < 2; c++) S->alpha[c] = S->active[c] ? S->rho[c] / acc[c] : 0.0;
@@ -378,16 +396,17 @@ k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, d
         unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     if (!any_active(S)) return;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, i = tid / kRowLanes, sub = tid % kRowLanes;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const float2 ti = spmv_row8(m, s, i, sub, i < nn);
-    if (i < nn && sub == 0) {
-        const float2 si = s[i];
-        t[i] = ti;
-        acc[0] = (double)ti.x * ti.x;
-        acc[1] = (double)ti.y * ti.y;
-        acc[2] = (double)ti.x * si.x;
-        acc[3] = (double)ti.y * si.y;
+    ROW_GROUPS(nn) {
+        const float2 ti = spmv_row8(m, s, i, sub, i < nn);
+        if (i < nn && sub == 0) {
+            const float2 si = s[i];
+            t[i] = ti;
+            acc[0] += (double)ti.x * ti.x;
+            acc[1] += (double)ti.y * ti.y;
+            acc[2] += (double)ti.x * si.x;
+            acc[3] += (double)ti.y * si.y;
+        }
     }
     if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0)
         for (int c = 0; c < 2; c++)
@@ -401,22 +420,21 @@ k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, co
           unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     if (!any_active(S)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float a[2], w[2];
     for (int c = 0; c < 2; c++) {
         a[c] = S->active[c] ? (float)S->alpha[c] : 0.f;
         w[c] = S->active[c] ? (float)S->w[c] : 0.f;
     }
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < nn) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
         const float2 pi = p[i], si = s[i], ti = t[i], xi = x[i], z = r0[i];
         x[i] = make_float2(xi.x + a[0] * pi.x + w[0] * si.x, xi.y + a[1] * pi.y + w[1] * si.y);
         const float2 ri = make_float2(si.x - w[0] * ti.x, si.y - w[1] * ti.y);
         r[i] = ri;
-        acc[0] = (double)ri.x * ri.x;
-        acc[1] = (double)ri.y * ri.y;
-        acc[2] = (double)z.x * ri.x;
-        acc[3] = (double)z.y * ri.y;
+        acc[0] += (double)ri.x * ri.x;
+        acc[1] += (double)ri.y * ri.y;
+        acc[2] += (double)z.x * ri.x;
+        acc[3] += (double)z.y * ri.y;
     }
     if (grid_sum<4>(acc, sh, partials, cnt, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
         S->iters++;
@@ -455,7 +473,7 @@ __global__ void k_qp_center(Grid g, int nn, const float2 *__restrict__ size, flo
 }  // namespace
 
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st) {
-    k_qp_bounds<<<qblocks(q.nnet), kQT, 0, st>>>(q.nnet, q.net_first, q.net_deg, q.owner, q.off, pos, q.bound,
+    k_qp_bounds<<<qgrid(q.nnet), kQT, 0, st>>>(q.nnet, q.net_first, q.net_deg, q.owner, q.off, pos, q.bound,
                                                  q.partials, q.cnt, hpwl);
 }
 
@@ -468,13 +486,13 @@ void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
 static QpMat mat(const QpDev &q) { return QpMat{q.row_x, q.col_x, q.row_y, q.col_y, q.val_x, q.val_y, q.diag}; }
 
 void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
-    k_qp_init<<<qblocks(kRowLanes * q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials,
+    k_qp_init<<<qgrid(kRowLanes * q.nn), kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.p, q.v, q.partials,
                                                          q.cnt, max_it, q.solve);
     k_qp_zero<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.solve, q.x);
 }
 
 void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
-    const int b = qblocks(q.nn), bm = qblocks(kRowLanes * q.nn);
+    const int b = qblocks(q.nn), bm = qgrid(kRowLanes * q.nn), br = qgrid(q.nn);
     for (int k = 0; k < count; k++) {
         k_qp_pre<<<1, 32, 0, st>>>(q.solve);
         k_qp_restart<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
@@ -482,7 +500,7 @@ void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
         k_qp_av<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
         k_qp_s<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.s, q.solve);
         k_qp_at<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
-        k_qp_step<<<b, kQT, 0, st>>>(q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
+        k_qp_step<<<br, kQT, 0, st>>>(q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
     }
 }
 
@@ -498,6 +516,6 @@ void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, c
     k_qp_center<<<qblocks(q.nn), kQT, 0, st>>>(g, q.nn, size, pos);
 }
 
-int qp_partial_blocks(int nn, int nnet) { return std::max(qblocks(kRowLanes * nn), qblocks(nnet)); }
+int qp_partial_blocks(int nn, int nnet) { return std::max(qgrid(kRowLanes * nn), qgrid(nnet)); }
 
 }  // namespace ep

@@ -17,7 +17,7 @@ that proposes the initial placement in place of the quadratic placement
     most `iters` BiCGSTAB iterations each (ep_quadratic_refine; rounds 0 =
     none).  (alpha, rounds, iters) are picked on validation designs (not the
     held-out ones): the least solver work (rounds x iters), then the largest
-    alpha, whose runs end with a mean HPWL within 0.3% of the QP-started
+    alpha, whose runs end with a mean HPWL within 0.15% of the QP-started
     runs, else the choice with the lowest mean HPWL;
   * evaluation: on held-out designs, the QP-started run against the
     proposal-started run (iterations and device seconds to overflow < 0.1,
@@ -160,7 +160,7 @@ def compare(gnn, nl, start, precision=placer.PREC_MIXED, tolerance=0.005):
 
 
 def pick_start(gnn, netlists, alphas=(0.0, 0.5), refinements=((0, 0), (1, 20), (1, 40), (1, 100), (2, 40)),
-               within=0.003):
+               within=0.0015):
     """On these (validation) netlists: the start (alpha, rounds, iters) with
     the least solver work (rounds x iters), then the largest alpha, whose
     runs end with a mean HPWL ratio to the QP-started runs of at most
