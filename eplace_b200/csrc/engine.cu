@@ -101,6 +101,7 @@ struct ep_engine {
     // creation; the quadratic placement and the learned warm start read them)
     int32_t *net_first = nullptr, *net_deg = nullptr, *pin_net = nullptr;
     int32_t *net_dev_order = nullptr;  // nets in device pin order (grouped by degree)
+    int n_big_nets = 0;                // nets above kWarpPins pins (the head of that order)
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
@@ -822,6 +823,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
             q += deg;
             return at;
         };
+        e->n_big_nets = (int)big_list.size();
         for (int n : big_list) {
             int at = put_net(n);
             net_tasks.push_back(make_int4(net_start[n + 1] - net_start[n], at, 1, 0));
@@ -911,6 +913,8 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         order.reserve(nnet);
         for (int p = 0; p < np; p++)
             if (p == 0 || e->h_pin_net[p] != e->h_pin_net[p - 1]) order.push_back(e->h_pin_net[p]);
+        for (int n = 0; n < nnet; n++)  // nets without pins last, so the order holds every net
+            if (e->h_net_deg[n] == 0) order.push_back(n);
         if ((s = dupload(e, e->net_first, e->h_net_first)) || (s = dupload(e, e->net_deg, e->h_net_deg)) ||
             (s = dupload(e, e->pin_net, e->h_pin_net)) || (s = dupload(e, e->net_dev_order, order)))
             return s;
@@ -1847,6 +1851,8 @@ ep_status qp_setup(ep_engine *e) {
     q.pin_net = e->pin_net;
     q.net_first = e->net_first;
     q.net_deg = e->net_deg;
+    q.net_order = e->net_dev_order;
+    q.n_big = e->n_big_nets;
     CK(cudaMemset(q.cnt, 0, sizeof(unsigned)));
     CK(cudaMallocHost((void **)&e->qp_out_h, 4 * sizeof(double)));
     CK(cudaMallocHost((void **)&e->qp_state_h, sizeof(QpSolve)));
@@ -2023,6 +2029,7 @@ int engine_graph(ep_engine *e, EngineGraph *g) {
     g->d_net_deg = e->net_deg;
     g->d_pin_net = e->pin_net;
     g->d_net_dev_order = e->net_dev_order;
+    g->n_big_nets = e->n_big_nets;
     g->d_obj_pin_start = e->obj_pin_start;
     g->d_obj_pin_dev = e->obj_pin_dev;
     g->d_area = e->area;

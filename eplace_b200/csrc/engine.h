@@ -186,6 +186,7 @@ struct EngineGraph {
     // the same netlist on the device
     const int32_t *d_pin_owner, *d_net_first, *d_net_deg, *d_pin_net;
     const int32_t *d_net_dev_order;  // [nnet] nets in device pin order (grouped by degree)
+    int n_big_nets;                  // nets above kWarpPins pins: the first n_big_nets of that order
     const int32_t *d_obj_pin_start, *d_obj_pin_dev;  // object -> its device pins
     const float *d_area, *d_npins;                   // [n_obj]
     const void *d_pos;                               // [n_obj + nt] centres, vec2<R>
@@ -214,6 +215,8 @@ struct QpDev {
     const int32_t *obj_pin_start, *obj_pin_dev;  // movable node -> its pins (modulePins order)
     const int32_t *pin_net;                      // device pin -> net
     const int32_t *net_first, *net_deg;          // net -> first device pin, pins
+    const int32_t *net_order;                    // nets in device pin order
+    int n_big;                                   // nets above kWarpPins pins (the head of net_order)
     const int32_t *owner;
     const float2 *off;
     int4 *bound;                                 // per net: x-min, x-max, y-min, y-max pin (in net)

@@ -71,6 +71,7 @@ struct Net {
     int nn, n_obj, N, nnet;
     const int32_t *owner, *net_first, *net_deg, *pin_net, *obj_pin_start, *obj_pin_dev;
     const int32_t *net_order;            // nets in device pin order (neighbouring nets of equal degree)
+    int n_big;                           // nets above kWarpPins pins: the head of net_order
     const int32_t *pad_start, *pad_net;  // terminals' pins (training only; may be null)
 };
 
@@ -116,14 +117,34 @@ __global__ void k_inv_deg(int nnet, const int32_t *__restrict__ deg, float *__re
     if (n < nnet) inv[n] = deg[n] > 0 ? 1.f / deg[n] : 0.f;
 }
 
-// thread k takes the k-th net in device pin order, so a warp's nets have
-// (nearly) the same degree
+// The nets above kWarpPins pins (the head of the device order) take a warp
+// each: lane l sums pins l, l + 32, ... and a fixed xor tree adds the lanes.
+// Every other net takes a thread, in device order, so a warp's nets have the
+// same degree.  Launched with 32 n_big + (nnet - n_big) threads.
 __global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ v,
                            float2 *__restrict__ a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, big = g.n_big * 32;
+    if (t < big) {  // whole warps
+        const int n = g.net_order[t >> 5], lane = t & 31;
+        float sx = 0.f, sy = 0.f;
+        for (int p = g.net_first[n] + lane, e = g.net_first[n] + g.net_deg[n]; p < e; p += 32) {
+            const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
+            sx += q.x;
+            sy += q.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane == 0) a[n] = make_float2(sx * inv_deg[n], sy * inv_deg[n]);
+        return;
+    }
+    const int k = g.n_big + (t - big);
     if (k >= g.nnet) return;
     const int n = g.net_order[k];
     float sx = 0.f, sy = 0.f;
+#pragma unroll 4
     for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
         const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
         sx += q.x;
@@ -155,12 +176,40 @@ __global__ void k_store_feature(int N, const float2 *__restrict__ v, float *__re
 }
 
 // ------------------------------------------------------ aggregations ------
-// One warp per row, a float2 of channels per lane.
-__global__ void k_net_mean(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ h,
-                           float2 *__restrict__ a) {
-    const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (n >= g.nnet) return;
+// One warp per row, a float2 of channels per lane.  k_net_mean: the first
+// n_big blocks take the nets above kWarpPins pins, a block each (warp w sums
+// pins w, w + 8, ..., the 8 warp sums are added in warp order); the other
+// nets take a warp each.
+constexpr int kBigWarps = kT / 32;
+__global__ void __launch_bounds__(kT) k_net_mean(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ h,
+                                                 float2 *__restrict__ a) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if ((int)blockIdx.x < g.n_big) {
+        __shared__ float2 part[kBigWarps][32];
+        const int n = g.net_order[blockIdx.x];
+        float2 s = make_float2(0.f, 0.f);
+        for (int p = g.net_first[n] + w, e = g.net_first[n] + g.net_deg[n]; p < e; p += kBigWarps) {
+            const float2 q = h[(size_t)node_of(g.owner[p], g.nn, g.n_obj) * 32 + lane];
+            s.x += q.x;
+            s.y += q.y;
+        }
+        part[w][lane] = s;
+        __syncthreads();
+        if (w == 0) {
+            float2 t = part[0][lane];
+            for (int k = 1; k < kBigWarps; k++) {
+                t.x += part[k][lane].x;
+                t.y += part[k][lane].y;
+            }
+            a[(size_t)n * 32 + lane] = make_float2(t.x * inv_deg[n], t.y * inv_deg[n]);
+        }
+        return;
+    }
+    const int k = g.n_big + ((int)(blockIdx.x - g.n_big) * kBigWarps + w);
+    if (k >= g.nnet) return;
+    const int n = g.net_order[k];
     float2 s = make_float2(0.f, 0.f);
+#pragma unroll 4
     for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
         const float2 q = h[(size_t)node_of(g.owner[p], g.nn, g.n_obj) * 32 + lane];
         s.x += q.x;
@@ -231,41 +280,60 @@ __global__ void k_net_mean_t_add(Net g, const float *__restrict__ inv_deg, const
 
 // ------------------------------------------------------------ dense -------
 // Y[r][o] = relu(b[o] + sum_k X[r][k] W[o][k]) with X = [XA (KA cols) | XB
-// (KB cols)], W BF16 [kH][KA+KB].  64 rows per 256-thread block, W
-// (transposed) and the rows staged in shared memory; a thread owns one row,
-// 16 outputs.
+// (KB cols)], W BF16 [kH][KA+KB].  kDenseRows rows per 256-thread block: W
+// (as float, rows padded to K + 1) and the block's rows (transposed, padded
+// to kDenseRows + 1) staged in shared memory, both without bank conflicts;
+// thread (tx, ty) accumulates rows ty + 32 j (j < 4) x outputs 8 tx .. 8 tx +
+// 7 in registers, k in order, so each output is the same sum as a plain
+// loop over k.
+constexpr int kDenseRows = 128;
 template <int KA, int KB>
 __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ XA, const float *__restrict__ XB,
                                               const __nv_bfloat16 *__restrict__ W, const float *__restrict__ b,
                                               float *__restrict__ Y) {
-    constexpr int K = KA + KB, KP = K + 1;
+    constexpr int K = KA + KB, WP = K + 1, XP = kDenseRows + 1;
     extern __shared__ float sm[];
-    float *Wt = sm;           // [K][kH]
-    float *Xs = sm + K * kH;  // [64][KP]
-    for (int i = threadIdx.x; i < kH * K; i += kT) Wt[(i % K) * kH + i / K] = bf(W[i]);
-    const int r0 = blockIdx.x * 64;
-    for (int i = threadIdx.x; i < 64 * K; i += kT) {
+    float *Ws = sm;           // [kH][WP]
+    float *Xt = sm + kH * WP;  // [K][XP]
+    for (int i = threadIdx.x; i < kH * K; i += kT) {
+        const int o = i / K, k = i - o * K;
+        Ws[o * WP + k] = bf(W[i]);
+    }
+    const int r0 = blockIdx.x * kDenseRows;
+    for (int i = threadIdx.x; i < kDenseRows * K; i += kT) {
         const int r = i / K, k = i - r * K, row = r0 + r;
         float v = 0.f;
         if (row < N) v = k < KA ? XA[(size_t)row * KA + k] : XB[(size_t)row * KB + (k - KA)];
-        Xs[r * KP + k] = v;
+        Xt[k * XP + r] = v;
     }
     __syncthreads();
-    const int r = threadIdx.x >> 2, o0 = (threadIdx.x & 3) * 16;
-    float acc[16];
+    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    float acc[4][8];
 #pragma unroll
-    for (int j = 0; j < 16; j++) acc[j] = b[o0 + j];
-    for (int k = 0; k < K; k++) {
-        const float x = Xs[r * KP + k];
+    for (int j = 0; j < 8; j++) {
+        const float bj = b[tx * 8 + j];
 #pragma unroll
-        for (int j = 0; j < 16; j++) acc[j] = fmaf(x, Wt[k * kH + o0 + j], acc[j]);
+        for (int i = 0; i < 4; i++) acc[i][j] = bj;
     }
-    if (r0 + r < N) {
-        float4 *y = reinterpret_cast<float4 *>(Y + (size_t)(r0 + r) * kH + o0);
+#pragma unroll 4
+    for (int k = 0; k < K; k++) {
+        float x[4], w[8];
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            y[j] = make_float4(fmaxf(acc[4 * j], 0.f), fmaxf(acc[4 * j + 1], 0.f), fmaxf(acc[4 * j + 2], 0.f),
-                               fmaxf(acc[4 * j + 3], 0.f));
+        for (int i = 0; i < 4; i++) x[i] = Xt[k * XP + ty + 32 * i];
+#pragma unroll
+        for (int j = 0; j < 8; j++) w[j] = Ws[(tx * 8 + j) * WP + k];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[i][j] = fmaf(x[i], w[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int row = r0 + ty + 32 * i;
+        if (row >= N) continue;
+        float4 *y = reinterpret_cast<float4 *>(Y + (size_t)row * kH + tx * 8);
+        y[0] = make_float4(fmaxf(acc[i][0], 0.f), fmaxf(acc[i][1], 0.f), fmaxf(acc[i][2], 0.f), fmaxf(acc[i][3], 0.f));
+        y[1] = make_float4(fmaxf(acc[i][4], 0.f), fmaxf(acc[i][5], 0.f), fmaxf(acc[i][6], 0.f), fmaxf(acc[i][7], 0.f));
     }
 }
 
@@ -528,7 +596,7 @@ namespace {
         }                                                                         \
     } while (0)
 
-size_t smem_dense(int K) { return sizeof(float) * ((size_t)K * kH + 64 * (size_t)(K + 1)); }
+size_t smem_dense(int K) { return sizeof(float) * ((size_t)kH * (K + 1) + (size_t)K * (kDenseRows + 1)); }
 size_t smem_dx(int K) { return sizeof(float) * ((size_t)kH * K + 64 * (size_t)(kH + 1)); }
 
 void set_smem_attrs() {
@@ -619,6 +687,7 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     n.obj_pin_start = eg.d_obj_pin_start;
     n.obj_pin_dev = eg.d_obj_pin_dev;
     n.net_order = eg.d_net_dev_order;
+    n.n_big = eg.n_big_nets;
     n.pad_start = g->pad_start;
     n.pad_net = g->pad_net;
     cudaStream_t st = eg.st;
@@ -636,7 +705,7 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     k_inv_deg<<<nblk(eg.nnet), kT, 0, st>>>(eg.nnet, eg.d_net_deg, g->inv_deg);
     int col = 3;
     for (int k = 1; k <= kDiffSteps[2]; k++) {
-        k_diff_net<<<nblk(eg.nnet), kT, 0, st>>>(n, g->inv_deg, g->v, g->netv);
+        k_diff_net<<<nblk(31LL * n.n_big + eg.nnet), kT, 0, st>>>(n, g->inv_deg, g->v, g->netv);
         k_diff_node<<<nblk(eg.nn), kT, 0, st>>>(n, g->inv_pins, g->netv, g->v);
         if (k == kDiffSteps[0] || k == kDiffSteps[1] || k == kDiffSteps[2]) {
             k_store_feature<<<nblk(N), kT, 0, st>>>(N, g->v, g->X, col);
@@ -693,12 +762,12 @@ ep_status forward(ep_gnn *g) {
     cudaStream_t st = g->eg.st;
     const float *w = g->w;
     const __nv_bfloat16 *wb = g->wb;
-    k_dense<kF, 0><<<nblk(N, 64), kT, smem_dense(kF), st>>>(N, g->X, nullptr, wb + kOffW0, w + kOffB0, g->h[0]);
+    k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, wb + kOffW0, w + kOffB0, g->h[0]);
     for (int l = 1; l <= kLayers; l++) {
-        k_net_mean<<<nblk((long long)n.nnet * 32), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
+        k_net_mean<<<n.n_big + nblk(n.nnet - n.n_big, kBigWarps), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
                                                                 (float2 *)g->a);
         k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
-        k_dense<kH, kH><<<nblk(N, 64), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], wb + off_w(l),
+        k_dense<kH, kH><<<nblk(N, kDenseRows), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], wb + off_w(l),
                                                                      w + off_b(l), g->h[l]);
     }
     k_output<<<nblk(N), kT, 0, st>>>(N, g->h[kLayers], wb + kOffW4, w + kOffB4, g->v, g->raw, g->pred);

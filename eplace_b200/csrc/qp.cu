@@ -51,15 +51,59 @@ __device__ __forceinline__ float2 abs_pin(const float2 *__restrict__ pos, const 
 
 // Net::calcBoundPin: strict compares in double, the first pin at the
 // extreme wins; bound = (x-min, x-max, y-min, y-max) as indices in the net.
+// Nets in device order: the nets above kWarpPins pins (the head of that
+// order) take a warp each -- lane l scans pins l, l + 32, ... and the lanes'
+// (value, first index) pairs meet in a tree that keeps the extreme value and,
+// among equal values, the lower index, which is the serial scan's answer --
+// and the others a thread each.  A grid-stride loop over 32 n_big + (nnet -
+// n_big) slots; the HPWL of the net (double) joins the grid sum.
+struct Ext {
+    double v;
+    int k;
+};
+__device__ __forceinline__ void ext_min(Ext &a, double v, int k) {
+    if (v < a.v || (v == a.v && k < a.k)) a = Ext{v, k};
+}
+__device__ __forceinline__ void ext_max(Ext &a, double v, int k) {
+    if (v > a.v || (v == a.v && k < a.k)) a = Ext{v, k};
+}
+
 __global__ void __launch_bounds__(kQT)
-k_qp_bounds(int nnet, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
-            const int32_t *__restrict__ owner, const float2 *__restrict__ off,
+k_qp_bounds(int nnet, int n_big, const int32_t *__restrict__ order, const int32_t *__restrict__ first,
+            const int32_t *__restrict__ deg, const int32_t *__restrict__ owner, const float2 *__restrict__ off,
             const float2 *__restrict__ pos, int4 *__restrict__ bound, double *__restrict__ partials,
             unsigned *__restrict__ cnt, double *__restrict__ hpwl) {
     __shared__ double sh[32];
     double acc[1] = {0.0};
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nnet; n += gridDim.x * blockDim.x) {
-        const int f = first[n], d = deg[n];
+    const long long big = 32LL * n_big, slots = big + (nnet - n_big);
+    const int lane = threadIdx.x & 31;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < slots;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < big) {  // whole warps (big is a multiple of 32, so is the stride)
+            const int n = order[t >> 5], f = first[n], d = deg[n];
+            Ext lx{1.79769e308, 0x7fffffff}, hx{-1.79769e308, 0x7fffffff};
+            Ext ly{1.79769e308, 0x7fffffff}, hy{-1.79769e308, 0x7fffffff};
+            for (int k = lane; k < d; k += 32) {
+                const float2 a = abs_pin(pos, off, owner[f + k], f + k);
+                ext_min(lx, a.x, k);
+                ext_max(hx, a.x, k);
+                ext_min(ly, a.y, k);
+                ext_max(hy, a.y, k);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ext_min(lx, __shfl_xor_sync(0xffffffffu, lx.v, o), __shfl_xor_sync(0xffffffffu, lx.k, o));
+                ext_max(hx, __shfl_xor_sync(0xffffffffu, hx.v, o), __shfl_xor_sync(0xffffffffu, hx.k, o));
+                ext_min(ly, __shfl_xor_sync(0xffffffffu, ly.v, o), __shfl_xor_sync(0xffffffffu, ly.k, o));
+                ext_max(hy, __shfl_xor_sync(0xffffffffu, hy.v, o), __shfl_xor_sync(0xffffffffu, hy.k, o));
+            }
+            if (lane == 0) {
+                bound[n] = make_int4(lx.k, hx.k, ly.k, hy.k);
+                acc[0] += (hx.v - lx.v) + (hy.v - ly.v);
+            }
+            continue;
+        }
+        const int n = order[n_big + (int)(t - big)], f = first[n], d = deg[n];
         double mnx = 1.79769e308, mxx = -1.79769e308, mny = 1.79769e308, mxy = -1.79769e308;
         int4 b = make_int4(0, 0, 0, 0);
         for (int k = 0; k < d; k++) {
@@ -111,8 +155,59 @@ __device__ __forceinline__ float pair_weight(float c, float dist) {
     return dist >= kMinDistance ? __fdiv_rn(c, dist) : __fdiv_rn(c, kMinDistance);
 }
 
+// Pair (i, owner of pin q2) on one axis (pa, oa: pin a's coordinate and
+// offset on that axis): adds the pair's weight to the diagonal sum and its
+// term to the right-hand side; returns the partner node when it is movable
+// (an off-diagonal entry of weight -w), -1 when it is i itself (no pair) or
+// fixed (right-hand side only).
+__device__ __forceinline__ int pair_terms(int i, int nn, int q2, int axis, const int32_t *__restrict__ owner,
+                                          const float2 *__restrict__ pos, const float2 *__restrict__ off, float c,
+                                          float pa, float oa, float &w, double &dsum, double &bsum) {
+    const int j = owner[q2];
+    if (j == i) return -1;
+    const float2 pb2 = abs_pin(pos, off, j, q2);
+    const float pb = axis ? pb2.y : pb2.x, ob = axis ? off[q2].y : off[q2].x;
+    w = pair_weight(c, fabsf(__fsub_rn(pa, pb)));
+    dsum += w;
+    if (j < nn) {
+        bsum += -(double)w * (double)__fsub_rn(oa, ob);
+        return j;
+    }
+    bsum += (double)w * (double)__fsub_rn(pb, oa);
+    return -1;
+}
+
+// A pin's partner set as a range: pins [0, end) of its net but `skip`, then
+// `extra` (-1: none) -- the bound pins' sets of partners_x / partners_y.
+struct PartnerRange {
+    int end, skip, extra;
+};
+__device__ __forceinline__ bool range_x(int a, int d, int lo, int hi, PartnerRange &r) {
+    if (a != lo && a != hi) return false;
+    r = PartnerRange{d, a, -1};
+    return true;
+}
+__device__ __forceinline__ bool range_y(int a, int d, int lo, int hi, PartnerRange &r) {
+    if (a == hi) {
+        r = PartnerRange{d, a, -1};
+        return true;
+    }
+    if (a != lo) return false;
+    r = PartnerRange{a, -1, hi > a ? hi : -1};
+    return true;
+}
+// partner sets above kLongPartners pins are taken by the whole warp
+constexpr int kLongPartners = 32;
+__device__ __forceinline__ bool is_long(const PartnerRange &r) {
+    return r.end - (r.skip >= 0) + (r.extra >= 0) > kLongPartners;
+}
+
 // One movable node's row of both systems: counts (fill = 0) or entries,
-// diagonal and right-hand side (fill = 1).
+// diagonal and right-hand side (fill = 1).  A thread per node takes its pins'
+// short partner sets in pin order; then the warp takes the long ones (a bound
+// pin of a large net pairs with every other pin of it), in pin order, 32
+// partners at a time, entries placed by a ballot prefix so they keep the
+// partner order, the sums of the pairs' terms through a fixed xor tree.
 __global__ void __launch_bounds__(kQT)
 k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int32_t *__restrict__ obj_pin_dev,
           const int32_t *__restrict__ pin_net, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
@@ -121,57 +216,115 @@ k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int
           const int32_t *__restrict__ row_y, int32_t *__restrict__ col_x, float *__restrict__ val_x,
           int32_t *__restrict__ col_y, float *__restrict__ val_y, float2 *__restrict__ diag,
           float2 *__restrict__ rhs) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nn) return;
-    int cx = 0, cy = 0;
-    double dx = 0.0, dy = 0.0, bx = 0.0, by = 0.0;
-    const int ox = fill ? row_x[i] : 0, oy = fill ? row_y[i] : 0;
-    for (int k = obj_pin_start[i]; k < obj_pin_start[i + 1]; k++) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+    const bool valid = i < nn;  // every lane stays for the warp's long sets
+    int cnt[2] = {0, 0};
+    double dsum[2] = {0.0, 0.0}, bsum[2] = {0.0, 0.0};
+    const int row0[2] = {fill && valid ? row_x[i] : 0, fill && valid ? row_y[i] : 0};
+    int32_t *const col[2] = {col_x, col_y};
+    float *const val[2] = {val_x, val_y};
+    const int k0 = valid ? obj_pin_start[i] : 0, np_i = valid ? obj_pin_start[i + 1] - k0 : 0;
+    auto entry = [&](int axis, int j, float w, int at) {
+        if (fill) {
+            col[axis][row0[axis] + at] = j;
+            val[axis][row0[axis] + at] = -w;
+        }
+    };
+    for (int k = k0; k < k0 + np_i; k++) {
         const int q = obj_pin_dev[k], n = pin_net[q], f = first[n], d = deg[n], a = q - f;
         const int4 bd = bound[n];
         const float c = (float)(1.0 / ((double)d - 1.0));
         const float2 pa = abs_pin(pos, off, i, q), oa = off[q];
-        partners_x(a, d, bd.x, bd.y, [&](int b) {
-            const int q2 = f + b, j = owner[q2];
-            if (j == i) return;
-            const float2 pb = abs_pin(pos, off, j, q2);
-            const float w = pair_weight(c, fabsf(__fsub_rn(pa.x, pb.x)));
-            dx += w;
-            if (j < nn) {
-                if (fill) {
-                    col_x[ox + cx] = j;
-                    val_x[ox + cx] = -w;
-                }
-                cx++;
-                bx += -(double)w * (double)__fsub_rn(oa.x, off[q2].x);
-            } else {
-                bx += (double)w * (double)__fsub_rn(pb.x, oa.x);
-            }
-        });
-        partners_y(a, d, bd.z, bd.w, [&](int b) {
-            const int q2 = f + b, j = owner[q2];
-            if (j == i) return;
-            const float2 pb = abs_pin(pos, off, j, q2);
-            const float w = pair_weight(c, fabsf(__fsub_rn(pa.y, pb.y)));
-            dy += w;
-            if (j < nn) {
-                if (fill) {
-                    col_y[oy + cy] = j;
-                    val_y[oy + cy] = -w;
-                }
-                cy++;
-                by += -(double)w * (double)__fsub_rn(oa.y, off[q2].y);
-            } else {
-                by += (double)w * (double)__fsub_rn(pb.y, oa.y);
-            }
-        });
+        PartnerRange rx, ry;
+        const bool lx = range_x(a, d, bd.x, bd.y, rx) && is_long(rx);
+        const bool ly = range_y(a, d, bd.z, bd.w, ry) && is_long(ry);
+        if (!lx)
+            partners_x(a, d, bd.x, bd.y, [&](int b) {
+                float w;
+                const int j = pair_terms(i, nn, f + b, 0, owner, pos, off, c, pa.x, oa.x, w, dsum[0], bsum[0]);
+                if (j >= 0) entry(0, j, w, cnt[0]++);
+            });
+        if (!ly)
+            partners_y(a, d, bd.z, bd.w, [&](int b) {
+                float w;
+                const int j = pair_terms(i, nn, f + b, 1, owner, pos, off, c, pa.y, oa.y, w, dsum[1], bsum[1]);
+                if (j >= 0) entry(1, j, w, cnt[1]++);
+            });
     }
+    const int steps = __reduce_max_sync(0xffffffffu, np_i);
+    for (int s = 0; s < steps; s++) {
+        int q = 0, f = 0, d = 0;
+        PartnerRange r[2] = {{0, -1, -1}, {0, -1, -1}};
+        bool lg[2] = {false, false};
+        if (s < np_i) {
+            q = obj_pin_dev[k0 + s];
+            const int n = pin_net[q];
+            f = first[n];
+            d = deg[n];
+            const int4 bd = bound[n];
+            lg[0] = range_x(q - f, d, bd.x, bd.y, r[0]) && is_long(r[0]);
+            lg[1] = range_y(q - f, d, bd.z, bd.w, r[1]) && is_long(r[1]);
+        }
+        for (int axis = 0; axis < 2; axis++) {
+            unsigned todo = __ballot_sync(0xffffffffu, lg[axis]);
+            while (todo) {  // warp-uniform
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int si = __shfl_sync(0xffffffffu, i, src), sq = __shfl_sync(0xffffffffu, q, src);
+                const int sf = __shfl_sync(0xffffffffu, f, src), sd = __shfl_sync(0xffffffffu, d, src);
+                const int end = __shfl_sync(0xffffffffu, r[axis].end, src);
+                const int skip = __shfl_sync(0xffffffffu, r[axis].skip, src);
+                const int extra = __shfl_sync(0xffffffffu, r[axis].extra, src);
+                const int at0 = __shfl_sync(0xffffffffu, cnt[axis], src);
+                const float c = (float)(1.0 / ((double)sd - 1.0));
+                const float2 pa2 = abs_pin(pos, off, si, sq), oa2 = off[sq];
+                const float pa = axis ? pa2.y : pa2.x, oa = axis ? oa2.y : oa2.x;
+                const int row = fill ? (axis ? row_y[si] : row_x[si]) : 0;
+                double ds = 0.0, bs = 0.0;
+                int added = 0;
+                for (int base = 0; base < end; base += 32) {
+                    const int b = base + lane;
+                    float w = 0.f;
+                    int j = -1;
+                    if (b < end && b != skip) j = pair_terms(si, nn, sf + b, axis, owner, pos, off, c, pa, oa, w, ds, bs);
+                    const unsigned m = __ballot_sync(0xffffffffu, j >= 0);
+                    if (fill && j >= 0) {
+                        const int at = row + at0 + added + __popc(m & ((1u << lane) - 1));
+                        col[axis][at] = j;
+                        val[axis][at] = -w;
+                    }
+                    added += __popc(m);
+                }
+                if (extra >= 0) {
+                    int j = -1;
+                    float w = 0.f;
+                    if (lane == 0) j = pair_terms(si, nn, sf + extra, axis, owner, pos, off, c, pa, oa, w, ds, bs);
+                    if (fill && j >= 0) {
+                        col[axis][row + at0 + added] = j;
+                        val[axis][row + at0 + added] = -w;
+                    }
+                    added += __shfl_sync(0xffffffffu, j >= 0 ? 1 : 0, 0);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ds += __shfl_xor_sync(0xffffffffu, ds, o);
+                    bs += __shfl_xor_sync(0xffffffffu, bs, o);
+                }
+                if (lane == src) {
+                    cnt[axis] += added;
+                    dsum[axis] += ds;
+                    bsum[axis] += bs;
+                }
+            }
+        }
+    }
+    if (!valid) return;
     if (!fill) {
-        count[i] = cx;
-        count[nn + i] = cy;
+        count[i] = cnt[0];
+        count[nn + i] = cnt[1];
     } else {
-        diag[i] = make_float2((float)dx, (float)dy);
-        rhs[i] = make_float2((float)bx, (float)by);
+        diag[i] = make_float2((float)dsum[0], (float)dsum[1]);
+        rhs[i] = make_float2((float)bsum[0], (float)bsum[1]);
     }
 }
 
@@ -181,24 +334,62 @@ struct QpMat {
     const float2 *diag;
 };
 
-// (A_x v.x, A_y v.y) for row i, computed by the 8 lanes of an aligned lane
-// group (sub = lane index in the group): lane k sums entries k, k + 8, ...
-// of the row in order, a fixed xor tree adds the 8 partial sums, and the
-// diagonal term comes last, so the result is the same on every run.  Rows
-// of bound pins of large nets hold hundreds of entries; eight lanes per row
-// keep those from holding up a warp.  Every lane of the warp must call it
-// (valid = false for lanes past the last row); all 8 lanes get the result.
-constexpr int kRowLanes = 8, kRowsPerWarp = 32 / kRowLanes;
-__device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__restrict__ v, int i, int sub, bool valid) {
-    float ax = 0.f, ay = 0.f;
-    if (valid) {
-        for (int e = m.row_x[i] + sub; e < m.row_x[i + 1]; e += kRowLanes) ax = fmaf(m.val_x[e], v[m.col_x[e]].x, ax);
-        for (int e = m.row_y[i] + sub; e < m.row_y[i + 1]; e += kRowLanes) ay = fmaf(m.val_y[e], v[m.col_y[e]].y, ay);
+// (A_x v.x, A_y v.y) for row i.  A row takes the kRowLanes lanes of an
+// aligned lane group (lane sub of the group sums entries sub, sub + 8, ...
+// of both axes in order, a fixed xor tree adds the 8 partial sums); a row of
+// more than kLongRow entries on either axis (the bound pins of large nets)
+// takes the whole warp after the short rows are done (lane l sums entries
+// l, l + 32, ..., a fixed xor tree over the warp).  The diagonal term comes
+// last.  The split depends only on the row lengths, so the result is the
+// same on every run.  Every lane of the warp must call it (valid = false
+// for lanes past the last row); every lane of the row's group gets the
+// result.
+constexpr int kRowLanes = 8, kRowsPerWarp = 32 / kRowLanes, kLongRow = 4 * kRowLanes;
+
+__device__ __forceinline__ void row_partial(const QpMat &m, const float2 *__restrict__ v, int bx, int lx, int by,
+                                            int ly, int lane, int step, float &ax, float &ay) {
+    const int len = max(lx, ly);
+#pragma unroll 2
+    for (int k = lane; k < len; k += step) {
+        if (k < lx) ax = fmaf(m.val_x[bx + k], v[m.col_x[bx + k]].x, ax);
+        if (k < ly) ay = fmaf(m.val_y[by + k], v[m.col_y[by + k]].y, ay);
     }
+}
+
+__device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__restrict__ v, int i, int sub, bool valid) {
+    const int lane = threadIdx.x & 31;
+    int bx = 0, lx = 0, by = 0, ly = 0;
+    if (valid) {
+        bx = m.row_x[i];
+        lx = m.row_x[i + 1] - bx;
+        by = m.row_y[i];
+        ly = m.row_y[i + 1] - by;
+    }
+    const bool is_long = max(lx, ly) > kLongRow;
+    float ax = 0.f, ay = 0.f;
+    if (!is_long) row_partial(m, v, bx, lx, by, ly, sub, kRowLanes, ax, ay);
 #pragma unroll
     for (int o = kRowLanes / 2; o > 0; o >>= 1) {
         ax += __shfl_xor_sync(0xffffffffu, ax, o);
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    unsigned longs = __ballot_sync(0xffffffffu, is_long && sub == 0);
+    while (longs) {  // warp-uniform
+        const int src = __ffs(longs) - 1;
+        longs &= longs - 1;
+        const int lbx = __shfl_sync(0xffffffffu, bx, src), llx = __shfl_sync(0xffffffffu, lx, src);
+        const int lby = __shfl_sync(0xffffffffu, by, src), lly = __shfl_sync(0xffffffffu, ly, src);
+        float sx = 0.f, sy = 0.f;
+        row_partial(m, v, lbx, llx, lby, lly, lane, 32, sx, sy);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane / kRowLanes == src / kRowLanes) {
+            ax = sx;
+            ay = sy;
+        }
     }
     if (valid) {
         const float2 d = m.diag[i], vi = v[i];
@@ -208,9 +399,6 @@ __device__ __forceinline__ float2 spmv_row8(const QpMat &m, const float2 *__rest
     return make_float2(ax, ay);
 }
 
-// Grid-stride loop over the rows of a matrix kernel, kRowsPerWarp rows per
-// warp and pass; the loop bound is uniform over a warp (spmv_row8 shuffles),
-// and row i, lane sub of its group, are declared for the body.
 __device__ __forceinline__ int row_group_first() {
     return ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kRowsPerWarp;
 }
@@ -473,8 +661,9 @@ __global__ void k_qp_center(Grid g, int nn, const float2 *__restrict__ size, flo
 }  // namespace
 
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st) {
-    k_qp_bounds<<<qgrid(q.nnet), kQT, 0, st>>>(q.nnet, q.net_first, q.net_deg, q.owner, q.off, pos, q.bound,
-                                                 q.partials, q.cnt, hpwl);
+    k_qp_bounds<<<qgrid(31 * q.n_big + q.nnet), kQT, 0, st>>>(q.nnet, q.n_big, q.net_order, q.net_first, q.net_deg,
+                                                               q.owner, q.off, pos, q.bound, q.partials, q.cnt,
+                                                               hpwl);
 }
 
 void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
@@ -516,6 +705,6 @@ void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, c
     k_qp_center<<<qblocks(q.nn), kQT, 0, st>>>(g, q.nn, size, pos);
 }
 
-int qp_partial_blocks(int nn, int nnet) { return std::max(qgrid(kRowLanes * nn), qgrid(nnet)); }
+int qp_partial_blocks(int nn, int nnet) { return kQpMaxBlocks; }
 
 }  // namespace ep
