@@ -11,8 +11,10 @@ device, to overflow < 0.1:
          the committed weights and alpha), the committed number of rounds of
          the quadratic model from it (ep_quadratic_refine), then mGP in the
          mixed-precision form;
-  plain  the device quadratic placement (the reference flow's start) then
-         mGP with every vector, map and wirelength term in FP64.
+  plain  the device quadratic placement (the reference flow's start, run
+         for the reference's own number of rounds on this design, whose last
+         round ends at its stopping test's threshold) then mGP with every
+         vector, map and wirelength term in FP64.
 Both are timed with CUDA events on the engines' stream around the whole
 step (host work inside it shows as elapsed time), L2 flushed (256 MiB write)
 before each; the line carries both arms, their HPWL ratio and the GP-only
@@ -86,6 +88,15 @@ def workload_config(nl, extra=None):
 def reference_iterations():
     with open(REF_RUNS) as f:
         return json.load(f)["stdcell_200k_qp_mgp"]["iterations"]
+
+
+def reference_qp_rounds():
+    """Rounds of the reference's quadratic placement on this design (its log).
+    Its last round ends with the solver error at the stopping threshold
+    (1e-6), where float rounding decides between stopping and a round or two
+    more; the plain arm runs the same number of rounds as the reference."""
+    with open(REF_RUNS) as f:
+        return len(json.load(f)["stdcell_200k_qp_mgp"]["qp_trace"])
 
 
 class ClockSampler:
@@ -306,6 +317,7 @@ def main():
         return e
 
     mixed, plain = engine(placer.PREC_MIXED), engine(placer.PREC_FP64)
+    qp_rounds = reference_qp_rounds()
     info = mixed.info
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -336,7 +348,7 @@ def main():
 
     def plain_step():
         plain.load_positions()
-        qp = plain.quadratic_placement()
+        qp = plain.quadratic_placement(max_iterations=qp_rounds - 1)
         plain.initialize()
         st = plain.nesterov_run()
         st["start_ms"] = qp["seconds"] * 1e3
@@ -366,7 +378,7 @@ def main():
 
     # GP only: the mixed form from the plain arm's start (the QP result)
     plain.load_positions()
-    plain.quadratic_placement()
+    plain.quadratic_placement(max_iterations=qp_rounds - 1)
     qp_xy = plain.get_positions()
     mixed.set_positions(qp_xy)
     gp_mixed_ms, gp_mixed = timed(lambda: (mixed.initialize(), mixed.nesterov_run())[1])
@@ -385,7 +397,7 @@ def main():
         if how == "gnn":
             warmstart.propose(gnn, e, start)
         else:
-            e.quadratic_placement()
+            e.quadratic_placement(max_iterations=qp_rounds - 1)
         e.initialize()
         st = e.nesterov_run()
         n = e.info.num_objects
@@ -423,7 +435,7 @@ def main():
                    product=("learned warm start (ep_gnn_propose, alpha %.2f, then %d rounds of ep_quadratic_refine"
                             " of at most %d solver iterations) + mixed-precision mGP"
                             % (start["alpha"], start["rounds"], start["iters"])),
-                   plain="device quadratic placement + FP64 mGP",
+                   plain="device quadratic placement (%d rounds, the reference's count) + FP64 mGP" % qp_rounds,
                    mixed_precision="FP32 positions, FFT Poisson, gather and WA; int64 fixed-point density; "
                                    "FP64 reductions; network BF16 weights, FP32 accumulate",
                    plain_precision="FP64 positions, FFT Poisson, gather and WA; int64 fixed-point density")),

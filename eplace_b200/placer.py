@@ -24,7 +24,7 @@ EXP_FAST, EXP_EXACT = 0, 1
 STEP_LIPSCHITZ, STEP_BB, STEP_BKTRK = 0, 1, 2
 DCT_FP32, DCT_BF16X3, DCT_AUTO, DCT_FFT = 0, 1, 2, 3
 PREC_MIXED, PREC_FP64 = 0, 1
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define EP_ABI_VERSION 2
+#define EP_ABI_VERSION 3
 
 typedef enum ep_status {
     EP_OK = 0,

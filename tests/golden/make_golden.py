@@ -193,11 +193,36 @@ def record_variants():
     print("variants:", {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
 
 
+def qp_with_trace(ref):
+    """QPPlacer::quadraticPlacement with its per-round log line captured:
+    [(round, max(xError, yError) as printed, HPWL after the round)]."""
+    import ctypes
+    import re
+    import tempfile
+    R.lib().ref_set_quiet(0)
+    saved = os.dup(1)
+    with tempfile.TemporaryFile() as tmp:
+        sys.stdout.flush()
+        os.dup2(tmp.fileno(), 1)
+        try:
+            ref.qp()
+            ctypes.CDLL(None).fflush(None)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+            R.lib().ref_set_quiet(1)
+        tmp.seek(0)
+        text = tmp.read().decode(errors="replace")
+    rows = re.findall(r"at iteration number\s+(\d+),\s+CG Error ([-\d.e+]+),\s+HPWL ([\d.]+)", text)
+    return [(int(a), float(b), float(c)) for a, b, c in rows]
+
+
 def record_bench_reference():
     """The reference's whole runs on bench.py's 200k-cell design (a few
     minutes of CPU): from its own quadratic placement (QPPlacer, as its flow
     starts) and from bench.design()'s seeded blob; iterations to overflow
-    < 0.1, final overflow and HPWL, and the stage times."""
+    < 0.1, final overflow and HPWL, and the stage times; for the quadratic
+    placement also its per-round log (error as printed, HPWL)."""
     import json
     import time
     sys.path.insert(0, ROOT)
@@ -210,7 +235,7 @@ def record_bench_reference():
         rec = {}
         if qp:
             t0 = time.time()
-            ref.qp()
+            rec["qp_trace"] = qp_with_trace(ref)
             t_qp = time.time() - t0
             rec["qp_hpwl"] = float(ref.hpwl())
         t0 = time.time()

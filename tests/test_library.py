@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults():
     L = placer.load()
-    assert L.ep_abi_version() == placer.ABI_VERSION == 2
+    assert L.ep_abi_version() == placer.ABI_VERSION == 3
     p = placer.default_params()
     assert p.target_density == pytest.approx(1.0)
     assert p.target_overflow == pytest.approx(0.10)
