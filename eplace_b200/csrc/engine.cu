@@ -1703,6 +1703,100 @@ ep_status ep_load_positions(ep_engine *e) {
     return EP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Header of an optimizer-state blob; the five vectors and the scalars follow.
+struct StateHeader {
+    char magic[8];
+    int32_t abi, precision, n_obj, n_nodes, n_terms, n_nets, n_pins, nx, ny, stage, in_run, initialized;
+    uint32_t scalar_bytes, vec_bytes;
+};
+constexpr char kStateMagic[8] = {'E', 'P', 'S', 'T', 'A', 'T', 'E', '1'};
+constexpr int kStateVecs = 5;  // pos, x, g, y_prev, g_prev
+
+StateHeader state_header(const ep_engine *e) {
+    StateHeader h{};
+    std::memcpy(h.magic, kStateMagic, sizeof(h.magic));
+    h.abi = EP_ABI_VERSION;
+    h.precision = e->fp64 ? EP_PREC_FP64 : EP_PREC_MIXED;
+    h.n_obj = e->n_obj;
+    h.n_nodes = e->n_nodes;
+    h.n_terms = e->n_terms;
+    h.n_nets = e->n_nets;
+    h.n_pins = e->n_pins;
+    h.nx = e->grid.nx;
+    h.ny = e->grid.ny;
+    h.stage = e->stage;
+    h.in_run = e->in_run ? 1 : 0;
+    h.initialized = e->initialized ? 1 : 0;
+    h.scalar_bytes = (uint32_t)sizeof(DevScalars);
+    h.vec_bytes = (uint32_t)(e->v2 * e->n_obj);
+    return h;
+}
+}  // namespace
+
+extern "C" {
+
+uint64_t ep_state_size(const ep_engine *e) {
+    if (!e) return 0;
+    return sizeof(StateHeader) + sizeof(DevScalars) + (uint64_t)kStateVecs * e->v2 * e->n_obj;
+}
+
+ep_status ep_save_state(ep_engine *e, void *buf, uint64_t bytes) {
+    if (!e || !buf || bytes != ep_state_size(e)) return EP_ERR_ARG;
+    ep_status s = fetch_scalars(e);  // synchronises the stream
+    if (s) return s;
+    const StateHeader h = state_header(e);
+    unsigned char *p = static_cast<unsigned char *>(buf);
+    std::memcpy(p, &h, sizeof(h));
+    std::memcpy(p + sizeof(h), e->hS, sizeof(DevScalars));
+    unsigned char *v = p + sizeof(h) + sizeof(DevScalars);
+    const void *src[kStateVecs] = {e->pos, e->x, e->g, e->y_prev, e->g_prev};
+    for (int k = 0; k < kStateVecs; k++)
+        CK(cudaMemcpyAsync(v + (size_t)k * h.vec_bytes, src[k], h.vec_bytes, cudaMemcpyDeviceToHost, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return EP_OK;
+}
+
+ep_status ep_load_state(ep_engine *e, const void *buf, uint64_t bytes) {
+    if (!e || !buf) return EP_ERR_ARG;
+    if (bytes != ep_state_size(e)) {
+        e->err = "state blob of another size than this engine's";
+        return EP_ERR_ARG;
+    }
+    const unsigned char *p = static_cast<const unsigned char *>(buf);
+    StateHeader h;
+    std::memcpy(&h, p, sizeof(h));
+    StateHeader mine = state_header(e);
+    if (std::memcmp(h.magic, kStateMagic, sizeof(h.magic)) || h.abi != mine.abi || h.precision != mine.precision ||
+        h.n_obj != mine.n_obj || h.n_nodes != mine.n_nodes || h.n_terms != mine.n_terms ||
+        h.n_nets != mine.n_nets || h.n_pins != mine.n_pins || h.nx != mine.nx || h.ny != mine.ny ||
+        h.scalar_bytes != mine.scalar_bytes || h.vec_bytes != mine.vec_bytes) {
+        e->err = "state blob of another design, grid, precision or library version";
+        return EP_ERR_ARG;
+    }
+    if (!e->initialized) {
+        e->err = "ep_initialize must run before ep_load_state";
+        return EP_ERR_STATE;
+    }
+    if (h.stage != e->stage) {
+        e->err = "the state was saved in another stage: switch the engine to it first";
+        return EP_ERR_STATE;
+    }
+    std::memcpy(e->hS, p + sizeof(h), sizeof(DevScalars));
+    DevScalars &S = *e->hS;
+    S.cnt_prep = S.cnt_wl = S.cnt_comb = S.cnt_upd = S.cnt_hp = 0;  // no reduction in flight
+    const unsigned char *v = p + sizeof(h) + sizeof(DevScalars);
+    void *dst[kStateVecs] = {e->pos, e->x, e->g, e->y_prev, e->g_prev};
+    for (int k = 0; k < kStateVecs; k++)
+        CK(cudaMemcpyAsync(dst[k], v + (size_t)k * h.vec_bytes, h.vec_bytes, cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(e->S, e->hS, sizeof(DevScalars), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    e->in_run = h.in_run != 0;
+    return EP_OK;
+}
+
 ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try {
     if (!e || !out || reps <= 0) return EP_ERR_ARG;
     std::memset(out, 0, sizeof(*out));

@@ -114,7 +114,7 @@ EXPORTS = (
     "ep_set_stream", "ep_synchronize", "ep_get_positions", "ep_set_positions", "ep_initialize",
     "ep_eval_gradient", "ep_get_gradient", "ep_get_component_gradients", "ep_get_bin_maps",
     "ep_get_positions_f64", "ep_get_field_f64", "ep_get_component_gradients_f64",
-    "ep_get_limits", "ep_set_limits", "ep_quadratic_refine",
+    "ep_get_limits", "ep_set_limits", "ep_quadratic_refine", "ep_state_size", "ep_save_state", "ep_load_state",
     "ep_gnn_num_weights", "ep_gnn_create", "ep_gnn_destroy", "ep_gnn_last_error", "ep_gnn_get_weights",
     "ep_gnn_set_weights", "ep_gnn_release", "ep_gnn_features", "ep_gnn_forward", "ep_gnn_loss_grad",
     "ep_gnn_train_step", "ep_gnn_propose",
@@ -177,6 +177,10 @@ def load():
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(QpStats)]
+    L.ep_state_size.argtypes = [vp]
+    L.ep_state_size.restype = ctypes.c_uint64
+    L.ep_save_state.argtypes = [vp, vp, ctypes.c_uint64]
+    L.ep_load_state.argtypes = [vp, vp, ctypes.c_uint64]
     L.ep_run_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(RunStats)]
     L.ep_netbin_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.c_float, ctypes.c_int32]
     L.ep_netbin_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(Netlist), ctypes.POINTER(ctypes.c_float),
@@ -569,6 +573,20 @@ class Engine:
 
     def load_positions(self):
         self._check(self._L.ep_load_positions(self.h))
+
+    def save_state(self):
+        """ep_save_state: the optimizer's whole state as bytes (checkpoint)."""
+        n = int(self._L.ep_state_size(self.h))
+        buf = ctypes.create_string_buffer(n)
+        self._check(self._L.ep_save_state(self.h, buf, n))
+        return buf.raw
+
+    def load_state(self, blob):
+        """ep_load_state: resume from save_state's bytes (same design and
+        parameters, after initialize, in the saved stage)."""
+        blob = bytes(blob)
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        self._check(self._L.ep_load_state(self.h, buf, len(blob)))
 
     def set_stream(self, stream_ptr):
         self._check(self._L.ep_set_stream(self.h, ctypes.c_void_p(stream_ptr)))

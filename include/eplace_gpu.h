@@ -220,6 +220,23 @@ ep_status ep_get_positions_f64(ep_engine *e, int32_t view, double *xy, int32_t c
 ep_status ep_save_positions(ep_engine *e);
 ep_status ep_load_positions(ep_engine *e);
 
+/* Optimizer state, for checkpoint and resume: everything a run in progress
+ * carries between ep_nesterov_step calls -- every object's centre (y_k), the
+ * main sequence x_k, the gradient, the previous step's point and gradient,
+ * every scalar of EplaceNesterovOpt and the penalty (a_k, lambda, 1/gamma,
+ * the last HPWL, overflow, step length, iteration count, stop flag) and the
+ * stage -- as ep_state_size bytes in host memory.  ep_load_state, on an
+ * engine created from the same netlist and parameters and initialized
+ * (ep_initialize), in the saved stage, restores it: the ep_nesterov_step
+ * calls that follow take the saved run's next steps bit for bit.  The
+ * reference keeps positions only (PlaceDB::saveNodesLocation,
+ * PlaceDB/placedb.cpp:1441-1465).  EP_ERR_ARG for a blob of another size,
+ * design, grid or precision; EP_ERR_STATE before ep_initialize or in
+ * another stage. */
+uint64_t ep_state_size(const ep_engine *e);
+ep_status ep_save_state(ep_engine *e, void *buf, uint64_t bytes);
+ep_status ep_load_state(ep_engine *e, const void *buf, uint64_t bytes);
+
 /* EPlacer_2D::initialization tail (EPlace/eplace.cpp:47-49): first
  * totalGradientUpdate with lambda 0, then penaltyFactorInitilization. */
 ep_status ep_initialize(ep_engine *e);

@@ -15,14 +15,18 @@ pytestmark = pytest.mark.gpu
 
 
 def _engine(nl, mode, bins, keep=1):
-    return placer.Engine(nl, placer.default_params(target_density=1.0, bins_x=bins, bins_y=bins,
+    bx, by = bins if isinstance(bins, tuple) else (bins, bins)
+    return placer.Engine(nl, placer.default_params(target_density=1.0, bins_x=bx, bins_y=by,
                                                    dct_mode=mode, keep_maps=keep))
 
 
-@pytest.mark.parametrize("bins", [128, 256])
+# 512 x 512 runs the split-K GEMMs (4-CTA clusters); the non-square grids
+# give the two transforms different sizes
+@pytest.mark.parametrize("bins", [(128, 128), (256, 256), (512, 512), (256, 128), (128, 384)])
 def test_tensor_core_field_matches_fp64_oracle(bins):
     nl = synth.blob_start(synth.standard_cell(20_000, seed=5), sigma_frac=0.15)
     e = _engine(nl, placer.DCT_BF16X3, bins)
+    assert (e.info.bins_x, e.info.bins_y) == bins and e.info.dct_mode == placer.DCT_BF16X3
     e.initialize()
     m = e.bin_maps()
     i = e.info
