@@ -13,7 +13,10 @@
 //     EplaceNesterovOpt loop (Optimization/nesterov.hpp:86-415) step by step;
 //   * read back every intermediate the hot path produces (bin maps, field,
 //     potential, density / wirelength / total gradients, tau, 1/gamma, lambda,
-//     HPWL) at full float precision, bypassing the %.0f .pl writer.
+//     HPWL) at full float precision, bypassing the %.0f .pl writer;
+//   * run the reference's CPU stages around global placement on whatever
+//     positions were set: SAMacroLegalizer (mLG), AbacusLegalizer and
+//     DetailedPlacer (main/ePlace_main.cpp:174-279).
 // Nothing here re-implements reference arithmetic: every number comes from
 // the reference's own functions.
 
@@ -35,6 +38,8 @@
 #include "opt.hpp"
 #include "parser.h"
 #include "qplace.h"
+#include "legalizer.h"
+#include "detailed.h"
 #include "Eigen/Dense"
 
 // The optimizer keeps its per-step methods private; the harness needs to call
@@ -209,6 +214,46 @@ double ref_qp(void *hp)
     QPPlacer qp(h->db);
     double t0 = now_s();
     qp.quadraticPlacement();
+    return now_s() - t0;
+}
+
+// SAMacroLegalizer::legalization (Legalization/legalizer.cpp:701-845), as
+// main/ePlace_main.cpp:176-181 runs it between mGP and FILLERONLY; returns
+// its seconds.
+double ref_macro_legalize(void *hp, float target_density)
+{
+    Quiet q;
+    RefHandle *h = static_cast<RefHandle *>(hp);
+    SAMacroLegalizer lg(h->db);
+    lg.setTargetDensity(target_density);
+    double t0 = now_s();
+    lg.legalization();
+    return now_s() - t0;
+}
+
+// AbacusLegalizer::legalization (Legalization/legalizer.cpp:58-183), the
+// flow's internal legalizer (main/ePlace_main.cpp:251-262); returns its
+// seconds.
+double ref_abacus(void *hp)
+{
+    Quiet q;
+    RefHandle *h = static_cast<RefHandle *>(hp);
+    AbacusLegalizer lg(h->db);
+    double t0 = now_s();
+    lg.legalization();
+    return now_s() - t0;
+}
+
+// DetailedPlacer::detailedPlacement (DetailedPlacement/detailed.cpp), run
+// after the internal legalizer (main/ePlace_main.cpp:268-279); returns its
+// seconds.
+double ref_detailed(void *hp)
+{
+    Quiet q;
+    RefHandle *h = static_cast<RefHandle *>(hp);
+    DetailedPlacer dp(h->db);
+    double t0 = now_s();
+    dp.detailedPlacement();
     return now_s() - t0;
 }
 

@@ -48,11 +48,13 @@ def lib():
                      "ref_opt_end", "ref_switch_filler_only", "ref_switch_cgp"):
             getattr(L, name).argtypes = [_vp]
             getattr(L, name).restype = None
-        for name in ("ref_qp", "ref_eval", "ref_opt_run", "ref_calc_hpwl"):
+        for name in ("ref_qp", "ref_eval", "ref_opt_run", "ref_calc_hpwl", "ref_abacus", "ref_detailed"):
             getattr(L, name).argtypes = [_vp]
             getattr(L, name).restype = ctypes.c_double
         L.ref_init.argtypes = [_vp, ctypes.c_float]
         L.ref_init.restype = ctypes.c_double
+        L.ref_macro_legalize.argtypes = [_vp, ctypes.c_float]
+        L.ref_macro_legalize.restype = ctypes.c_double
         L.ref_netlist_counts.argtypes = [_vp, _i32p]
         L.ref_get_info.argtypes = [_vp, _f64p]
         L.ref_get_positions.argtypes = [_vp, _f32p, _f32p]
@@ -133,6 +135,19 @@ class RefPlacer:
     # --- netlist-stage helpers -------------------------------------------------
     def qp(self):
         return lib().ref_qp(self.h)
+
+    # --- the CPU stages around global placement (main/ePlace_main.cpp:174-279)
+    def macro_legalize(self, target_density):
+        """SAMacroLegalizer::legalization on the current positions; seconds."""
+        return lib().ref_macro_legalize(self.h, float(target_density))
+
+    def abacus(self):
+        """AbacusLegalizer::legalization on the current positions; seconds."""
+        return lib().ref_abacus(self.h)
+
+    def detailed(self):
+        """DetailedPlacer::detailedPlacement after the legalizer; seconds."""
+        return lib().ref_detailed(self.h)
 
     def node_centers(self):
         cx = np.zeros(self.num_nodes, np.float32)

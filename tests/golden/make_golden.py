@@ -13,7 +13,11 @@ computes on the same netlist and starting positions:
   * the first optimizer steps (positions, tau, lambda after each);
   * the whole mGP run (iterations, final tau, HPWL);
   * variants.npz: the LSE and BB options and the mixed-size stage sequence
-    (record_variants).
+    (record_variants);
+  * flows.npz: the CPU stages around global placement, the macro legalizer
+    between mGP and cGP and Abacus + detailed placement on config 1
+    (record_flows);
+  * reference_runs.json (--bench): the whole runs on bench.py's design.
 
     python tests/golden/make_golden.py [--variants-only] [--bench]
 """
@@ -32,6 +36,7 @@ from oracle import refharness as R  # noqa: E402
 REF_SRC = os.environ.get("EPLACE_REF_SRC", "")
 REF_SMOKE = os.path.join(REF_SRC, "examples", "smoke", "smoke.aux")
 TRAJ_STEPS = 5
+C1_SEEDS = (1, 2, 4)
 
 
 def designs():
@@ -193,6 +198,62 @@ def record_variants():
     print("variants:", {k: (v if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
 
 
+def record_flows():
+    """The reference's CPU stages around global placement, on designs the
+    GPU flow tests rerun with the engine in place of its global placement:
+      * mlg_*: mixed_5k from its recorded start: initialization, mGP, the SA
+        macro legalizer (SAMacroLegalizer), FILLERONLY and cGP, as
+        main/ePlace_main.cpp:174-211 runs them (node centres after mGP and
+        after mLG, HPWL after each stage, the cGP outcome);
+      * c1_<seed>_*: config 1 (synth.smoke) from the netlist: QPPlacer,
+        initialization, mGP, AbacusLegalizer, DetailedPlacer
+        (main/ePlace_main.cpp:248-279): HPWL after GP, legalization and
+        detailed placement, and the final centres.  The reference's
+        DetailedPlacer ends the process with a segmentation fault on smoke
+        seeds 3 and 7 (after its own QP, mGP and Abacus); C1_SEEDS leaves
+        them out.
+    Written to flows.npz."""
+    out = {}
+    g = np.load(os.path.join(HERE, "mixed_5k.npz"))
+    mx = synth.blob_start(synth.mixed_size(5000, 6, 3, seed=5))
+    assert np.array_equal(np.asarray(g["nl_node_w"]), mx.node_w)
+    ref = R.RefPlacer(mx)
+    ref.initialization(mx.target_density)
+    ref.opt_run()
+    cx, cy = ref.node_centers()
+    out["mlg_mgp_cx"], out["mlg_mgp_cy"], out["mlg_mgp_hpwl"] = cx, cy, np.float64(ref.hpwl())
+    out["mlg_seconds"] = np.float64(ref.macro_legalize(mx.target_density))
+    cx, cy = ref.node_centers()
+    out["mlg_cx"], out["mlg_cy"], out["mlg_hpwl"] = cx, cy, np.float64(ref.hpwl())
+    ref.switch_filler_only()
+    fo = run_stage(ref)
+    ref.switch_cgp()
+    cg = run_stage(ref)
+    out["mlg_fo_hpwl"] = fo["hpwl"]
+    for k in ("iterations", "overflow", "hpwl"):
+        out["mlg_cgp_" + k] = cg[k]
+    out["mlg_cgp_cx"], out["mlg_cgp_cy"] = ref.node_centers()
+    ref.close()
+    for seed in C1_SEEDS:
+        nl = synth.smoke(seed)
+        ref = R.RefPlacer(nl)
+        ref.qp()
+        ref.initialization(nl.target_density)
+        ref.opt_run()
+        k = f"c1_{seed}_"
+        out[k + "gp_hpwl"] = np.float64(ref.hpwl())
+        out[k + "gp_overflow"] = np.float64(ref.info()["overflow"])
+        ref.abacus()
+        out[k + "lg_hpwl"] = np.float64(ref.hpwl())
+        ref.detailed()
+        out[k + "dp_hpwl"] = np.float64(ref.hpwl())
+        out[k + "cx"], out[k + "cy"] = ref.node_centers()
+        ref.close()
+    path = os.path.join(HERE, "flows.npz")
+    np.savez_compressed(path, **out)
+    print("flows:", {k: (float(v) if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
+
+
 def qp_with_trace(ref):
     """QPPlacer::quadraticPlacement with its per-round log line captured:
     [(round, max(xError, yError) as printed, HPWL after the round)]."""
@@ -263,5 +324,6 @@ if __name__ == "__main__":
         for name, nl, qp in designs():
             record(name, nl, qp)
     record_variants()
+    record_flows()
     if "--bench" in sys.argv:
         record_bench_reference()
