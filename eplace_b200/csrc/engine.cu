@@ -13,6 +13,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <chrono>
 #include <cstring>
 #include <new>
 #include <random>
@@ -102,6 +103,7 @@ struct ep_engine {
     int32_t *net_first = nullptr, *net_deg = nullptr, *pin_net = nullptr;
     int32_t *net_dev_order = nullptr;  // nets in device pin order (grouped by degree)
     int n_big_nets = 0;                // nets above kWarpPins pins (the head of that order)
+    double create_s[3] = {0.0, 0.0, 0.0};  // ep_create phases (ep_info.create_seconds)
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
@@ -522,6 +524,13 @@ const char *ep_last_error(const ep_engine *e) { return e ? e->err.c_str() : "nul
 // ep_create's body; the host arrays it builds may throw std::bad_alloc,
 // which ep_create turns into EP_ERR_NOMEM.
 static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_params *params) {
+    const auto t_start = std::chrono::steady_clock::now();
+    auto lap = [&e, &t_start](int k) {
+        const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+        double before = 0.0;
+        for (int j = 0; j < k; j++) before += e->create_s[j];
+        e->create_s[k] = t - before;
+    };
     e->prm = *params;
     const ep_params &P = e->prm;
     ep_status s = check_netlist(e, nl);
@@ -881,6 +890,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     kc.want_wl_value = P.keep_maps ? 1 : 0;
     kc.fp64 = e->fp64;
 
+    lap(0);
     // ---- device ----
     const size_t v2 = e->v2;
     if ((s = dalloc_bytes(e, e->pos, v2 * (no + nt))) || (s = dalloc_bytes(e, e->x, v2 * no)) ||
@@ -973,6 +983,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         (s = dalloc(e, kc.part_hp, (size_t)2 * std::max(1, reduction_blocks(d, 0)))))
         return s;
 
+    lap(1);
     int rc = EP_ERR_UNSUPPORTED;
     if (P.dct_mode == EP_DCT_AUTO && e->fp64) {
         // the FP64 form has the fast transforms only
@@ -995,6 +1006,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     s = upload_view(e, EP_STAGE_MGP);
     if (s) return s;
     CK(cudaDeviceSynchronize());
+    lap(2);
     return EP_OK;
 }
 
@@ -1061,6 +1073,7 @@ ep_status ep_get_info(const ep_engine *e, ep_info *info) {
     info->density_scale = e->kc.qscale;
     info->dct_mode = e->dct.mode;
     info->precision = e->fp64 ? EP_PREC_FP64 : EP_PREC_MIXED;
+    for (int k = 0; k < 3; k++) info->create_seconds[k] = e->create_s[k];
     return EP_OK;
 }
 

@@ -85,7 +85,8 @@ class Info(ctypes.Structure):
                 ("filler_w", ctypes.c_float), ("filler_h", ctypes.c_float),
                 ("std_area", ctypes.c_double), ("macro_area", ctypes.c_double),
                 ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double),
-                ("dct_mode", ctypes.c_int32), ("precision", ctypes.c_int32)]
+                ("dct_mode", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("create_seconds", ctypes.c_double * 3)]
 
 
 class RunStats(ctypes.Structure):

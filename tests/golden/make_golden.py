@@ -207,8 +207,10 @@ def record_flows():
         after mLG, HPWL after each stage, the cGP outcome);
       * c1_<seed>_*: config 1 (synth.smoke) from the netlist: QPPlacer,
         initialization, mGP, AbacusLegalizer, DetailedPlacer
-        (main/ePlace_main.cpp:248-279): HPWL after GP, legalization and
-        detailed placement, and the final centres.  The reference's
+        (main/ePlace_main.cpp:248-279): every object's centre after
+        initialization (the QP result and the reference's fillers), HPWL
+        and iterations after GP, HPWL after legalization and detailed
+        placement, and the final centres.  The reference's
         DetailedPlacer ends the process with a segmentation fault on smoke
         seeds 3 and 7 (after its own QP, mGP and Abacus); C1_SEEDS leaves
         them out.
@@ -239,9 +241,11 @@ def record_flows():
         ref = R.RefPlacer(nl)
         ref.qp()
         ref.initialization(nl.target_density)
-        ref.opt_run()
         k = f"c1_{seed}_"
+        out[k + "init_cx"], out[k + "init_cy"] = ref.positions()  # QP result and the fillers
+        ref.opt_run()
         out[k + "gp_hpwl"] = np.float64(ref.hpwl())
+        out[k + "gp_iterations"] = np.int64(ref.info()["iter_count"])
         out[k + "gp_overflow"] = np.float64(ref.info()["overflow"])
         ref.abacus()
         out[k + "lg_hpwl"] = np.float64(ref.hpwl())
