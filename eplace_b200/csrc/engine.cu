@@ -68,14 +68,18 @@ struct ep_engine {
     float *npins = nullptr, *area = nullptr, *node_f = nullptr, *filler_f = nullptr;
     void *rho = nullptr, *phi = nullptr;
     float *sxy = nullptr;
-    int32_t *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pin_dev = nullptr;
+    int32_t *pin_owner = nullptr, *obj_pin_start = nullptr, *obj_pin_dev = nullptr, *pin_obj_slot = nullptr;
     int32_t *big_objs = nullptr, *big_slot = nullptr;
     int4 *net_tasks = nullptr;
     int32_t *view_idx[3] = {nullptr, nullptr, nullptr};
     unsigned long long *node_q = nullptr, *filler_q = nullptr;
     DevScalars *S = nullptr;
     DevScalars *hS = nullptr;  // pinned mirror
+    // device memory: buffers are carved from a few large chunks (one
+    // cudaMalloc per chunk, chunks doubling from 4 MiB), freed together
     std::vector<void *> allocs;
+    unsigned char *arena_cur = nullptr;
+    size_t arena_left = 0, arena_next = 4u << 20;
 
     DeviceNetlist dn{};
     DctPlan dct;
@@ -103,7 +107,7 @@ struct ep_engine {
     int32_t *net_first = nullptr, *net_deg = nullptr, *pin_net = nullptr;
     int32_t *net_dev_order = nullptr;  // nets in device pin order (grouped by degree)
     int n_big_nets = 0;                // nets above kWarpPins pins (the head of that order)
-    double create_s[3] = {0.0, 0.0, 0.0};  // ep_create phases (ep_info.create_seconds)
+    double create_s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ep_create phases (ep_info.create_seconds)
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
@@ -176,13 +180,24 @@ void location_to_center_h(const Grid &g, float llx, float lly, float w, float h,
 template <typename T>
 ep_status dalloc(ep_engine *e, T *&p, size_t n) {
     if (n == 0) n = 1;
-    cudaError_t rc = cudaMalloc((void **)&p, n * sizeof(T));
-    if (rc != cudaSuccess) {
-        e->err = std::string("cudaMalloc: ") + cudaGetErrorString(rc);
-        p = nullptr;
-        return EP_ERR_NOMEM;
+    const size_t bytes = (n * sizeof(T) + 255) & ~(size_t)255;  // 256-byte aligned buffers
+    if (bytes > e->arena_left) {
+        const size_t chunk = std::max(bytes, e->arena_next);
+        void *q = nullptr;
+        cudaError_t rc = cudaMalloc(&q, chunk);
+        if (rc != cudaSuccess) {
+            e->err = std::string("cudaMalloc: ") + cudaGetErrorString(rc);
+            p = nullptr;
+            return EP_ERR_NOMEM;
+        }
+        e->allocs.push_back(q);
+        e->arena_cur = static_cast<unsigned char *>(q);
+        e->arena_left = chunk;
+        e->arena_next = std::min<size_t>(2 * e->arena_next, (size_t)1 << 30);
     }
-    e->allocs.push_back((void *)p);
+    p = reinterpret_cast<T *>(e->arena_cur);
+    e->arena_cur += bytes;
+    e->arena_left -= bytes;
     return EP_OK;
 }
 
@@ -603,6 +618,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     g.ury = top;
     g.td = P.target_density;
 
+    lap(0);
     // ---- node classes (PlaceDB::addNode) ----
     std::vector<uint8_t> is_macro(nn, 0);
     for (int i = 0; i < nn; i++) {
@@ -783,6 +799,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     }
 
     // ---- pins: net CSR and the object -> pin CSR (pins in id order) ----
+    lap(1);
     std::vector<int32_t> owner(np), net_start(nnet + 1, 0);
     std::vector<float2> off(np);
     for (int n = 0; n <= nnet; n++) net_start[n] = nnet > 0 ? nl->net_start[n] : 0;
@@ -861,9 +878,12 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         for (int k = 0; k < d; k++) e->h_pin_net[dev_of_pin[a + k]] = n;
     }
     // each object's pins (reference order) -> their device positions
-    std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0);
+    std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0), pin_obj_slot(std::max(np, 1), -1);
     for (int p = 0; p < np; p++)
-        if (pin_slot[p] >= 0) obj_pin_dev[pin_slot[p]] = dev_of_pin[p];
+        if (pin_slot[p] >= 0) {
+            obj_pin_dev[pin_slot[p]] = dev_of_pin[p];
+            pin_obj_slot[dev_of_pin[p]] = pin_slot[p];
+        }
 
     // stage views (EPlace/eplace.cpp:190-203)
     for (int o = 0; o < no; o++) {
@@ -890,7 +910,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     kc.want_wl_value = P.keep_maps ? 1 : 0;
     kc.fp64 = e->fp64;
 
-    lap(0);
+    lap(2);
     // ---- device ----
     const size_t v2 = e->v2;
     if ((s = dalloc_bytes(e, e->pos, v2 * (no + nt))) || (s = dalloc_bytes(e, e->x, v2 * no)) ||
@@ -904,6 +924,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         (s = dalloc_bytes(e, e->rho, e->r * nb)) || (s = dupload(e, e->sxy, h_sxy)) ||
         (s = dupload(e, e->pin_owner, dev_owner)) || (s = dupload(e, e->obj_pin_start, ops)) ||
         (s = dupload(e, e->obj_pin_dev, obj_pin_dev)) || (s = dupload(e, e->net_tasks, net_tasks)) ||
+        (s = dupload(e, e->pin_obj_slot, pin_obj_slot)) ||
         (s = dupload(e, e->big_objs, big)) ||
         (s = dupload(e, e->big_slot, big_slot)) || (s = dalloc(e, e->node_q, nb)) ||
         (s = dalloc(e, e->filler_q, nb)) || (s = dalloc(e, e->S, 1)))
@@ -972,6 +993,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     d.pin_off = e->pin_off;
     d.obj_pin_start = e->obj_pin_start;
     d.obj_pin_dev = e->obj_pin_dev;
+    d.pin_obj_slot = e->pin_obj_slot;
     d.net_tasks = e->net_tasks;
     d.n_net_tasks = (int)net_tasks.size();
     d.big_objs = e->big_objs;
@@ -983,7 +1005,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         (s = dalloc(e, kc.part_hp, (size_t)2 * std::max(1, reduction_blocks(d, 0)))))
         return s;
 
-    lap(1);
+    lap(3);
     int rc = EP_ERR_UNSUPPORTED;
     if (P.dct_mode == EP_DCT_AUTO && e->fp64) {
         // the FP64 form has the fast transforms only
@@ -1006,7 +1028,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     s = upload_view(e, EP_STAGE_MGP);
     if (s) return s;
     CK(cudaDeviceSynchronize());
-    lap(2);
+    lap(4);
     return EP_OK;
 }
 
@@ -1073,7 +1095,7 @@ ep_status ep_get_info(const ep_engine *e, ep_info *info) {
     info->density_scale = e->kc.qscale;
     info->dct_mode = e->dct.mode;
     info->precision = e->fp64 ? EP_PREC_FP64 : EP_PREC_MIXED;
-    for (int k = 0; k < 3; k++) info->create_seconds[k] = e->create_s[k];
+    for (int k = 0; k < 5; k++) info->create_seconds[k] = e->create_s[k];
     return EP_OK;
 }
 
@@ -1891,7 +1913,7 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
     s = timed("poisson_dct", dct_launches(e->dct), (fft ? 36.0 * q : 16.0) * nbin, dct_flops,
               [&] { dct_run(e->dct, e->rho, e->field, nullptr, e->S, e->st); }, nothing);
     if (s) return s;
-    s = timed("wirelength", d.n_net_tasks > 0, (12.0 + 16.0 * q) * npin + 16.0 * d.n_net_tasks, 0.0,
+    s = timed("wirelength", d.n_net_tasks > 0, (16.0 + 16.0 * q) * npin + 16.0 * d.n_net_tasks, 0.0,
               [&] { launch_wirelength(e->kc, d, e->pin_grad, e->S, e->st); }, nothing);
     if (s) return s;
     if (d.n_big_objs > 0) {
@@ -1899,7 +1921,7 @@ ep_status ep_time_kernels(ep_engine *e, int32_t reps, ep_kernel_times *out) try 
                   [&] { launch_gather_big(e->kc, d, e->field, e->gd_big, e->S, e->st); }, nothing);
         if (s) return s;
     }
-    s = timed("combine", 1, (29.0 + 56.0 * q) * nobj + (4.0 + 8.0 * q) * npin, 0.0,
+    s = timed("combine", 1, (29.0 + 56.0 * q) * nobj + 8.0 * q * npin, 0.0,
               [&] {
                   launch_combine(e->kc, d, e->field, e->gd_big, e->pin_grad, e->g, e->g_prev,
                                  e->y_prev, nullptr, nullptr, 1, e->S, e->st);

@@ -110,6 +110,10 @@ struct DeviceNetlist {
     const float2 *pin_off;
     const int32_t *obj_pin_start;  // [n_obj + 1] object -> its pins (reference pin order)
     const int32_t *obj_pin_dev;    // device position of each of those pins
+    const int32_t *pin_obj_slot;   // [n_pins] device pin -> its slot in that object-major
+                                   // order (-1 for terminal pins): where the per-net pass
+                                   // writes the pin's gradient, so each object's pin
+                                   // gradients lie contiguous for the combine
     const int4 *net_tasks;         // per warp of the per-net pass: degree, first pin, nets,
                                    // ceil(2^16 / degree) (0 for nets above kWarpPins pins)
     int n_net_tasks;

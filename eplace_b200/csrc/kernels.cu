@@ -200,6 +200,7 @@ struct PinCtx {
     const int32_t *__restrict__ owner;
     const float2 *__restrict__ off;
     const vec2<R> *__restrict__ pos;
+    const int32_t *__restrict__ slot;  // device pin -> object-major gradient slot (-1: terminal)
 };
 
 // Pin::calculateAbsolutePos: centre + offset.
@@ -414,7 +415,8 @@ __device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const Pin
                   mul_rn(xy.y, e.emy), e.emy, mul_rn(xy.y, e.eny), e.eny};
         seg_sums<R>(s, D, base, k);
         const NetSums<R> ns = net_sums<R>(s);
-        if (act) out[p0 + lane] = pin_gradient<LSE, R>(e, xy, igx, igy, net_coef<R>(ns));
+        const int sl = act ? pc.slot[p0 + lane] : -1;
+        if (sl >= 0) out[sl] = pin_gradient<LSE, R>(e, xy, igx, igy, net_coef<R>(ns));
         if (want_value && act && k == 0) r.value = net_value<R>(ns, x1, x0, y1, y0, igx, igy, LSE);
     }
     return r;
@@ -457,7 +459,9 @@ __device__ __forceinline__ NetOut net_in_warp(const int4 t, int lane, const PinC
         const NetCoef<R> c = net_coef<R>(ns);
         for (int k = lane; k < D; k += 32) {
             const vec2<R> xy = k < kStagedPins ? stage[k] : pin_xy<R>(pc, p0 + k);
-            out[p0 + k] = pin_gradient<LSE, R>(pin_exps<EXACT, R>(xy, x1, x0, y1, y0, igx, igy), xy, igx, igy, c);
+            const int sl = pc.slot[p0 + k];
+            if (sl >= 0)
+                out[sl] = pin_gradient<LSE, R>(pin_exps<EXACT, R>(xy, x1, x0, y1, y0, igx, igy), xy, igx, igy, c);
         }
         if (want_value && lane == 0) r.value = net_value<R>(ns, x1, x0, y1, y0, igx, igy, LSE);
     }
@@ -630,11 +634,11 @@ k_combine(Grid g, DeviceNetlist d, const vec2<R> *__restrict__ field, const vec2
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // dg2, dy2, s.y, |gwl|, |gd|
 
     // Wirelength gradient of the object: its pins' gradients added in pin
-    // order (EPlace/eplace.cpp:539-547).  The objects of a warp own one
-    // contiguous run of pin slots, so the warp stages that run's gradients
-    // in shared memory with all its loads in flight at once (kPinChunk per
-    // round), then every lane adds its own pins from there in order.
-    // Fillers own no pins.
+    // order (EPlace/eplace.cpp:539-547).  The per-net pass wrote them in
+    // object-major order, so the objects of a warp own one contiguous run of
+    // gradient slots: the warp stages that run in shared memory with
+    // coalesced loads all in flight at once (kPinChunk per round), then
+    // every lane adds its own pins from there in order.  Fillers own no pins.
     __shared__ vec2<R> pin_sm[kThreads / 32][kPinChunk];
     R wx = (R)0, wy = (R)0;
     {
@@ -646,15 +650,11 @@ k_combine(Grid g, DeviceNetlist d, const vec2<R> *__restrict__ field, const vec2
         const int wend = __reduce_max_sync(0xffffffffu, (unsigned)pe);
         for (int base = wbeg; base < wend; base += kPinChunk) {  // warp-uniform
             const int n = min(kPinChunk, wend - base);
-            int idx[kPinChunk / 32];
 #pragma unroll
             for (int u = 0; u < kPinChunk / 32; u++) {
                 const int t = lane + 32 * u;
-                idx[u] = t < n ? d.obj_pin_dev[base + t] : -1;
+                if (t < n) sm[t] = pin_grad[base + t];
             }
-#pragma unroll
-            for (int u = 0; u < kPinChunk / 32; u++)
-                if (idx[u] >= 0) sm[lane + 32 * u] = pin_grad[idx[u]];
             __syncwarp();
             const int k1 = min(pe, base + n);
             for (int k = max(ps, base); k < k1; k++) {
@@ -999,7 +999,7 @@ void launch_prep(const KernelCtx &c, ull *node_q, ull *filler_q, const float2 *s
 template <bool WL, bool EXACT, bool LSE, typename R>
 static void launch_nets(const KernelCtx &c, const DeviceNetlist &d, void *pin_grad, double *partials, int mode,
                         DevScalars *S, cudaStream_t st) {
-    PinCtx<R> pc{d.pin_owner, d.pin_off, V<R>(d.pos)};
+    PinCtx<R> pc{d.pin_owner, d.pin_off, V<R>(d.pos), d.pin_obj_slot};
     if (d.n_net_tasks == 0) return;
     launch_kp(k_wl<WL, EXACT, LSE, R>, reduction_blocks(d, 0), kNetWarps * 32, 0, st, launch_priority(false),
               d.net_tasks, d.n_net_tasks, pc, V<R>(pin_grad), c.want_wl_value, partials, mode, S);

@@ -413,7 +413,8 @@ __device__ __forceinline__ int row_group_stride() { return ((gridDim.x * blockDi
 // recurrence kept in device memory (QpSolve) and updated by the finalising
 // block of the grid reduction that produces its inputs; vector kernels read
 // alpha, beta and omega from there.  Per axis c:
-//   pre      rho_old = rho; rho = r0.r; restart when |rho| < eps^2 r0sq
+//   head     rho_old = rho; rho = r0.r; restart when |rho| < eps^2 r0sq
+//            (in the finaliser of the previous step, or of the set-up)
 //   restart  (only when flagged) r = b - A x, r0 = r; rho = r0sq = |r|^2,
 //            the iteration count reset at the first restart
 //   dir      p = r + beta (p - omega v), beta = (rho / rho_old)(alpha / omega)
@@ -427,6 +428,21 @@ __device__ __forceinline__ int row_group_stride() { return ((gridDim.x * blockDi
 // every kernel returns at once when neither axis is active, so iterations
 // can be enqueued ahead of the convergence test.
 __device__ __forceinline__ bool any_active(const QpSolve *S) { return S->active[0] || S->active[1]; }
+
+// The head of an iteration (rho_old = rho; rho = r0.r; the restart test),
+// run by the finaliser that ends the previous iteration (or the set-up).
+__device__ void qp_pre(QpSolve *S) {
+    if (!any_active(S)) return;
+    const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
+    int restart = 0;
+    for (int c = 0; c < 2; c++) {
+        S->rho_old[c] = S->rho[c];
+        if (!S->active[c]) continue;
+        S->rho[c] = S->r0r[c];
+        if (fabs(S->rho[c]) < eps2 * S->r0sq[c]) restart |= 1 << c;
+    }
+    S->restart_mask = restart;
+}
 
 // r = b - A x, r0 = r, p = v = 0; |r|^2 and |b|^2 per system, then the
 // solver's initial state.
@@ -474,6 +490,7 @@ k_qp_init(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__restr
             }
         }
         S->max_it = max_it;
+        qp_pre(S);
     }
 }
 
@@ -485,18 +502,7 @@ __global__ void k_qp_zero(int nn, const QpSolve *__restrict__ S, float2 *__restr
     if (S->zero_mask & 2) x[i].y = 0.f;
 }
 
-__global__ void k_qp_pre(QpSolve *__restrict__ S) {
-    if (threadIdx.x != 0 || !any_active(S)) return;
-    const double eps = 1.1920928955078125e-07, eps2 = eps * eps;
-    int restart = 0;
-    for (int c = 0; c < 2; c++) {
-        S->rho_old[c] = S->rho[c];
-        if (!S->active[c]) continue;
-        S->rho[c] = S->r0r[c];
-        if (fabs(S->rho[c]) < eps2 * S->r0sq[c]) restart |= 1 << c;
-    }
-    S->restart_mask = restart;
-}
+
 
 // Restart of the flagged systems: r = b - A x, r0 = r; rho = r0sq = |r|^2.
 __global__ void __launch_bounds__(kQT)
@@ -633,6 +639,7 @@ k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, co
             S->it[c]++;
             S->active[c] = S->rr[c] > S->tol2[c] && S->it[c] < S->max_it;
         }
+        qp_pre(S);
     }
 }
 
@@ -683,7 +690,6 @@ void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
 void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
     const int b = qblocks(q.nn), bm = qgrid(kRowLanes * q.nn), br = qgrid(q.nn);
     for (int k = 0; k < count; k++) {
-        k_qp_pre<<<1, 32, 0, st>>>(q.solve);
         k_qp_restart<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
         k_qp_dir<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.p, q.solve);
         k_qp_av<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);

@@ -86,7 +86,7 @@ class Info(ctypes.Structure):
                 ("std_area", ctypes.c_double), ("macro_area", ctypes.c_double),
                 ("total_row_area", ctypes.c_double), ("density_scale", ctypes.c_double),
                 ("dct_mode", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("create_seconds", ctypes.c_double * 3)]
+                ("create_seconds", ctypes.c_double * 5)]
 
 
 class RunStats(ctypes.Structure):

@@ -142,11 +142,12 @@ typedef struct ep_info {
     double density_scale;         /* fixed-point units per unit area of the bin maps */
     int32_t dct_mode;             /* ep_dct_mode in use (never EP_DCT_AUTO) */
     int32_t precision;            /* ep_precision in use */
-    /* wall seconds of ep_create: [0] host set-up (checks, CUDA context,
-     * streams, core, fillers, static density maps, the netlist's device
-     * layout), [1] device allocation and upload, [2] transform plan and
-     * the final synchronisation */
-    double create_seconds[3];
+    /* wall seconds of ep_create: [0] checks, CUDA device, streams and
+     * events, core region; [1] node classes, fillers, terminal and base
+     * density maps; [2] the netlist's device layout (pin order, per-net
+     * tasks, object -> pin maps); [3] device allocation and upload;
+     * [4] transform plan and the final synchronisation */
+    double create_seconds[5];
 } ep_info;
 
 typedef struct ep_run_stats {

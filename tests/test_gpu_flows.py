@@ -31,8 +31,9 @@ def flows():
     return load_golden("flows")
 
 
-def _config1_engine(nl):
-    return placer.Engine(nl, placer.default_params(target_density=0.8, bins_x=16, bins_y=16,
+def _config1_engine(nl, bins):
+    """bins 0: the reference's bin-count rule (8 x 8 on these designs)."""
+    return placer.Engine(nl, placer.default_params(target_density=0.8, bins_x=bins, bins_y=bins,
                                                    precision=placer.PREC_FP64))
 
 
@@ -51,13 +52,15 @@ def _legalize_and_check(nl, seed, xy, tmp_path):
 
 @pytest.mark.parametrize("seed", [1, 2, 4])
 def test_config1_from_reference_start_then_reference_legalizer(flows, seed, tmp_path):
-    """From the reference's own start (its QP result and fillers): the engine's
-    mGP within 10% of the reference's iterations and 1% of its HPWL; after
-    the reference's Abacus + detailed placement on it, legal and within 3% of
-    the reference's flow."""
+    """From the reference's own start (its QP result and fillers) on the
+    reference's bin grid (its rule gives 8 x 8 here; the reference cannot be
+    given another): the engine's mGP within 10% of the reference's
+    iterations and 1% of its HPWL; after the reference's Abacus + detailed
+    placement on it, legal and within 3% of the reference's flow."""
     nl = synth.smoke(seed)
     k = f"c1_{seed}_"
-    e = _config1_engine(nl)
+    e = _config1_engine(nl, 0)
+    assert e.info.bins_x == e.info.bins_y == 8
     e.set_positions(np.stack([flows[k + "init_cx"], flows[k + "init_cy"]], 1))
     e.initialize()
     st = e.nesterov_run()
@@ -73,12 +76,13 @@ def test_config1_from_reference_start_then_reference_legalizer(flows, seed, tmp_
 
 @pytest.mark.parametrize("seed", [1, 2, 4])
 def test_config1_engine_flow_then_reference_legalizer(flows, seed, tmp_path):
-    """The engine's whole global placement (device QP, its own fillers, mGP),
-    then the reference's Abacus + detailed placement: legal, and within 6% of
-    the reference's flow (on 100 cells the fillers' random start alone moves
-    the result by a few percent)."""
+    """Config 1 as specified -- 16 x 16 bins -- with the engine's whole global
+    placement (device QP, its own fillers, mGP), then the reference's Abacus
+    + detailed placement: legal, and within 6% of the reference's flow (which
+    ran on its own 8 x 8 grid; on 100 cells the grid and the fillers' random
+    start move the result by a few percent)."""
     nl = synth.smoke(seed)
-    e = _config1_engine(nl)
+    e = _config1_engine(nl, 16)
     e.quadratic_placement()
     e.initialize()
     st = e.nesterov_run()
