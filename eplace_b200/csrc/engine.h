@@ -61,7 +61,6 @@ inline void launch_kp(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sm
 constexpr int kWarpPins = 32;
 constexpr int kStagedPins = 128;
 constexpr int kNetWarps = 8;  // warps per block of the per-net pass
-constexpr int kTasksPerWarp = 2;  // consecutive tasks a warp of the per-net pass takes
 // Objects whose bin footprint may exceed this many bins take the
 // block-per-object scatter / gather path.
 constexpr int kSmallObjectBins = 16;

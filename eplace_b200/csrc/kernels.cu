@@ -396,33 +396,14 @@ __device__ __forceinline__ NetSums<R> net_sums(const R (&s)[8]) {
     return NetSums<R>{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7]};
 }
 
-// A lane's pin of a packed task: its position and gradient slot (-1 for a
-// lane past the task's nets and for a terminal's pin).
-template <typename R>
-struct LanePin {
-    vec2<R> xy;
-    int slot;
-};
-template <typename R>
-__device__ __forceinline__ LanePin<R> lane_pin(const int4 t, int lane, const PinCtx<R> &pc) {
-    const bool act = ((lane * t.w) >> 16) < t.z;
-    LanePin<R> L{mk2<R>((R)0, (R)0), -1};
-    if (act) {
-        L.xy = pin_xy<R>(pc, t.y + lane);
-        L.slot = pc.slot[t.y + lane];
-    }
-    return L;
-}
-
-// Nets of degree D <= 32 packed on the lanes of one warp, the lane's pin
-// already loaded (lane_pin).
+// Nets of degree D <= 32 packed on the lanes of one warp.
 template <bool WL, bool EXACT, bool LSE, typename R>
-__device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const LanePin<R> &L,
-                                               vec2<R> *__restrict__ out, R igx, R igy, int want_value) {
-    const int D = t.x;
+__device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const PinCtx<R> &pc, vec2<R> *__restrict__ out,
+                                               R igx, R igy, int want_value) {
+    const int D = t.x, p0 = t.y;
     const int seg = (lane * t.w) >> 16, base = seg * D, k = lane - base;
     const bool act = seg < t.z;
-    const vec2<R> xy = L.xy;
+    const vec2<R> xy = act ? pin_xy<R>(pc, p0 + lane) : mk2<R>((R)0, (R)0);
     // bound pins (Net::calcBoundPin, PlaceCommon/objects.cpp:75-144)
     R x1 = xy.x, x0 = xy.x, y1 = xy.y, y0 = xy.y;
     seg_bounds<R>(x1, x0, y1, y0, D, base, k);
@@ -434,7 +415,8 @@ __device__ __forceinline__ NetOut nets_in_warp(const int4 t, int lane, const Lan
                   mul_rn(xy.y, e.emy), e.emy, mul_rn(xy.y, e.eny), e.eny};
         seg_sums<R>(s, D, base, k);
         const NetSums<R> ns = net_sums<R>(s);
-        if (L.slot >= 0) out[L.slot] = pin_gradient<LSE, R>(e, xy, igx, igy, net_coef<R>(ns));
+        const int sl = act ? pc.slot[p0 + lane] : -1;
+        if (sl >= 0) out[sl] = pin_gradient<LSE, R>(e, xy, igx, igy, net_coef<R>(ns));
         if (want_value && act && k == 0) r.value = net_value<R>(ns, x1, x0, y1, y0, igx, igy, LSE);
     }
     return r;
@@ -496,35 +478,13 @@ k_wl(const int4 *__restrict__ tasks, int n_tasks, PinCtx<R> pc, vec2<R> *__restr
     if (WL && S->done) return;
     const R igx = (R)S->inv_gamma_x, igy = (R)S->inv_gamma_y;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // two consecutive tasks per warp: when both are packed tasks, both
-    // pins' loads are in flight before either task's arithmetic
-    const int w = (blockIdx.x * kNetWarps + wid) * kTasksPerWarp;
+    const int w = blockIdx.x * kNetWarps + wid;
     NetOut r{0.0, 0.0};
     if (w < n_tasks) {  // warp-uniform
-        const int4 t0 = tasks[w];
-        const bool has1 = w + 1 < n_tasks;
-        const int4 t1 = has1 ? tasks[w + 1] : make_int4(0, 0, 0, 0);
-        vec2<R> *sg = stage[WL ? wid : 0];
-        if (t0.x <= kWarpPins && t1.x <= kWarpPins) {
-            const LanePin<R> a = lane_pin<R>(t0, lane, pc);
-            const LanePin<R> b = lane_pin<R>(t1, lane, pc);
-            r = nets_in_warp<WL, EXACT, LSE, R>(t0, lane, a, out, igx, igy, want_value);
-            if (has1) {
-                const NetOut r1 = nets_in_warp<WL, EXACT, LSE, R>(t1, lane, b, out, igx, igy, want_value);
-                r.hpwl += r1.hpwl;
-                r.value += r1.value;
-            }
-        } else {
-            for (int j = 0; j < (has1 ? 2 : 1); j++) {
-                const int4 t = j ? t1 : t0;
-                const NetOut rj = t.x <= kWarpPins
-                                      ? nets_in_warp<WL, EXACT, LSE, R>(t, lane, lane_pin<R>(t, lane, pc), out, igx,
-                                                                        igy, want_value)
-                                      : net_in_warp<WL, EXACT, LSE, R>(t, lane, pc, out, igx, igy, want_value, sg);
-                r.hpwl += rj.hpwl;
-                r.value += rj.value;
-            }
-        }
+        const int4 t = tasks[w];
+        r = t.x <= kWarpPins ? nets_in_warp<WL, EXACT, LSE, R>(t, lane, pc, out, igx, igy, want_value)
+                             : net_in_warp<WL, EXACT, LSE, R>(t, lane, pc, out, igx, igy, want_value,
+                                                              stage[WL ? wid : 0]);
     }
     // the smooth wirelength value rides along only when asked for
     bool last;
@@ -977,7 +937,7 @@ int prep_blocks(const Grid &g) { return std::min(blocks_for(g.nx * g.ny, kThread
 
 int reduction_blocks(const DeviceNetlist &d, int which) {
     switch (which) {
-        case 0: return blocks_for(d.n_net_tasks, kNetWarps * kTasksPerWarp);
+        case 0: return blocks_for(d.n_net_tasks, kNetWarps);
         default: return blocks_for(d.n_obj, kThreads);
     }
 }
