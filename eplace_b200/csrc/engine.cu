@@ -10,6 +10,7 @@
 // then laid out on the device as SoA arrays plus two CSRs (net -> pins,
 // object -> pins) and the loop of kernels.cu / dct.cu runs there.
 #include <algorithm>
+#include <future>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -538,6 +539,28 @@ const char *ep_last_error(const ep_engine *e) { return e ? e->err.c_str() : "nul
 
 // ep_create's body; the host arrays it builds may throw std::bad_alloc,
 // which ep_create turns into EP_ERR_NOMEM.
+// Ascending sort of non-negative floats (the node areas) by their bit
+// patterns, which order like the values: three 11-bit LSD radix passes.
+// Anything else (a negative or NaN area) goes through std::sort.
+static void sort_areas(std::vector<float> &a) {
+    for (float v : a)
+        if (!(v >= 0.0f)) {
+            std::sort(a.begin(), a.end());
+            return;
+        }
+    const size_t n = a.size();
+    std::vector<uint32_t> k(n), tmp(n);
+    for (size_t i = 0; i < n; i++) std::memcpy(&k[i], &a[i], 4);
+    for (int shift = 0; shift < 33; shift += 11) {
+        size_t cnt[2049] = {0};
+        for (size_t i = 0; i < n; i++) cnt[((k[i] >> shift) & 2047) + 1]++;
+        for (int d = 0; d < 2048; d++) cnt[d + 1] += cnt[d];
+        for (size_t i = 0; i < n; i++) tmp[cnt[(k[i] >> shift) & 2047]++] = k[i];
+        k.swap(tmp);
+    }
+    for (size_t i = 0; i < n; i++) std::memcpy(&a[i], &k[i], 4);
+}
+
 static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_params *params) {
     const auto t_start = std::chrono::steady_clock::now();
     auto lap = [&e, &t_start](int k) {
@@ -632,15 +655,36 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     }
 
     // ---- fillers (fillerInitialization) ----
+    // Terminal area on the rows, summed over terminals then rows in order.  A
+    // row outside a terminal's y-range adds an exact zero, so only the rows
+    // whose bottom lies below the terminal's top and above its bottom minus
+    // the tallest row are visited (found by bisection), still in row order.
     float overlap = 0;
-    for (int t = 0; t < nt; t++) {
-        if (nl->term_is_ni && nl->term_is_ni[t]) continue;
-        for (int r = 0; r < nr; r++)
-            overlap += (float)overlap_area_h(nl->term_llx[t], nl->term_lly[t],
-                                             nl->term_llx[t] + nl->term_w[t],
-                                             nl->term_lly[t] + nl->term_h[t], nl->row_llx[r],
-                                             nl->row_lly[r], nl->row_urx[r],
-                                             (float)((double)nl->row_lly[r] + nl->row_h[r]));
+    {
+        std::vector<int> by_y(nr);
+        for (int r = 0; r < nr; r++) by_y[r] = r;
+        std::stable_sort(by_y.begin(), by_y.end(), [&](int a, int b) { return nl->row_lly[a] < nl->row_lly[b]; });
+        std::vector<float> ys(nr);
+        float max_h = 0.0f;
+        for (int k = 0; k < nr; k++) {
+            ys[k] = nl->row_lly[by_y[k]];
+            max_h = std::max(max_h, nl->row_h[by_y[k]]);
+        }
+        std::vector<int> cand;
+        for (int t = 0; t < nt; t++) {
+            if (nl->term_is_ni && nl->term_is_ni[t]) continue;
+            const float tb = nl->term_lly[t], tt = nl->term_lly[t] + nl->term_h[t];
+            const size_t k0 = std::lower_bound(ys.begin(), ys.end(), (float)((double)tb - max_h) - 1.0f) - ys.begin();
+            const size_t k1 = std::upper_bound(ys.begin(), ys.end(), tt) - ys.begin();
+            cand.assign(by_y.begin() + k0, by_y.begin() + k1);
+            std::sort(cand.begin(), cand.end());
+            for (int r : cand)
+                overlap += (float)overlap_area_h(nl->term_llx[t], nl->term_lly[t],
+                                                 nl->term_llx[t] + nl->term_w[t],
+                                                 nl->term_lly[t] + nl->term_h[t], nl->row_llx[r],
+                                                 nl->row_lly[r], nl->row_urx[r],
+                                                 (float)((double)nl->row_lly[r] + nl->row_h[r]));
+        }
     }
     float whitespace = total_row_area - overlap;
     float sa = 0, ma = 0;
@@ -657,7 +701,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     e->macro_area = ma;
     float node_scaled = sa + ma * P.target_density;
     float total_filler = whitespace * P.target_density - node_scaled;
-    std::sort(areas.begin(), areas.end());
+    sort_areas(areas);
     int lo = (int)(0.05 * (float)nn), hi = (int)(0.95 * (float)nn);
     float acc = 0;
     for (int i = lo; i < hi; i++) acc += areas[i];
@@ -688,58 +732,63 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     const int nb = nbx * nby;
     const float bin_area_f = g.sx * g.sy;
 
-    // terminal density (EPlace/eplace.cpp:327-374) and base density (:385-409)
-    std::vector<float> term_d(nb, 0.0f), base_d(nb, 0.0f);
-    auto bin_box = [&](int i, int j, float &l, float &b, float &r, float &t) {
-        l = (float)i * g.sx + g.llx;
-        b = (float)j * g.sy + g.lly;
-        r = l + g.sx;
-        t = b + g.sy;
-    };
-    for (int t = 0; t < nt; t++) {
-        float llx = nl->term_llx[t], lly = nl->term_lly[t];
-        float urx = llx + nl->term_w[t], ury = lly + nl->term_h[t];
-        if (llx < g.llx || llx + nl->term_w[t] > g.urx) continue;
-        if (lly < g.lly || lly + nl->term_h[t] > g.ury) continue;
-        int i0 = (int)((llx - g.llx) / g.sx), i1 = (int)((urx - g.llx) / g.sx);
-        int j0 = (int)((lly - g.lly) / g.sy), j1 = (int)((ury - g.lly) / g.sy);
-        i1 = std::min(i1, nbx - 1);
-        j1 = std::min(j1, nby - 1);
-        for (int i = std::max(i0, 0); i <= i1; i++)
-            for (int j = std::max(j0, 0); j <= j1; j++) {
-                float l, b, r, tt;
-                bin_box(i, j, l, b, r, tt);
-                term_d[(size_t)i * nby + j] +=
-                    (float)(P.target_density * overlap_area_h(l, b, r, tt, llx, lly, urx, ury));
-            }
-    }
-    {
-        // only rows meeting a bin's y-range contribute non-zero terms; they
-        // are summed in row order, as the reference's full loop would
-        std::vector<std::vector<int>> rows_of(nby);
-        for (int j = 0; j < nby; j++) {
-            float l, b, r, t;
-            bin_box(0, j, l, b, r, t);
-            for (int rr = 0; rr < nr; rr++) {
-                double rb = nl->row_lly[rr], rt = (float)((double)nl->row_lly[rr] + nl->row_h[rr]);
-                if (overlap_len_h(b, t, rb, rt) != 0) rows_of[j].push_back(rr);
-            }
+    // terminal density (EPlace/eplace.cpp:327-374) and base density
+    // (:385-409): read-only inputs, computed on a second host thread while
+    // this one lays out the objects and pins
+    std::future<std::vector<float2>> stat_job = std::async(std::launch::async, [&, nbx, nby, nb]() {
+        std::vector<float> term_d(nb, 0.0f), base_d(nb, 0.0f);
+        auto bin_box = [&](int i, int j, float &l, float &b, float &r, float &t) {
+            l = (float)i * g.sx + g.llx;
+            b = (float)j * g.sy + g.lly;
+            r = l + g.sx;
+            t = b + g.sy;
+        };
+        for (int t = 0; t < nt; t++) {
+            float llx = nl->term_llx[t], lly = nl->term_lly[t];
+            float urx = llx + nl->term_w[t], ury = lly + nl->term_h[t];
+            if (llx < g.llx || llx + nl->term_w[t] > g.urx) continue;
+            if (lly < g.lly || lly + nl->term_h[t] > g.ury) continue;
+            int i0 = (int)((llx - g.llx) / g.sx), i1 = (int)((urx - g.llx) / g.sx);
+            int j0 = (int)((lly - g.lly) / g.sy), j1 = (int)((ury - g.lly) / g.sy);
+            i1 = std::min(i1, nbx - 1);
+            j1 = std::min(j1, nby - 1);
+            for (int i = std::max(i0, 0); i <= i1; i++)
+                for (int j = std::max(j0, 0); j <= j1; j++) {
+                    float l, b, r, tt;
+                    bin_box(i, j, l, b, r, tt);
+                    term_d[(size_t)i * nby + j] +=
+                        (float)(P.target_density * overlap_area_h(l, b, r, tt, llx, lly, urx, ury));
+                }
         }
-        for (int i = 0; i < nbx; i++)
+        {
+            // only rows meeting a bin's y-range contribute non-zero terms; they
+            // are summed in row order, as the reference's full loop would
+            std::vector<std::vector<int>> rows_of(nby);
             for (int j = 0; j < nby; j++) {
                 float l, b, r, t;
-                bin_box(i, j, l, b, r, t);
-                float avail = 0;
-                for (int rr : rows_of[j])
-                    avail += (float)overlap_area_h(l, b, r, t, nl->row_llx[rr], nl->row_lly[rr],
-                                                   nl->row_urx[rr],
-                                                   (float)((double)nl->row_lly[rr] + nl->row_h[rr]));
-                base_d[(size_t)i * nby + j] =
-                    f_equal_h(bin_area_f, avail) ? 0.0f : P.target_density * (bin_area_f - avail);
+                bin_box(0, j, l, b, r, t);
+                for (int rr = 0; rr < nr; rr++) {
+                    double rb = nl->row_lly[rr], rt = (float)((double)nl->row_lly[rr] + nl->row_h[rr]);
+                    if (overlap_len_h(b, t, rb, rt) != 0) rows_of[j].push_back(rr);
+                }
             }
-    }
-    std::vector<float2> stat(nb);
-    for (int k = 0; k < nb; k++) stat[k] = make_float2(term_d[k], base_d[k]);
+            for (int i = 0; i < nbx; i++)
+                for (int j = 0; j < nby; j++) {
+                    float l, b, r, t;
+                    bin_box(i, j, l, b, r, t);
+                    float avail = 0;
+                    for (int rr : rows_of[j])
+                        avail += (float)overlap_area_h(l, b, r, t, nl->row_llx[rr], nl->row_lly[rr],
+                                                       nl->row_urx[rr],
+                                                       (float)((double)nl->row_lly[rr] + nl->row_h[rr]));
+                    base_d[(size_t)i * nby + j] =
+                        f_equal_h(bin_area_f, avail) ? 0.0f : P.target_density * (bin_area_f - avail);
+                }
+        }
+        std::vector<float2> st(nb);
+        for (int k = 0; k < nb; k++) st[k] = make_float2(term_d[k], base_d[k]);
+        return st;
+    });
 
     // ---- objects ----
     e->h_size.resize(no);
@@ -910,6 +959,7 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     kc.want_wl_value = P.keep_maps ? 1 : 0;
     kc.fp64 = e->fp64;
 
+    const std::vector<float2> stat = stat_job.get();
     lap(2);
     // ---- device ----
     const size_t v2 = e->v2;

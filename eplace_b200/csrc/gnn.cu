@@ -123,6 +123,7 @@ __global__ void k_inv_deg(int nnet, const int32_t *__restrict__ deg, float *__re
 // same degree.  Launched with 32 n_big + (nnet - n_big) threads.
 __global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ v,
                            float2 *__restrict__ a) {
+    pdl_begin();
     const int t = blockIdx.x * blockDim.x + threadIdx.x, big = g.n_big * 32;
     if (t < big) {  // whole warps
         const int n = g.net_order[t >> 5], lane = t & 31;
@@ -155,6 +156,7 @@ __global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float
 
 __global__ void k_diff_node(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ a,
                             float2 *__restrict__ v) {
+    pdl_begin();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nn) return;
     const int q0 = g.obj_pin_start[c], q1 = g.obj_pin_start[c + 1];
@@ -169,6 +171,7 @@ __global__ void k_diff_node(Net g, const float *__restrict__ inv_pins, const flo
 }
 
 __global__ void k_store_feature(int N, const float2 *__restrict__ v, float *__restrict__ X, int col) {
+    pdl_begin();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     X[(size_t)c * kF + col] = v[c].x;
@@ -705,10 +708,12 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     k_inv_deg<<<nblk(eg.nnet), kT, 0, st>>>(eg.nnet, eg.d_net_deg, g->inv_deg);
     int col = 3;
     for (int k = 1; k <= kDiffSteps[2]; k++) {
-        k_diff_net<<<nblk(31LL * n.n_big + eg.nnet), kT, 0, st>>>(n, g->inv_deg, g->v, g->netv);
-        k_diff_node<<<nblk(eg.nn), kT, 0, st>>>(n, g->inv_pins, g->netv, g->v);
+        // programmatic serialisation: the next pass's blocks wait resident
+        launch_k(k_diff_net, nblk(31LL * n.n_big + eg.nnet), kT, 0, st, n, (const float *)g->inv_deg,
+                 (const float2 *)g->v, g->netv);
+        launch_k(k_diff_node, nblk(eg.nn), kT, 0, st, n, (const float *)g->inv_pins, (const float2 *)g->netv, g->v);
         if (k == kDiffSteps[0] || k == kDiffSteps[1] || k == kDiffSteps[2]) {
-            k_store_feature<<<nblk(N), kT, 0, st>>>(N, g->v, g->X, col);
+            launch_k(k_store_feature, nblk(N), kT, 0, st, N, (const float2 *)g->v, g->X, col);
             col += 2;
         }
     }

@@ -510,6 +510,7 @@ k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__re
              float2 *__restrict__ r0, double *__restrict__ partials, unsigned *__restrict__ cnt,
              QpSolve *__restrict__ S) {
     __shared__ double sh[2 * 32];
+    pdl_begin();
     const int mask = S->restart_mask;
     if (!mask || !any_active(S)) return;  // uniform over the grid
     double acc[2] = {0.0, 0.0};
@@ -540,6 +541,7 @@ k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__re
 __global__ void __launch_bounds__(kQT)
 k_qp_dir(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ p,
          const QpSolve *__restrict__ S) {
+    pdl_begin();
     if (!any_active(S)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
@@ -557,6 +559,7 @@ __global__ void __launch_bounds__(kQT)
 k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict__ r0, float2 *__restrict__ v,
         double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[2 * 32];
+    pdl_begin();
     if (!any_active(S)) return;
     double acc[2] = {0.0, 0.0};
     ROW_GROUPS(nn) {
@@ -576,6 +579,7 @@ k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict_
 __global__ void __launch_bounds__(kQT)
 k_qp_s(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ s,
        const QpSolve *__restrict__ S) {
+    pdl_begin();
     if (!any_active(S)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
@@ -589,6 +593,7 @@ __global__ void __launch_bounds__(kQT)
 k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, double *__restrict__ partials,
         unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
+    pdl_begin();
     if (!any_active(S)) return;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     ROW_GROUPS(nn) {
@@ -613,6 +618,7 @@ k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, co
           const float2 *__restrict__ r0, float2 *__restrict__ x, float2 *__restrict__ r, double *__restrict__ partials,
           unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
+    pdl_begin();
     if (!any_active(S)) return;
     float a[2], w[2];
     for (int c = 0; c < 2; c++) {
@@ -690,12 +696,14 @@ void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
 void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
     const int b = qblocks(q.nn), bm = qgrid(kRowLanes * q.nn), br = qgrid(q.nn);
     for (int k = 0; k < count; k++) {
-        k_qp_restart<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
-        k_qp_dir<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.p, q.solve);
-        k_qp_av<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
-        k_qp_s<<<b, kQT, 0, st>>>(q.nn, q.r, q.v, q.s, q.solve);
-        k_qp_at<<<bm, kQT, 0, st>>>(q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
-        k_qp_step<<<br, kQT, 0, st>>>(q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
+        // programmatic serialisation: each kernel's blocks are resident and
+        // waiting (pdl_begin) while the previous one drains
+        launch_k(k_qp_restart, bm, kQT, 0, st, q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
+        launch_k(k_qp_dir, b, kQT, 0, st, q.nn, q.r, q.v, q.p, q.solve);
+        launch_k(k_qp_av, bm, kQT, 0, st, q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
+        launch_k(k_qp_s, b, kQT, 0, st, q.nn, q.r, q.v, q.s, q.solve);
+        launch_k(k_qp_at, bm, kQT, 0, st, q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
+        launch_k(k_qp_step, br, kQT, 0, st, q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
     }
 }
 

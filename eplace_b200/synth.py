@@ -317,17 +317,20 @@ def standard_cell(num_cells=200_000, num_nets=None, num_terminals=None, seed=7,
 
 
 def mixed_size(num_cells=20_000, num_movable_macros=12, num_fixed_macros=4, seed=11,
-               utilisation=0.75, target_density=1.0, bins=0):
+               utilisation=0.75, target_density=1.0, bins=0, macro_rows=None, **cell_options):
     """Mixed-size design (the ePlace-MS shape at reduced scale): standard cells as
     in ``standard_cell`` plus movable macros (square or 2:1, side log-uniform
-    between 2% and 8% of the die) and fixed macros inside the core, which
-    exercise the macro density scaling, terminal density and base density."""
+    between 2% and 8% of the die, or between ``macro_rows`` = (lo, hi) rows)
+    and fixed macros inside the core, which exercise the macro density
+    scaling, terminal density and base density.  ``cell_options`` go to
+    ``standard_cell``."""
     base = standard_cell(num_cells=num_cells, seed=seed, utilisation=utilisation,
-                         target_density=target_density, bins=bins)
+                         target_density=target_density, bins=bins, **cell_options)
     rng = np.random.default_rng(seed + 1000)
     side = base.core()[2]
     nm, nf = num_movable_macros, num_fixed_macros
-    ms = np.exp(rng.uniform(np.log(0.02 * side), np.log(0.08 * side), nm + nf))
+    lo, hi = (0.02 * side, 0.08 * side) if macro_rows is None else macro_rows
+    ms = np.exp(rng.uniform(np.log(lo), np.log(hi), nm + nf))
     ms = np.maximum(np.rint(ms), 2.0)
     aspect = np.where(rng.random(nm + nf) < 0.5, 1.0, 2.0)
     mw, mh = ms * aspect, ms
@@ -376,6 +379,16 @@ def mixed_size(num_cells=20_000, num_movable_macros=12, num_fixed_macros=4, seed
         term_is_ni=np.zeros(t_old + nf, np.uint8), net_start=_i32(net_start),
         pin_owner=_i32(owner), pin_dx=_f32(dx), pin_dy=_f32(dy), target_density=target_density,
         bins=bins, meta=dict(generator="mixed_size", seed=seed), **rows)
+
+
+def config3(seed=31):
+    """The ePlace-MS workload: 1M standard cells as ``standard_cell`` draws
+    them, 300 movable macros (square or 2:1, side 50-400 rows, log-uniform)
+    and 50 fixed macros inside the core, nets with the same degree law (1.1M
+    with the macros' own), utilisation 0.75, 1024 x 1024 bins."""
+    return mixed_size(1_000_000, 300, 50, seed=seed, utilisation=0.75, target_density=1.0, bins=1024,
+                      macro_rows=(50.0, 400.0), num_nets=1_100_000, num_terminals=4_000,
+                      every_cell_pinned=True, local_pads=True)
 
 
 def blob_start(nl, seed=3, sigma_frac=0.05):
