@@ -79,16 +79,19 @@ def _overlap_pairs(a, b, same=False):
     return out
 
 
-def check(nl, cx, cy, fixed_macro=None, max_report=10, macros_only=False):
+def check(nl, cx, cy, fixed_macro=None, max_report=10, macros_only=False, macros_vs_fixed=True):
     """Legality of movable-node centres (cx, cy) on netlist nl.
 
     fixed_macro: optional bool array over nodes marking macros that count as
     fixed obstacles (they are checked for overlap with one another and with
     the cells but not for row alignment).  Movable nodes taller than one row
     are macros.  macros_only: only the macro tests (after macro legalization,
-    before the cells are legalized).  Returns a dict: counts per violation
-    kind, the first few offending node indices per kind, and legal (no
-    violation at all)."""
+    before the cells are legalized).  macros_vs_fixed=False leaves out the
+    overlap of movable macros with fixed objects (counted apart, as
+    "macro_fixed_overlap"): the reference's SA macro legalizer does not see
+    the fixed objects (Legalization/legalizer.h:305-307).  Returns a dict: counts
+    per violation kind, the first few offending node indices per kind, and
+    legal (no violation at all)."""
     n = nl.num_nodes
     cx = np.asarray(cx, np.float32)[:n]
     cy = np.asarray(cy, np.float32)[:n]
@@ -155,14 +158,16 @@ def check(nl, cx, cy, fixed_macro=None, max_report=10, macros_only=False):
         bad["fixed_overlap"].append(int(cell_idx[i]))
     for i, j in _overlap_pairs(macs, macs, same=True):
         bad["macro_overlap"].append(int(mac_idx[j]))
-    for i, _ in _overlap_pairs(macs, terms):
-        bad["macro_overlap"].append(int(mac_idx[i]))
+    vs_fixed = [int(mac_idx[i]) for i, _ in _overlap_pairs(macs, terms)]
+    if macros_vs_fixed:
+        bad["macro_overlap"] += vs_fixed
     core_x0, core_y0 = RX.min(), RY.min()
     core_x1, core_y1 = RU.max(), (RY + RH).max()
     for i in mac_idx:
         if X[i] < core_x0 or Y[i] < core_y0 or X[i] + W[i] > core_x1 or Y[i] + H[i] > core_y1:
             bad["outside_core"].append(int(i))
-    out = {"legal": not any(bad.values()), "scale_bits": s, "cells": int(cell.sum()), "macros": int(macro.sum())}
+    out = {"legal": not any(bad.values()), "scale_bits": s, "cells": int(cell.sum()), "macros": int(macro.sum()),
+           "macro_fixed_overlap": len(set(vs_fixed))}
     for k, v in bad.items():
         out[k] = len(set(v))
         out[k + "_first"] = sorted(set(v))[:max_report]

@@ -19,7 +19,7 @@ computes on the same netlist and starting positions:
     (record_flows);
   * reference_runs.json (--bench): the whole runs on bench.py's design.
 
-    python tests/golden/make_golden.py [--variants-only] [--bench]
+    python tests/golden/make_golden.py [--variants-only] [--bench] [--config3]
 """
 import os
 import sys
@@ -258,6 +258,43 @@ def record_flows():
     print("flows:", {k: (float(v) if np.ndim(v) == 0 else np.shape(v)) for k, v in out.items()})
 
 
+def record_config3():
+    """The reference's mixed-size flow on config 3 (synth.config3: 1M cells,
+    300 movable + 50 fixed macros, 1024 x 1024 bins) from a seeded blob
+    start: initialization, mGP, SAMacroLegalizer, FILLERONLY, cGP
+    (main/ePlace_main.cpp:174-211), with each stage's iterations, overflow,
+    HPWL and seconds.  Half an hour of CPU; written to config3_flow.json."""
+    import json
+    import time
+    nl = synth.blob_start(synth.config3())
+    ref = R.RefPlacer(nl)
+    out = {}
+    t0 = time.time()
+    ref.initialization(nl.target_density)
+    out["init_seconds"] = time.time() - t0
+    i = ref.info()
+    out.update(fillers=int(i["num_fillers"]), bins=int(i["bins_x"]))
+    for stage, run in (("mgp", None), ("mlg", None), ("fo", None), ("cgp", None)):
+        t0 = time.time()
+        if stage == "mlg":
+            ref.macro_legalize(nl.target_density)
+            out["mlg_seconds"] = time.time() - t0
+            out["mlg_hpwl"] = float(ref.hpwl())
+            continue
+        if stage == "fo":
+            ref.switch_filler_only()
+        elif stage == "cgp":
+            ref.switch_cgp()
+        r = run_stage(ref)
+        out[stage] = dict(iterations=int(r["iterations"]), overflow=float(r["overflow"]), hpwl=float(r["hpwl"]),
+                          seconds=time.time() - t0)
+        print(stage, out[stage], flush=True)
+    ref.close()
+    out["note"] = "reference CPU path, 1 thread, from synth.blob_start(synth.config3())"
+    with open(os.path.join(HERE, "config3_flow.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def qp_with_trace(ref):
     """QPPlacer::quadraticPlacement with its per-round log line captured:
     [(round, max(xError, yError) as printed, HPWL after the round)]."""
@@ -331,3 +368,5 @@ if __name__ == "__main__":
     record_flows()
     if "--bench" in sys.argv:
         record_bench_reference()
+    if "--config3" in sys.argv:
+        record_config3()

@@ -6,8 +6,8 @@ run.  TEST INFRASTRUCTURE ONLY.
 
     python tests/ref_stages.py <design> <in.npz> <out.npz> <stage> [<stage> ...]
 
-design: smoke:<seed> (synth.smoke) or mixed_5k (the golden mixed-size
-design); in.npz holds cx, cy (movable-node centres) and target_density;
+design: smoke:<seed> (synth.smoke), mixed_5k (the golden mixed-size
+design) or config3 (synth.config3 from its seeded blob); in.npz holds cx, cy (movable-node centres) and target_density;
 stages, in order: mlg (SAMacroLegalizer), abacus (AbacusLegalizer),
 detailed (DetailedPlacer).  out.npz gets <stage>_cx, <stage>_cy,
 <stage>_hpwl and <stage>_seconds after each stage.
@@ -28,6 +28,8 @@ def design(name):
         return synth.smoke(int(name.split(":")[1]))
     if name == "mixed_5k":
         return synth.blob_start(synth.mixed_size(5000, 6, 3, seed=5))
+    if name == "config3":
+        return synth.blob_start(synth.config3())
     raise ValueError(name)
 
 
@@ -38,7 +40,7 @@ def run(design_name, cx, cy, target_density, stages, tmpdir):
     np.savez(src, cx=np.asarray(cx, np.float32), cy=np.asarray(cy, np.float32),
              target_density=np.float32(target_density))
     r = subprocess.run([sys.executable, os.path.abspath(__file__), design_name, src, dst, *stages],
-                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+                       cwd=ROOT, capture_output=True, text=True, timeout=1800)
     out = dict(np.load(dst)) if r.returncode == 0 and os.path.exists(dst) else {}
     return r.returncode, out
 
