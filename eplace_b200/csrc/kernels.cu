@@ -923,14 +923,14 @@ __global__ void k_wrap_up(Grid g, int n, const uint8_t *__restrict__ flags, cons
 
 // ------------------------------------------------------------- launchers --
 int launch_priority(bool high) {
-    static int lo = 1, hi = 1;
-    if (lo > 0) {
+    // the range is the same on every device; a function-local static is
+    // initialised once even when engines are created on several threads
+    static const int2 range = [] {
         int l = 0, h = 0;
         cudaDeviceGetStreamPriorityRange(&l, &h);
-        hi = h;
-        lo = l;
-    }
-    return high ? hi : lo;
+        return make_int2(l, h);
+    }();
+    return high ? range.y : range.x;
 }
 
 int prep_blocks(const Grid &g) { return std::min(blocks_for(g.nx * g.ny, kThreads), 148 * 8); }

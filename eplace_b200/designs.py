@@ -93,10 +93,10 @@ def engine_batch(netlists, device=0, max_steps=0, **params):
     from . import placer
     engines = []
     try:
-        for nl in netlists:
-            p = placer.default_params(target_density=float(nl.target_density), device=device, **params)
-            e = placer.Engine(nl, p)
-            engines.append(e)
+        engines = placer.create_engines(
+            netlists, [placer.default_params(target_density=float(nl.target_density), device=device, **params)
+                       for nl in netlists])
+        for e in engines:
             e.initialize()
         stats = placer.run_batch(engines, max_steps=max_steps)
         out = []

@@ -364,6 +364,32 @@ class BookshelfDesign:
             pass
 
 
+def create_engines(netlists, params, threads=0):
+    """One Engine per netlist (params: one Params, or one per netlist), built
+    on a pool of host threads: ep_create's host set-up of one design runs
+    beside another's (ctypes releases the interpreter lock for the call).
+    threads 0: up to 8, at most one per design.  Each engine is what
+    Engine(nl, p) gives alone (its fillers come from its own seed)."""
+    import concurrent.futures as cf
+    plist = params if isinstance(params, (list, tuple)) else [params] * len(netlists)
+    n = threads if threads > 0 else min(8, os.cpu_count() or 1, max(1, len(netlists)))
+    if n <= 1:
+        return [Engine(nl, p) for nl, p in zip(netlists, plist)]
+    with cf.ThreadPoolExecutor(max_workers=n) as ex:
+        futs = [ex.submit(Engine, nl, p) for nl, p in zip(netlists, plist)]
+        engines, err = [], None
+        for f in futs:
+            try:
+                engines.append(f.result())
+            except Exception as x:  # close the others, then raise the first error
+                err = err or x
+        if err is not None:
+            for e in engines:
+                e.close()
+            raise err
+    return engines
+
+
 def run_batch(engines, max_steps=0):
     """ep_run_batch: the optimizer loops of several engines at once (each
     engine initialized first); returns one run-stats dict per engine."""

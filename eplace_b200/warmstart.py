@@ -92,13 +92,12 @@ def place_designs(netlists, precision=placer.PREC_MIXED):
     """QP then mGP for every netlist (mGP runs batched); returns the engines
     (positions at their mGP result), the training targets [num_nodes, 4]
     (QP centre, final centre) and the run statistics."""
-    engines, qp_xy = [], []
-    for nl in netlists:
-        e = placer.Engine(nl, placer.default_params(target_density=1.0, precision=precision))
+    engines = placer.create_engines(netlists, placer.default_params(target_density=1.0, precision=precision))
+    qp_xy = []
+    for nl, e in zip(netlists, engines):
         e.quadratic_placement()
         qp_xy.append(e.get_positions()[:nl.num_nodes])
         e.initialize()
-        engines.append(e)
     stats = placer.run_batch(engines)
     targets = [np.concatenate([q, e.get_positions()[:nl.num_nodes]], 1)
                for q, e, nl in zip(qp_xy, engines, netlists)]
