@@ -11,6 +11,7 @@
 // object -> pins) and the loop of kernels.cu / dct.cu runs there.
 #include <algorithm>
 #include <future>
+#include <thread>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -539,6 +540,32 @@ const char *ep_last_error(const ep_engine *e) { return e ? e->err.c_str() : "nul
 
 // ep_create's body; the host arrays it builds may throw std::bad_alloc,
 // which ep_create turns into EP_ERR_NOMEM.
+extern "C++" {
+// Host threads for a loop over n items (pins or nets): one per 100k items,
+// at most 8 and at most the hardware's.
+static int host_threads(long long n) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return (int)std::max<long long>(1, std::min<long long>({8LL, (long long)hw, n / 100000 + 1}));
+}
+
+// fn(thread, begin, end) over `nth` contiguous ranges of [0, n), the first
+// on the calling thread.
+template <typename F>
+static void parallel_ranges(int n, int nth, F &&fn) {
+    if (nth <= 1 || n < 2) {
+        fn(0, 0, n);
+        return;
+    }
+    std::vector<std::future<void>> jobs;
+    for (int t = 1; t < nth; t++)
+        jobs.push_back(std::async(std::launch::async, [&fn, t, n, nth] {
+            fn(t, (int)((long long)n * t / nth), (int)((long long)n * (t + 1) / nth));
+        }));
+    fn(0, 0, (int)((long long)n / nth));
+    for (auto &j : jobs) j.get();
+}
+}  // extern "C++"
+
 // Ascending sort of non-negative floats (the node areas) by their bit
 // patterns, which order like the values: three 11-bit LSD radix passes.
 // Anything else (a negative or NaN area) goes through std::sort.
@@ -849,25 +876,45 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
 
     // ---- pins: net CSR and the object -> pin CSR (pins in id order) ----
     lap(1);
+    // ---- pins: net CSR and the object -> pin CSR (pins in id order) ----
+    // Host loops over pins and nets run on `nth` threads in contiguous
+    // ranges; every result is what the sequential loops give.
+    const int nth = host_threads(np);
     std::vector<int32_t> owner(np), net_start(nnet + 1, 0);
     std::vector<float2> off(np);
     for (int n = 0; n <= nnet; n++) net_start[n] = nnet > 0 ? nl->net_start[n] : 0;
-    for (int p = 0; p < np; p++) {
-        int ow = nl->pin_owner[p];
-        owner[p] = ow < nn ? ow : no + (ow - nn);  // terminals follow all objects
-        off[p] = make_float2(nl->pin_dx[p], nl->pin_dy[p]);
-        if (ow < nn) h_npins[ow] += 1.0f;
-    }
+    parallel_ranges(np, nth, [&](int, int p0, int p1) {
+        for (int p = p0; p < p1; p++) {
+            const int ow = nl->pin_owner[p];
+            owner[p] = ow < nn ? ow : no + (ow - nn);  // terminals follow all objects
+            off[p] = make_float2(nl->pin_dx[p], nl->pin_dy[p]);
+        }
+    });
     // each object's pins in the reference's pin order (pin_slot: place of a
-    // pin in that list), so the gradient sum runs in the reference's order
+    // pin in that list), so the gradient sum runs in the reference's order:
+    // a counting sort, each thread's range of pins starting where the
+    // previous ranges' pins of the same object end
     std::vector<int32_t> ops(no + 1, 0), pin_slot(np, -1);
-    for (int p = 0; p < np; p++)
-        if (owner[p] < no) ops[owner[p] + 1]++;
-    for (int o = 0; o < no; o++) ops[o + 1] += ops[o];
     {
-        std::vector<int32_t> fill(ops.begin(), ops.end() - 1);
-        for (int p = 0; p < np; p++)
-            if (owner[p] < no) pin_slot[p] = fill[owner[p]]++;
+        std::vector<std::vector<int32_t>> cnt(nth, std::vector<int32_t>(no, 0));
+        parallel_ranges(np, nth, [&](int t, int p0, int p1) {
+            for (int p = p0; p < p1; p++)
+                if (owner[p] < no) cnt[t][owner[p]]++;
+        });
+        for (int o = 0; o < no; o++) {
+            int32_t at = 0;
+            for (int t = 0; t < nth; t++) {
+                const int32_t c = cnt[t][o];
+                cnt[t][o] = at;  // this thread's first slot, relative to the object's start
+                at += c;
+            }
+            ops[o + 1] = ops[o] + at;
+            if (o < nn) h_npins[o] = (float)at;
+        }
+        parallel_ranges(np, nth, [&](int t, int p0, int p1) {
+            for (int p = p0; p < p1; p++)
+                if (owner[p] < no) pin_slot[p] = ops[owner[p]] + cnt[t][owner[p]]++;
+        });
     }
     // Device pin order for the per-net pass (kernels.cu): nets above
     // kWarpPins pins first, largest first (a warp each), then degree
@@ -886,16 +933,17 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         std::stable_sort(big_list.begin(), big_list.end(), [&](int a, int b) {
             return net_start[a + 1] - net_start[a] > net_start[b + 1] - net_start[b];
         });
+        // nets in device order with their first device pin, then the copy
+        std::vector<int> order;
+        std::vector<int32_t> first;
+        order.reserve(nnet);
+        first.reserve(nnet);
         int q = 0;
         auto put_net = [&](int n) {
-            int a = net_start[n], deg = net_start[n + 1] - a;
-            for (int k = 0; k < deg; k++) {
-                dev_owner[q + k] = owner[a + k];
-                dev_off[q + k] = off[a + k];
-                dev_of_pin[a + k] = q + k;
-            }
-            int at = q;
-            q += deg;
+            order.push_back(n);
+            first.push_back(q);
+            const int at = q;
+            q += net_start[n + 1] - net_start[n];
             return at;
         };
         e->n_big_nets = (int)big_list.size();
@@ -906,11 +954,21 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
         for (int d = kWarpPins; d >= 1; d--) {
             const size_t per = kWarpPins / d;
             for (size_t i = 0; i < by_deg[d].size(); i += per) {
-                int first = q, count = (int)std::min(per, by_deg[d].size() - i);
+                int at = q, count = (int)std::min(per, by_deg[d].size() - i);
                 for (int j = 0; j < count; j++) put_net(by_deg[d][i + j]);
-                net_tasks.push_back(make_int4(d, first, count, (65536 + d - 1) / d));
+                net_tasks.push_back(make_int4(d, at, count, (65536 + d - 1) / d));
             }
         }
+        parallel_ranges((int)order.size(), nth, [&](int, int i0, int i1) {
+            for (int i = i0; i < i1; i++) {
+                const int n = order[i], a = net_start[n], deg = net_start[n + 1] - a, at = first[i];
+                for (int k = 0; k < deg; k++) {
+                    dev_owner[at + k] = owner[a + k];
+                    dev_off[at + k] = off[a + k];
+                    dev_of_pin[a + k] = at + k;
+                }
+            }
+        });
     }
     // quadratic placement: nets in device order
     e->h_pin_owner = dev_owner;
@@ -920,21 +978,26 @@ static ep_status create_engine(ep_engine *e, const ep_netlist *nl, const ep_para
     e->h_net_first.assign(nnet, 0);
     e->h_net_deg.assign(nnet, 0);
     e->h_pin_net.assign(np, 0);
-    for (int n = 0; n < nnet; n++) {
-        const int a = net_start[n], d = net_start[n + 1] - a;
-        e->h_net_deg[n] = d;
-        if (d > 0) e->h_net_first[n] = dev_of_pin[a];
-        for (int k = 0; k < d; k++) e->h_pin_net[dev_of_pin[a + k]] = n;
-    }
-    // each object's pins (reference order) -> their device positions
-    std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0), pin_obj_slot(std::max(np, 1), -1);
-    for (int p = 0; p < np; p++)
-        if (pin_slot[p] >= 0) {
-            obj_pin_dev[pin_slot[p]] = dev_of_pin[p];
-            pin_obj_slot[dev_of_pin[p]] = pin_slot[p];
+    parallel_ranges(nnet, nth, [&](int, int n0, int n1) {
+        for (int n = n0; n < n1; n++) {
+            const int a = net_start[n], d = net_start[n + 1] - a;
+            e->h_net_deg[n] = d;
+            if (d > 0) e->h_net_first[n] = dev_of_pin[a];
+            for (int k = 0; k < d; k++) e->h_pin_net[dev_of_pin[a + k]] = n;
         }
+    });
+    // each object's pins (reference order) -> their device positions, and back
+    std::vector<int32_t> obj_pin_dev(std::max(ops[no], 1), 0), pin_obj_slot(std::max(np, 1), -1);
+    parallel_ranges(np, nth, [&](int, int p0, int p1) {
+        for (int p = p0; p < p1; p++)
+            if (pin_slot[p] >= 0) {
+                obj_pin_dev[pin_slot[p]] = dev_of_pin[p];
+                pin_obj_slot[dev_of_pin[p]] = pin_slot[p];
+            }
+    });
 
     // stage views (EPlace/eplace.cpp:190-203)
+    for (int v = 0; v < 3; v++) e->h_view[v].reserve(no);
     for (int o = 0; o < no; o++) {
         e->h_view[EP_STAGE_MGP].push_back(o);
         if (o >= nn) e->h_view[EP_STAGE_FILLERONLY].push_back(o);
