@@ -283,34 +283,34 @@ __global__ void k_net_mean_t_add(Net g, const float *__restrict__ inv_deg, const
 
 // ------------------------------------------------------------ dense -------
 // Y[r][o] = relu(b[o] + sum_k X[r][k] W[o][k]) with X = [XA (KA cols) | XB
-// (KB cols)], W BF16 [kH][KA+KB].  kDenseRows rows per 256-thread block: W
-// (as float, rows padded to K + 1) and the block's rows (transposed, padded
-// to kDenseRows + 1) staged in shared memory, both without bank conflicts;
-// thread (tx, ty) accumulates rows ty + 32 j (j < 4) x outputs 8 tx .. 8 tx +
-// 7 in registers, k in order, so each output is the same sum as a plain
-// loop over k.
+// (KB cols)], W the BF16 weights, read here from their FP32 transposed copy
+// Wt[k][o] (k_transpose_w).  kDenseRows rows per 256-thread block: Wt and
+// the block's rows (row-major, padded to K + 1) staged in shared memory;
+// thread (tx, ty) accumulates rows 4 ty .. 4 ty + 3 x outputs 8 tx .. 8 tx + 7
+// in registers, k in order (two 16-byte weight loads and four row loads per
+// 32 FMAs, without bank conflicts), so each output is the same sum as a
+// plain loop over k.
 constexpr int kDenseRows = 128;
 template <int KA, int KB>
 __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ XA, const float *__restrict__ XB,
-                                              const __nv_bfloat16 *__restrict__ W, const float *__restrict__ b,
+                                              const float *__restrict__ Wt, const float *__restrict__ b,
                                               float *__restrict__ Y) {
-    constexpr int K = KA + KB, WP = K + 1, XP = kDenseRows + 1;
+    constexpr int K = KA + KB, XP = K + 1;
     extern __shared__ float sm[];
-    float *Ws = sm;           // [kH][WP]
-    float *Xt = sm + kH * WP;  // [K][XP]
-    for (int i = threadIdx.x; i < kH * K; i += kT) {
-        const int o = i / K, k = i - o * K;
-        Ws[o * WP + k] = bf(W[i]);
-    }
+    float *Ws = sm;            // [K][kH]
+    float *Xs = sm + K * kH;   // [kDenseRows][XP]
+    for (int i = threadIdx.x; i < K * kH / 4; i += kT)
+        reinterpret_cast<float4 *>(Ws)[i] = reinterpret_cast<const float4 *>(Wt)[i];
     const int r0 = blockIdx.x * kDenseRows;
     for (int i = threadIdx.x; i < kDenseRows * K; i += kT) {
         const int r = i / K, k = i - r * K, row = r0 + r;
         float v = 0.f;
         if (row < N) v = k < KA ? XA[(size_t)row * KA + k] : XB[(size_t)row * KB + (k - KA)];
-        Xt[k * XP + r] = v;
+        Xs[r * XP + k] = v;
     }
     __syncthreads();
     const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
     float acc[4][8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {
@@ -320,11 +320,11 @@ __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ X
     }
 #pragma unroll 4
     for (int k = 0; k < K; k++) {
-        float x[4], w[8];
+        float x[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) x[i] = Xt[k * XP + ty + 32 * i];
-#pragma unroll
-        for (int j = 0; j < 8; j++) w[j] = Ws[(tx * 8 + j) * WP + k];
+        for (int i = 0; i < 4; i++) x[i] = Xs[(ty * 4 + i) * XP + k];
+        const float4 wa = W4[k * (kH / 4) + tx * 2], wb = W4[k * (kH / 4) + tx * 2 + 1];
+        const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -332,11 +332,28 @@ __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ X
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int row = r0 + ty + 32 * i;
+        const int row = r0 + ty * 4 + i;
         if (row >= N) continue;
         float4 *y = reinterpret_cast<float4 *>(Y + (size_t)row * kH + tx * 8);
         y[0] = make_float4(fmaxf(acc[i][0], 0.f), fmaxf(acc[i][1], 0.f), fmaxf(acc[i][2], 0.f), fmaxf(acc[i][3], 0.f));
         y[1] = make_float4(fmaxf(acc[i][4], 0.f), fmaxf(acc[i][5], 0.f), fmaxf(acc[i][6], 0.f), fmaxf(acc[i][7], 0.f));
+    }
+}
+
+// The dense layers' BF16 weights as FP32, transposed to [k][o] (layer 0,
+// then layers 1..3), for k_dense.
+constexpr int kWt0 = 0, kWtL = kF * kH, kWtSize = kF * kH + kLayers * 2 * kH * kH;
+inline int wt_off(int l) { return l == 0 ? kWt0 : kWtL + (l - 1) * 2 * kH * kH; }
+__global__ void k_transpose_w(const __nv_bfloat16 *__restrict__ wb, float *__restrict__ wt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kWtSize) return;
+    if (i < kWtL) {
+        const int k = i / kH, o = i % kH;
+        wt[i] = bf(wb[kOffW0 + o * kF + k]);
+    } else {
+        const int l = (i - kWtL) / (2 * kH * kH) + 1, j = (i - kWtL) % (2 * kH * kH);
+        const int k = j / kH, o = j % kH;
+        wt[i] = bf(wb[kOffL + (l - 1) * kLayerParams + o * 2 * kH + k]);
     }
 }
 
@@ -566,6 +583,7 @@ struct ep_gnn {
     std::string err;
     float *w = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *wb = nullptr;
+    float *wt = nullptr;  // the dense layers' weights as FP32 [k][o] (k_transpose_w)
     double *loss = nullptr;
     int64_t step = 0;
     // bound netlist
@@ -599,7 +617,7 @@ namespace {
         }                                                                         \
     } while (0)
 
-size_t smem_dense(int K) { return sizeof(float) * ((size_t)kH * (K + 1) + (size_t)K * (kDenseRows + 1)); }
+size_t smem_dense(int K) { return sizeof(float) * ((size_t)K * kH + (size_t)kDenseRows * (K + 1)); }
 size_t smem_dx(int K) { return sizeof(float) * ((size_t)kH * K + 64 * (size_t)(kH + 1)); }
 
 void set_smem_attrs() {
@@ -767,12 +785,13 @@ ep_status forward(ep_gnn *g) {
     cudaStream_t st = g->eg.st;
     const float *w = g->w;
     const __nv_bfloat16 *wb = g->wb;
-    k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, wb + kOffW0, w + kOffB0, g->h[0]);
+    k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, g->wt + wt_off(0), w + kOffB0,
+                                                                    g->h[0]);
     for (int l = 1; l <= kLayers; l++) {
         k_net_mean<<<n.n_big + nblk(n.nnet - n.n_big, kBigWarps), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
                                                                 (float2 *)g->a);
         k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
-        k_dense<kH, kH><<<nblk(N, kDenseRows), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], wb + off_w(l),
+        k_dense<kH, kH><<<nblk(N, kDenseRows), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], g->wt + wt_off(l),
                                                                      w + off_b(l), g->h[l]);
     }
     k_output<<<nblk(N), kT, 0, st>>>(N, g->h[kLayers], wb + kOffW4, w + kOffB4, g->v, g->raw, g->pred);
@@ -856,6 +875,7 @@ ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) try {
         cudaMalloc(&g->adam_m, sizeof(float) * kParams) != cudaSuccess ||
         cudaMalloc(&g->adam_v, sizeof(float) * kParams) != cudaSuccess ||
         cudaMalloc(&g->wb, sizeof(__nv_bfloat16) * kParams) != cudaSuccess ||
+        cudaMalloc(&g->wt, sizeof(float) * kWtSize) != cudaSuccess ||
         cudaMalloc(&g->loss, sizeof(double)) != cudaSuccess) {
         g->err = "cudaMalloc failed for the network's weights";
         return EP_ERR_NOMEM;
@@ -882,7 +902,7 @@ void ep_gnn_destroy(ep_gnn *g) {
     cudaDeviceSynchronize();
     for (void *p : g->ws) cudaFree(p);
     for (void *p : {(void *)g->w, (void *)g->grad, (void *)g->adam_m, (void *)g->adam_v, (void *)g->wb,
-                    (void *)g->loss})
+                    (void *)g->wt, (void *)g->loss})
         if (p) cudaFree(p);
     delete g;
 }
@@ -899,6 +919,7 @@ ep_status ep_gnn_set_weights(ep_gnn *g, const float *w) {
     GK(cudaMemset(g->adam_m, 0, sizeof(float) * kParams));
     GK(cudaMemset(g->adam_v, 0, sizeof(float) * kParams));
     k_to_bf16<<<nblk(kParams), kT>>>(kParams, g->w, g->wb);
+    k_transpose_w<<<nblk(kWtSize), kT>>>(g->wb, g->wt);
     GK(cudaGetLastError());
     GK(cudaDeviceSynchronize());
     g->step = 0;
@@ -964,6 +985,7 @@ ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target4, float
     g->step++;
     const float c1 = 1.f / (1.f - std::pow(0.9f, (float)g->step)), c2 = 1.f / (1.f - std::pow(0.999f, (float)g->step));
     k_adam<<<nblk(kParams), kT, 0, g->eg.st>>>(kParams, g->w, g->grad, g->adam_m, g->adam_v, lr, c1, c2, g->wb);
+    k_transpose_w<<<nblk(kWtSize), kT, 0, g->eg.st>>>(g->wb, g->wt);
     GK(cudaGetLastError());
     if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, g->eg.st));
     GK(cudaStreamSynchronize(g->eg.st));

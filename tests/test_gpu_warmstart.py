@@ -53,6 +53,8 @@ def test_trained_start_against_qp_and_an_untrained_network():
     bare = dict(start, rounds=0)
     trained = placer.Gnn(weights=w)
     untrained = placer.Gnn(seed=123)
+    # a network's first proposal allocates its workspace: not part of a start
+    _learned_run(trained, warmstart.design(60_000, 4999), start)
     ratios, ratios_untrained, t_learned, t_qp = [], [], [], []
     for s in SEEDS:
         nl = warmstart.design(60_000, s)
