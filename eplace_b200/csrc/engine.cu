@@ -2088,7 +2088,8 @@ ep_status qp_setup(ep_engine *e) {
         (s = dalloc(e, q.rhs, nn)) || (s = dalloc(e, q.x, nn)) || (s = dalloc(e, q.r, nn)) ||
         (s = dalloc(e, q.r0, nn)) || (s = dalloc(e, q.p, nn)) || (s = dalloc(e, q.v, nn)) ||
         (s = dalloc(e, q.s, nn)) || (s = dalloc(e, q.t, nn)) || (s = dalloc(e, q.partials, 4 * (size_t)pb)) ||
-        (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)) || (s = dalloc(e, q.solve, 1)))
+        (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)) || (s = dalloc(e, q.solve, 1)) ||
+        (s = dalloc(e, q.scan, (size_t)qp_scan_blocks(nn) + 2)))
         return s;
     q.pin_net = e->pin_net;
     q.net_first = e->net_first;
@@ -2099,6 +2100,7 @@ ep_status qp_setup(ep_engine *e) {
     CK(cudaMallocHost((void **)&e->qp_out_h, 4 * sizeof(double)));
     CK(cudaMallocHost((void **)&e->qp_state_h, sizeof(QpSolve)));
     e->qp_cap_x = e->qp_cap_y = cap;
+    q.cap_x = q.cap_y = (int)std::min<size_t>(cap, (size_t)INT32_MAX);
     e->qp_ready = true;
     return EP_OK;
 }
@@ -2112,25 +2114,13 @@ ep_status qp_read(ep_engine *e, int n) {
 
 // Build both systems at the current centres: count, prefix sum, fill.
 ep_status qp_build(ep_engine *e, const float2 *qpos) {
+    // counts, the CSR offsets by a scan on the device, then the entries: no
+    // host round trip (an allocation overflow is flagged in the solver state
+    // and reported by qp_solve)
     QpDev &q = e->qp;
-    const int nn = q.nn;
     qp_rows(q, 0, qpos, e->st);
-    std::vector<int32_t> cnt(2 * (size_t)nn), rx(nn + 1), ry(nn + 1);
-    CK(cudaMemcpyAsync(cnt.data(), q.count, cnt.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, e->st));
-    CK(cudaStreamSynchronize(e->st));
-    rx[0] = ry[0] = 0;
-    for (int i = 0; i < nn; i++) {
-        rx[i + 1] = rx[i] + cnt[i];
-        ry[i + 1] = ry[i] + cnt[nn + i];
-    }
-    if ((size_t)rx[nn] > e->qp_cap_x || (size_t)ry[nn] > e->qp_cap_y) {
-        e->err = "quadratic placement: more matrix entries than the bound allows";
-        return EP_ERR_STATE;
-    }
-    CK(cudaMemcpyAsync(q.row_x, rx.data(), rx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
-    CK(cudaMemcpyAsync(q.row_y, ry.data(), ry.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->st));
+    qp_offsets(q, e->st);
     qp_rows(q, 1, qpos, e->st);
-    CK(cudaStreamSynchronize(e->st));  // the host vectors above go out of scope
     CK(cudaGetLastError());
     return EP_OK;
 }
@@ -2156,6 +2146,10 @@ ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, double err[2], 
         CK(cudaMemcpyAsync(e->qp_state_h, q.solve, sizeof(QpSolve), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         h = *e->qp_state_h;
+        if (h.overflow) {
+            e->err = "quadratic placement: more matrix entries than the bound allows";
+            return EP_ERR_STATE;
+        }
         if (!h.active[0] && !h.active[1]) break;
     }
     CK(cudaGetLastError());

@@ -210,6 +210,7 @@ struct QpSolve {
     double rho[2], rho_old[2], alpha[2], w[2], r0sq[2], rr[2], bb[2], tol2[2], r0r[2];
     int it[2], restarts[2], active[2];
     int restart_mask, zero_mask, iters, max_it;
+    int overflow;  // the last matrix build needed more entries than allocated
 };
 // Device view of one engine's quadratic placement: the netlist in device pin
 // order (nets contiguous) plus the per-round systems and BiCGSTAB vectors,
@@ -234,9 +235,14 @@ struct QpDev {
     unsigned *cnt;
     double *out;      // [4] sums of the last reduction (bounds: HPWL)
     QpSolve *solve;   // device BiCGSTAB state
+    int32_t *scan;    // [qp_scan_blocks + 2] chunk totals of the row counts, then the two totals
+    int cap_x, cap_y; // entries allocated per system
 };
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st);
 void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st);
+// CSR row offsets of both systems from the counts, on the device
+void qp_offsets(const QpDev &q, cudaStream_t st);
+int qp_scan_blocks(int nn);
 // r = b - A x and the solver's initial state (zero right-hand sides give x = 0)
 void qp_init(const QpDev &q, int max_it, cudaStream_t st);
 // enqueue `count` BiCGSTAB iterations (no-ops once both axes have stopped)

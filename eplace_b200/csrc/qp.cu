@@ -202,6 +202,99 @@ __device__ __forceinline__ bool is_long(const PartnerRange &r) {
     return r.end - (r.skip >= 0) + (r.extra >= 0) > kLongPartners;
 }
 
+// ---- CSR row offsets on the device ------------------------------------------
+// The counts of both systems lie in one array c[0 .. 2 nn) (X rows, then Y
+// rows); with E the exclusive prefix sum of c over [0, 2 nn], row_x[i] =
+// E[i] (i <= nn) and row_y[i] = E[nn + i] - E[nn].  Three passes over
+// chunks of kScanChunk entries: chunk totals; one block scanning the totals
+// (and finding E[nn], E[2 nn]); each chunk's prefix sums.  Integer sums:
+// the same offsets the host loop gave.
+constexpr int kScanItems = 4, kScanChunk = kQT * kScanItems;
+
+__device__ __forceinline__ int block_excl_scan(int v, int &total) {
+    __shared__ int warp_tot[kQT / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int k = 0; k < kQT / 32; k++) {
+        if (k < w) before += warp_tot[k];
+        total += warp_tot[k];
+    }
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kQT) k_qp_chunk_sums(const int32_t *__restrict__ c, int n2, int32_t *__restrict__ sums) {
+    const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
+    int v = 0;
+#pragma unroll
+    for (int u = 0; u < kScanItems; u++) v += base + u < n2 ? c[base + u] : 0;
+    int total;
+    block_excl_scan(v, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of the chunk totals in place, then E[nn] and
+// E[2 nn] into sums[nb], sums[nb + 1], and the overflow flag
+__global__ void __launch_bounds__(kQT) k_qp_chunk_scan(int32_t *__restrict__ sums, int nb, const int32_t *__restrict__ c,
+                                                      int nn, int cap_x, int cap_y, QpSolve *__restrict__ S) {
+    __shared__ int carry_s;
+    int carry = 0;
+    for (int t0 = 0; t0 < nb; t0 += kQT) {
+        const int i = t0 + threadIdx.x;
+        const int v = i < nb ? sums[i] : 0;
+        int total;
+        const int ex = block_excl_scan(v, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
+    }
+    // E[nn]: the scanned total of nn's chunk plus that chunk's entries before nn
+    const int ch = nn / kScanChunk;
+    int part = 0;
+    for (int k = ch * kScanChunk + threadIdx.x; k < nn; k += kQT) part += c[k];
+    int total;
+    block_excl_scan(part, total);
+    if (threadIdx.x == 0) carry_s = carry;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int enn = sums[ch] + total;
+        sums[nb] = enn;
+        sums[nb + 1] = carry_s;
+        S->overflow = enn > cap_x || carry_s - enn > cap_y;
+    }
+}
+
+__global__ void __launch_bounds__(kQT) k_qp_offsets(const int32_t *__restrict__ c, int nn, const int32_t *__restrict__ sums,
+                                                   int nb, int32_t *__restrict__ row_x, int32_t *__restrict__ row_y) {
+    const int n2 = 2 * nn, base = blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
+    int v[kScanItems], s = 0;
+#pragma unroll
+    for (int u = 0; u < kScanItems; u++) {
+        v[u] = base + u < n2 ? c[base + u] : 0;
+        s += v[u];
+    }
+    int total;
+    int e = sums[blockIdx.x] + block_excl_scan(s, total);
+    const int enn = sums[nb];
+#pragma unroll
+    for (int u = 0; u < kScanItems; u++) {
+        const int i = base + u;  // E[i] = e
+        if (i <= n2) {
+            if (i <= nn) row_x[i] = e;
+            if (i >= nn) row_y[i - nn] = e - enn;
+        }
+        e += v[u];
+    }
+}
+
 // One movable node's row of both systems: counts (fill = 0) or entries,
 // diagonal and right-hand side (fill = 1).  A thread per node takes its pins'
 // short partner sets in pin order; then the warp takes the long ones (a bound
@@ -215,7 +308,8 @@ k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int
           const float2 *__restrict__ pos, int32_t *__restrict__ count, const int32_t *__restrict__ row_x,
           const int32_t *__restrict__ row_y, int32_t *__restrict__ col_x, float *__restrict__ val_x,
           int32_t *__restrict__ col_y, float *__restrict__ val_y, float2 *__restrict__ diag,
-          float2 *__restrict__ rhs) {
+          float2 *__restrict__ rhs, const QpSolve *__restrict__ S) {
+    if (fill && S->overflow) return;  // uniform: the offsets exceed the allocation, the solve reports it
     const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
     const bool valid = i < nn;  // every lane stays for the warp's long sets
     int cnt[2] = {0, 0};
@@ -682,7 +776,16 @@ void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st)
 void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
     k_qp_rows<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, fill, q.obj_pin_start, q.obj_pin_dev, q.pin_net, q.net_first,
                                              q.net_deg, q.bound, q.owner, q.off, pos, q.count, q.row_x, q.row_y,
-                                             q.col_x, q.val_x, q.col_y, q.val_y, q.diag, q.rhs);
+                                             q.col_x, q.val_x, q.col_y, q.val_y, q.diag, q.rhs, q.solve);
+}
+
+int qp_scan_blocks(int nn) { return (2 * nn + 1 + kScanChunk - 1) / kScanChunk; }
+
+void qp_offsets(const QpDev &q, cudaStream_t st) {
+    const int nb = qp_scan_blocks(q.nn);
+    k_qp_chunk_sums<<<nb, kQT, 0, st>>>(q.count, 2 * q.nn, q.scan);
+    k_qp_chunk_scan<<<1, kQT, 0, st>>>(q.scan, nb, q.count, q.nn, q.cap_x, q.cap_y, q.solve);
+    k_qp_offsets<<<nb, kQT, 0, st>>>(q.count, q.nn, q.scan, nb, q.row_x, q.row_y);
 }
 
 static QpMat mat(const QpDev &q) { return QpMat{q.row_x, q.col_x, q.row_y, q.col_y, q.val_x, q.val_y, q.diag}; }
