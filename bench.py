@@ -433,8 +433,9 @@ def main():
                "config": workload_config(nl, dict(
                    fillers=info.num_fillers, parallelism=f"replicas x{world}" if world > 1 else "1 GPU",
                    product=("learned warm start (ep_gnn_propose, alpha %.2f, then %d rounds of ep_quadratic_refine"
-                            " of at most %d solver iterations) + mixed-precision mGP"
-                            % (start["alpha"], start["rounds"], start["iters"])),
+                            " of at most %d%s solver iterations) + mixed-precision mGP"
+                            % (start["alpha"], start["rounds"], start["iters"],
+                               " Jacobi-preconditioned" if start.get("jacobi") else "")),
                    plain="device quadratic placement (%d rounds, the reference's count) + FP64 mGP" % qp_rounds,
                    mixed_precision="FP32 positions, FFT Poisson, gather and WA; int64 fixed-point density; "
                                    "FP64 reductions; network BF16 weights, FP32 accumulate",

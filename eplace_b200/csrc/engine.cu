@@ -2089,7 +2089,8 @@ ep_status qp_setup(ep_engine *e) {
         (s = dalloc(e, q.r0, nn)) || (s = dalloc(e, q.p, nn)) || (s = dalloc(e, q.v, nn)) ||
         (s = dalloc(e, q.s, nn)) || (s = dalloc(e, q.t, nn)) || (s = dalloc(e, q.partials, 4 * (size_t)pb)) ||
         (s = dalloc(e, q.cnt, 1)) || (s = dalloc(e, q.out, 4)) || (s = dalloc(e, q.solve, 1)) ||
-        (s = dalloc(e, q.scan, (size_t)qp_scan_blocks(nn) + 2)))
+        (s = dalloc(e, q.scan, (size_t)qp_scan_blocks(nn) + 2)) || (s = dalloc(e, q.y, nn)) ||
+        (s = dalloc(e, q.z, nn)) || (s = dalloc(e, q.dinv, nn)))
         return s;
     q.pin_net = e->pin_net;
     q.net_first = e->net_first;
@@ -2132,16 +2133,17 @@ ep_status qp_build(ep_engine *e, const float2 *qpos) {
 // The host enqueues iterations in chunks and reads the solver state once per
 // chunk.  err[c] = |r|/|b| at the end, the value QPPlacer reads as
 // solver.error().
-ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, double err[2], int &iters) {
+ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, bool jacobi, double err[2], int &iters) {
     QpDev &q = e->qp;
     cudaStream_t st = e->st;
     constexpr int kChunk = 10;
     qp_to_x(q, qpos, st);
+    if (jacobi) qp_dinv(q, st);
     qp_init(q, max_it, st);
     QpSolve h{};
     for (int done = 0; done < max_it;) {
         const int n = std::min(kChunk, max_it - done);
-        qp_iterations(q, n, st);
+        qp_iterations(q, n, jacobi, st);
         done += n;
         CK(cudaMemcpyAsync(e->qp_state_h, q.solve, sizeof(QpSolve), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -2168,7 +2170,7 @@ extern "C" {
 // max_iterations rounds from the current centres.  solver_its: BiCGSTAB
 // iterations per round (the reference's 100).
 static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool from_centre, int solver_its,
-                                     ep_qp_stats *stats) {
+                                     bool jacobi, ep_qp_stats *stats) {
     if (e->in_run) {
         e->err = "ep_quadratic_placement cannot run inside an optimizer run";
         return EP_ERR_STATE;
@@ -2194,7 +2196,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
     for (int i = 0;; i++) {
         if ((s = qp_build(e, qpos))) return s;
         int it = 0;
-        if ((s = qp_solve(e, qpos, solver_its, err, it))) return s;  // solver.setMaxIterations(100)
+        if ((s = qp_solve(e, qpos, solver_its, jacobi, err, it))) return s;  // solver.setMaxIterations(100)
         solver_iters += it;
         qp_from_x(q, e->grid, e->size, qpos, st);  // updateModuleLocation
         qp_bounds(q, qpos, q.out, st);             // calcNetBoundPins
@@ -2228,16 +2230,18 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
 ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_stats *stats) {
     if (!e) return EP_ERR_ARG;
     try {
-        return quadratic_placement(e, max_iterations, true, 100, stats);
+        return quadratic_placement(e, max_iterations, true, 100, false, stats);
     } catch (const std::bad_alloc &) {
         return host_oom(e);
     }
 }
 
-ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, ep_qp_stats *stats) {
-    if (!e || rounds < 1 || solver_iterations < 0) return EP_ERR_ARG;
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, int32_t preconditioner,
+                              ep_qp_stats *stats) {
+    if (!e || rounds < 1 || solver_iterations < 0 || preconditioner < 0 || preconditioner > 1) return EP_ERR_ARG;
     try {
-        return quadratic_placement(e, rounds, false, solver_iterations > 0 ? solver_iterations : 100, stats);
+        return quadratic_placement(e, rounds, false, solver_iterations > 0 ? solver_iterations : 100,
+                                   preconditioner == 1, stats);
     } catch (const std::bad_alloc &) {
         return host_oom(e);
     }

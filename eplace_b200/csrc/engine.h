@@ -231,6 +231,7 @@ struct QpDev {
     float *val_x, *val_y;
     float2 *diag, *rhs;
     float2 *x, *r, *r0, *p, *v, *s, *t;
+    float2 *y, *z, *dinv;  // Jacobi-preconditioned solves: M^-1 p, M^-1 s, 1 / diagonal
     double *partials;
     unsigned *cnt;
     double *out;      // [4] sums of the last reduction (bounds: HPWL)
@@ -246,7 +247,9 @@ int qp_scan_blocks(int nn);
 // r = b - A x and the solver's initial state (zero right-hand sides give x = 0)
 void qp_init(const QpDev &q, int max_it, cudaStream_t st);
 // enqueue `count` BiCGSTAB iterations (no-ops once both axes have stopped)
-void qp_iterations(const QpDev &q, int count, cudaStream_t st);
+void qp_iterations(const QpDev &q, int count, bool jacobi, cudaStream_t st);
+// 1 / diagonal of both systems (the Jacobi preconditioner), after a build
+void qp_dinv(const QpDev &q, cudaStream_t st);
 void qp_to_x(const QpDev &q, const float2 *pos, cudaStream_t st);
 void qp_from_x(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);
 void qp_center(const QpDev &q, const Grid &g, const float2 *size, float2 *pos, cudaStream_t st);

@@ -631,10 +631,11 @@ k_qp_restart(int nn, QpMat m, const float2 *__restrict__ rhs, const float2 *__re
     }
 }
 
-// p = r + beta (p - omega v)
+// p = r + beta (p - omega v); with a diagonal preconditioner (dinv, else
+// null) also y = M^-1 p, the vector the SpMV then takes
 __global__ void __launch_bounds__(kQT)
 k_qp_dir(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ p,
-         const QpSolve *__restrict__ S) {
+         const float2 *__restrict__ dinv, float2 *__restrict__ y, const QpSolve *__restrict__ S) {
     pdl_begin();
     if (!any_active(S)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -645,7 +646,12 @@ k_qp_dir(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, flo
         w[c] = S->active[c] ? (float)S->w[c] : 0.f;
     }
     const float2 ri = r[i], vi = v[i], pi = p[i];
-    p[i] = make_float2(ri.x + b[0] * (pi.x - w[0] * vi.x), ri.y + b[1] * (pi.y - w[1] * vi.y));
+    const float2 pn = make_float2(ri.x + b[0] * (pi.x - w[0] * vi.x), ri.y + b[1] * (pi.y - w[1] * vi.y));
+    p[i] = pn;
+    if (dinv) {
+        const float2 d = dinv[i];
+        y[i] = make_float2(pn.x * d.x, pn.y * d.y);
+    }
 }
 
 // v = A p; alpha = rho / (r0.v)
@@ -669,29 +675,34 @@ k_qp_av(int nn, QpMat m, const float2 *__restrict__ p, const float2 *__restrict_
         for (int c = 0; c < 2; c++) S->alpha[c] = S->active[c] ? S->rho[c] / acc[c] : 0.0;
 }
 
-// s = r - alpha v
+// s = r - alpha v; with the preconditioner also z = M^-1 s
 __global__ void __launch_bounds__(kQT)
 k_qp_s(int nn, const float2 *__restrict__ r, const float2 *__restrict__ v, float2 *__restrict__ s,
-       const QpSolve *__restrict__ S) {
+       const float2 *__restrict__ dinv, float2 *__restrict__ z, const QpSolve *__restrict__ S) {
     pdl_begin();
     if (!any_active(S)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
     const float ax = (float)S->alpha[0], ay = (float)S->alpha[1];
     const float2 ri = r[i], vi = v[i];
-    s[i] = make_float2(ri.x - ax * vi.x, ri.y - ay * vi.y);
+    const float2 si = make_float2(ri.x - ax * vi.x, ri.y - ay * vi.y);
+    s[i] = si;
+    if (dinv) {
+        const float2 d = dinv[i];
+        z[i] = make_float2(si.x * d.x, si.y * d.y);
+    }
 }
 
-// t = A s; omega = t.s / t.t
+// t = A z (z = s, or M^-1 s); omega = t.s / t.t
 __global__ void __launch_bounds__(kQT)
-k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, double *__restrict__ partials,
-        unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
+k_qp_at(int nn, QpMat m, const float2 *__restrict__ z, const float2 *__restrict__ s, float2 *__restrict__ t,
+        double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     pdl_begin();
     if (!any_active(S)) return;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     ROW_GROUPS(nn) {
-        const float2 ti = spmv_row8(m, s, i, sub, i < nn);
+        const float2 ti = spmv_row8(m, z, i, sub, i < nn);
         if (i < nn && sub == 0) {
             const float2 si = s[i];
             t[i] = ti;
@@ -706,11 +717,12 @@ k_qp_at(int nn, QpMat m, const float2 *__restrict__ s, float2 *__restrict__ t, d
             if (S->active[c]) S->w[c] = acc[c] > 0.0 ? acc[2 + c] / acc[c] : 0.0;
 }
 
-// x += alpha p + omega s; r = s - omega t; |r|^2, r0.r; convergence per axis.
+// x += alpha y + omega z (y, z = p, s, or their preconditioned forms);
+// r = s - omega t; |r|^2, r0.r; convergence per axis.
 __global__ void __launch_bounds__(kQT)
-k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, const float2 *__restrict__ t,
-          const float2 *__restrict__ r0, float2 *__restrict__ x, float2 *__restrict__ r, double *__restrict__ partials,
-          unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
+k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ zs, const float2 *__restrict__ s,
+          const float2 *__restrict__ t, const float2 *__restrict__ r0, float2 *__restrict__ x, float2 *__restrict__ r,
+          double *__restrict__ partials, unsigned *__restrict__ cnt, QpSolve *__restrict__ S) {
     __shared__ double sh[4 * 32];
     pdl_begin();
     if (!any_active(S)) return;
@@ -721,8 +733,8 @@ k_qp_step(int nn, const float2 *__restrict__ p, const float2 *__restrict__ s, co
     }
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
-        const float2 pi = p[i], si = s[i], ti = t[i], xi = x[i], z = r0[i];
-        x[i] = make_float2(xi.x + a[0] * pi.x + w[0] * si.x, xi.y + a[1] * pi.y + w[1] * si.y);
+        const float2 pi = p[i], zi = zs[i], si = s[i], ti = t[i], xi = x[i], z = r0[i];
+        x[i] = make_float2(xi.x + a[0] * pi.x + w[0] * zi.x, xi.y + a[1] * pi.y + w[1] * zi.y);
         const float2 ri = make_float2(si.x - w[0] * ti.x, si.y - w[1] * ti.y);
         r[i] = ri;
         acc[0] += (double)ri.x * ri.x;
@@ -796,19 +808,33 @@ void qp_init(const QpDev &q, int max_it, cudaStream_t st) {
     k_qp_zero<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.solve, q.x);
 }
 
-void qp_iterations(const QpDev &q, int count, cudaStream_t st) {
+// M^-1 of the Jacobi preconditioner: 1 / diagonal (1 where the diagonal is 0)
+__global__ void k_qp_dinv(int nn, const float2 *__restrict__ diag, float2 *__restrict__ dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const float2 d = diag[i];
+    dinv[i] = make_float2(d.x != 0.f ? 1.f / d.x : 1.f, d.y != 0.f ? 1.f / d.y : 1.f);
+}
+
+void qp_iterations(const QpDev &q, int count, bool jacobi, cudaStream_t st) {
     const int b = qblocks(q.nn), bm = qgrid(kRowLanes * q.nn), br = qgrid(q.nn);
     for (int k = 0; k < count; k++) {
         // programmatic serialisation: each kernel's blocks are resident and
         // waiting (pdl_begin) while the previous one drains
         launch_k(k_qp_restart, bm, kQT, 0, st, q.nn, mat(q), q.rhs, q.x, q.r, q.r0, q.partials, q.cnt, q.solve);
-        launch_k(k_qp_dir, b, kQT, 0, st, q.nn, q.r, q.v, q.p, q.solve);
-        launch_k(k_qp_av, bm, kQT, 0, st, q.nn, mat(q), q.p, q.r0, q.v, q.partials, q.cnt, q.solve);
-        launch_k(k_qp_s, b, kQT, 0, st, q.nn, q.r, q.v, q.s, q.solve);
-        launch_k(k_qp_at, bm, kQT, 0, st, q.nn, mat(q), q.s, q.t, q.partials, q.cnt, q.solve);
-        launch_k(k_qp_step, br, kQT, 0, st, q.nn, q.p, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
+        // Eigen's preconditioned form: y = M^-1 p and z = M^-1 s go into the
+        // SpMVs and the update; without a preconditioner y = p and z = s
+        const float2 *dinv = jacobi ? q.dinv : nullptr;
+        const float2 *y = jacobi ? q.y : q.p, *z = jacobi ? q.z : q.s;
+        launch_k(k_qp_dir, b, kQT, 0, st, q.nn, q.r, q.v, q.p, dinv, q.y, q.solve);
+        launch_k(k_qp_av, bm, kQT, 0, st, q.nn, mat(q), y, q.r0, q.v, q.partials, q.cnt, q.solve);
+        launch_k(k_qp_s, b, kQT, 0, st, q.nn, q.r, q.v, q.s, dinv, q.z, q.solve);
+        launch_k(k_qp_at, bm, kQT, 0, st, q.nn, mat(q), z, q.s, q.t, q.partials, q.cnt, q.solve);
+        launch_k(k_qp_step, br, kQT, 0, st, q.nn, y, z, q.s, q.t, q.r0, q.x, q.r, q.partials, q.cnt, q.solve);
     }
 }
+
+void qp_dinv(const QpDev &q, cudaStream_t st) { k_qp_dinv<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.diag, q.dinv); }
 
 void qp_to_x(const QpDev &q, const float2 *pos, cudaStream_t st) {
     k_qp_to_x<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, pos, q.x);

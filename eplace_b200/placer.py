@@ -177,7 +177,7 @@ def load():
         getattr(L, n).argtypes = [vp]
     L.ep_time_kernels.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(KernelTimes)]
     L.ep_quadratic_placement.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(QpStats)]
-    L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(QpStats)]
+    L.ep_quadratic_refine.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(QpStats)]
     L.ep_state_size.argtypes = [vp]
     L.ep_state_size.restype = ctypes.c_uint64
     L.ep_save_state.argtypes = [vp, vp, ctypes.c_uint64]
@@ -566,10 +566,12 @@ class Engine:
         self._check(self._L.ep_quadratic_placement(self.h, int(max_iterations), ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
-    def quadratic_refine(self, rounds, solver_iterations=0):
-        """ep_quadratic_refine: rounds of the quadratic model from the current centres."""
+    def quadratic_refine(self, rounds, solver_iterations=0, jacobi=False):
+        """ep_quadratic_refine: rounds of the quadratic model from the current
+        centres (jacobi: diagonally preconditioned solves)."""
         st = QpStats()
-        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), int(solver_iterations), ctypes.byref(st)))
+        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), int(solver_iterations), int(bool(jacobi)),
+                                                ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
     def switch_stage(self, stage, filler_ll=None):

@@ -14,10 +14,10 @@ that proposes the initial placement in place of the quadratic placement
     design (normalised to the core), one design per step in a seeded order;
   * the start: the network's proposal q + alpha (f - q), q and f the two
     heads, then `rounds` rounds of the quadratic model from there with at
-    most `iters` BiCGSTAB iterations each (ep_quadratic_refine; rounds 0 =
-    none).  (alpha, rounds, iters) are picked on validation designs (not the
-    held-out ones): the least solver work (rounds x iters), then the largest
-    alpha, whose runs end with a mean HPWL within 0.15% of the QP-started
+    most `iters` BiCGSTAB iterations each, Jacobi-preconditioned or not
+    (ep_quadratic_refine; rounds 0 = none).  (alpha, rounds, iters, jacobi)
+    are picked on validation designs (not the held-out ones): the least
+    solver work (rounds x iters), then the largest alpha, whose runs end with a mean HPWL within 0.15% of the QP-started
     runs, else the choice with the lowest mean HPWL;
   * evaluation: on held-out designs, the QP-started run against the
     proposal-started run (iterations and device seconds to overflow < 0.1,
@@ -55,24 +55,27 @@ def training_sizes(count, seed, lo=2_000, hi=50_000):
 
 
 def load_weights(path=WEIGHTS):
-    """(weights, start) of a trained network; start = dict(alpha, rounds, iters)."""
+    """(weights, start) of a trained network; start = dict(alpha, rounds,
+    iters, jacobi)."""
     z = np.load(path)
     iters = int(z["iters"]) if "iters" in z.files else 100
-    return z["weights"], dict(alpha=float(z["alpha"]), rounds=int(z["rounds"]), iters=iters)
+    jacobi = int(z["jacobi"]) if "jacobi" in z.files else 0
+    return z["weights"], dict(alpha=float(z["alpha"]), rounds=int(z["rounds"]), iters=iters, jacobi=jacobi)
 
 
 def save_weights(path, weights, start, meta):
     np.savez(path, weights=np.asarray(weights, np.float32), alpha=np.float32(start["alpha"]),
-             rounds=np.int32(start["rounds"]), iters=np.int32(start["iters"]), meta=np.array(json.dumps(meta)))
+             rounds=np.int32(start["rounds"]), iters=np.int32(start["iters"]),
+             jacobi=np.int32(start.get("jacobi", 0)), meta=np.array(json.dumps(meta)))
 
 
 def propose(gnn, engine, start):
     """The learned start: the network's proposal, then start["rounds"]
     rounds of the quadratic model from it (start["iters"] solver iterations
-    each)."""
+    each, Jacobi-preconditioned when start["jacobi"])."""
     gnn.propose(engine, start["alpha"])
     if start["rounds"] > 0:
-        engine.quadratic_refine(start["rounds"], start["iters"])
+        engine.quadratic_refine(start["rounds"], start["iters"], start.get("jacobi", 0))
 
 
 def log_pair(directory, name, nl, final_xy):
@@ -158,14 +161,16 @@ def compare(gnn, nl, start, precision=placer.PREC_MIXED, tolerance=0.005):
     return out
 
 
-def pick_start(gnn, netlists, alphas=(0.0, 0.5), refinements=((0, 0), (1, 20), (1, 40), (1, 100), (2, 40)),
+def pick_start(gnn, netlists, alphas=(0.0, 0.5),
+               refinements=((0, 0, 0), (1, 10, 1), (1, 15, 1), (1, 20, 1), (1, 20, 0), (1, 40, 0), (1, 40, 1),
+                            (1, 100, 0)),
                within=0.0015):
-    """On these (validation) netlists: the start (alpha, rounds, iters) with
-    the least solver work (rounds x iters), then the largest alpha, whose
-    runs end with a mean HPWL ratio to the QP-started runs of at most
-    1 + within, else the one with the lowest mean ratio.  Returns it and the
-    table of mean ratios and iterations."""
-    keys = [(a, r, it) for r, it in refinements for a in alphas]
+    """On these (validation) netlists: the start (alpha, rounds, iters,
+    jacobi) with the least solver work (rounds x iters), then the largest
+    alpha, whose runs end with a mean HPWL ratio to the QP-started runs of
+    at most 1 + within, else the one with the lowest mean ratio.  Returns it
+    and the table of mean ratios and iterations."""
+    keys = [(a, r, it, j) for r, it, j in refinements for a in alphas]
     ratio = {k: [] for k in keys}
     iters = {k: [] for k in keys}
     for nl in netlists:
@@ -173,20 +178,21 @@ def pick_start(gnn, netlists, alphas=(0.0, 0.5), refinements=((0, 0), (1, 20), (
         e.save_positions()
         e.quadratic_placement()
         ref = run_from(e, "qp")["hpwl"]
-        for a, r, it in keys:
+        for a, r, it, j in keys:
             e.load_positions()
-            propose(gnn, e, dict(alpha=a, rounds=r, iters=it))
-            st = run_from(e, f"gnn{a}/{r}x{it}")
-            ratio[(a, r, it)].append(st["hpwl"] / ref)
-            iters[(a, r, it)].append(st["iterations"])
+            propose(gnn, e, dict(alpha=a, rounds=r, iters=it, jacobi=j))
+            st = run_from(e, f"gnn{a}/{r}x{it}j{j}")
+            ratio[(a, r, it, j)].append(st["hpwl"] / ref)
+            iters[(a, r, it, j)].append(st["iterations"])
         gnn.release(e)
         e.close()
     mean = {k: float(np.mean(v)) for k, v in ratio.items()}
     ok = [k for k in keys if mean[k] <= 1.0 + within]
     best = min(ok, key=lambda k: (k[1] * k[2], -k[0])) if ok else min(mean, key=mean.get)
-    table = {f"{a}/{r}x{it}": dict(hpwl_ratio=mean[(a, r, it)], iterations=float(np.mean(iters[(a, r, it)])))
-             for a, r, it in keys}
-    return dict(alpha=best[0], rounds=best[1], iters=best[2]), table
+    table = {f"{a}/{r}x{it}{'j' if j else ''}": dict(hpwl_ratio=mean[(a, r, it, j)],
+                                                     iterations=float(np.mean(iters[(a, r, it, j)])))
+             for a, r, it, j in keys}
+    return dict(alpha=best[0], rounds=best[1], iters=best[2], jacobi=best[3]), table
 
 
 def _seeds(spec):

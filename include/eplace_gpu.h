@@ -296,9 +296,12 @@ ep_status ep_quadratic_placement(ep_engine *e, int32_t max_iterations, ep_qp_sta
 /* `rounds` rounds of the same quadratic model starting from the current
  * centres instead of the core centre (no convergence test), each with at
  * most solver_iterations BiCGSTAB iterations (0 = the reference's 100): a
- * short refinement of a start from elsewhere, e.g. ep_gnn_propose.  No
+ * short refinement of a start from elsewhere, e.g. ep_gnn_propose.
+ * preconditioner 0: none (QPPlacer's IdentityPreconditioner); 1: Jacobi
+ * (the systems' diagonals, as Eigen's DiagonalPreconditioner).  No
  * counterpart in the reference. */
-ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, ep_qp_stats *stats);
+ep_status ep_quadratic_refine(ep_engine *e, int32_t rounds, int32_t solver_iterations, int32_t preconditioner,
+                              ep_qp_stats *stats);
 
 /* FirstOrderOptimizer::opt (Optimization/opt.hpp:30-36) with
  * EplaceNesterovOpt (Optimization/nesterov.hpp:86-415) for the current stage:
