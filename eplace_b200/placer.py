@@ -568,9 +568,9 @@ class Engine:
 
     def quadratic_refine(self, rounds, solver_iterations=0, jacobi=False):
         """ep_quadratic_refine: rounds of the quadratic model from the current
-        centres (jacobi: diagonally preconditioned solves)."""
+        centres (jacobi 1: diagonally preconditioned solves, 0: none)."""
         st = QpStats()
-        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), int(solver_iterations), int(bool(jacobi)),
+        self._check(self._L.ep_quadratic_refine(self.h, int(rounds), int(solver_iterations), int(jacobi),
                                                 ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in QpStats._fields_}
 
