@@ -110,6 +110,7 @@ struct ep_engine {
     int32_t *net_dev_order = nullptr;  // nets in device pin order (grouped by degree)
     int n_big_nets = 0;                // nets above kWarpPins pins (the head of that order)
     double create_s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ep_create phases (ep_info.create_seconds)
+    int64_t qp_launches = 0;                         // kernels of the current quadratic placement call
     uint64_t uid = 0;  // distinct per engine created in this process
     QpDev qp{};
     bool qp_ready = false;
@@ -2122,6 +2123,7 @@ ep_status qp_build(ep_engine *e, const float2 *qpos) {
     qp_rows(q, 0, qpos, e->st);
     qp_offsets(q, e->st);
     qp_rows(q, 1, qpos, e->st);
+    e->qp_launches += 5;
     CK(cudaGetLastError());
     return EP_OK;
 }
@@ -2140,10 +2142,12 @@ ep_status qp_solve(ep_engine *e, const float2 *qpos, int max_it, bool jacobi, do
     qp_to_x(q, qpos, st);
     if (jacobi) qp_dinv(q, st);
     qp_init(q, max_it, st);
+    e->qp_launches += 3 + (jacobi ? 1 : 0);
     QpSolve h{};
     for (int done = 0; done < max_it;) {
         const int n = std::min(kChunk, max_it - done);
         qp_iterations(q, n, jacobi, st);
+        e->qp_launches += 6LL * n;
         done += n;
         CK(cudaMemcpyAsync(e->qp_state_h, q.solve, sizeof(QpSolve), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -2188,6 +2192,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
     const int max_outer = max_iterations > 0 ? max_iterations : 20;  // IPiteCount, default 20
     const double target_error = 0.000001;                           // qplace.cpp:47
     CK(cudaEventRecord(e->ev0, st));
+    e->qp_launches = (e->fp64 ? 2 : 0) + (from_centre ? 1 : 0) + 1;
     if (from_centre) qp_center(q, e->grid, e->size, qpos, st);  // moveNodesCenterToCenter
     qp_bounds(q, qpos, q.out, st);
     if ((s = qp_read(e, 1))) return s;
@@ -2200,6 +2205,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
         solver_iters += it;
         qp_from_x(q, e->grid, e->size, qpos, st);  // updateModuleLocation
         qp_bounds(q, qpos, q.out, st);             // calcNetBoundPins
+        e->qp_launches += 2;
         if ((s = qp_read(e, 1))) return s;
         hpwl = e->qp_out_h[0];
         outer = i + 1;
@@ -2223,6 +2229,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
         stats->error_x = err[0];
         stats->error_y = err[1];
         stats->seconds = ms * 1e-3;
+        stats->kernel_launches = e->qp_launches;
     }
     return EP_OK;
 }

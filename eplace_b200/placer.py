@@ -97,7 +97,8 @@ class RunStats(ctypes.Structure):
 
 class QpStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int32), ("solver_iterations", ctypes.c_int32), ("hpwl", ctypes.c_double),
-                ("error_x", ctypes.c_double), ("error_y", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("error_x", ctypes.c_double), ("error_y", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("kernel_launches", ctypes.c_int64)]
 
 
 MAX_TIMED = 12

@@ -72,10 +72,12 @@ def save_weights(path, weights, start, meta):
 def propose(gnn, engine, start):
     """The learned start: the network's proposal, then start["rounds"]
     rounds of the quadratic model from it (start["iters"] solver iterations
-    each, Jacobi-preconditioned when start["jacobi"])."""
+    each, Jacobi-preconditioned when start["jacobi"]); returns the
+    refinement's statistics (None without refinement)."""
     gnn.propose(engine, start["alpha"])
     if start["rounds"] > 0:
-        engine.quadratic_refine(start["rounds"], start["iters"], start.get("jacobi", 0))
+        return engine.quadratic_refine(start["rounds"], start["iters"], start.get("jacobi", 0))
+    return None
 
 
 def log_pair(directory, name, nl, final_xy):

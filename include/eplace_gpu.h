@@ -166,6 +166,7 @@ typedef struct ep_qp_stats {
     double hpwl;               /* HPWL after the last round (calcNetBoundPins) */
     double error_x, error_y;   /* |r| / |b| of the last solves (solver.error()) */
     double seconds;            /* device time, CUDA events */
+    int64_t kernel_launches;   /* engine kernels this call launched */
 } ep_qp_stats;
 
 /* Per-kernel device times of one evaluation + step (ep_time_kernels). */
