@@ -52,11 +52,11 @@ DESIGN = dict(cells=200_000, seed=7, start_seed=3, start_sigma=0.05)
 REF_RUNS = os.path.join(ROOT, "tests", "golden", "reference_runs.json")
 SAMPLE_ITERS = 8  # reference optimizer steps of the cpu_baseline sample
 # kernels one ep_gnn_propose launches on a netlist it has not bound: the
-# features (initial values, terminal pin counts and feature, 1/degree, 128
-# diffusion steps of 2 kernels, 3 feature stores), the forward pass (input
-# layer, 3 x (net mean, node mean, dense), output), the proposal and the
-# position store
-GNN_LAUNCHES = 4 + 2 * 128 + 3 + 1 + 3 * 3 + 1 + 2
+# features (initial values, terminal pin counts and feature, 1/degree, the
+# aggregation indices, 128 diffusion steps of 2 kernels, 3 feature stores),
+# the forward pass (input layer, 3 x (net mean, node mean, dense), output),
+# the proposal and the position store
+GNN_LAUNCHES = 5 + 2 * 128 + 3 + 1 + 3 * 3 + 1 + 2
 
 
 def netlist():

@@ -2289,6 +2289,7 @@ int engine_graph(ep_engine *e, EngineGraph *g) {
     g->grid = e->grid;
     g->st = e->st;
     g->device = e->device;
+    g->d_status = &e->S->status;
     return EP_OK;
 }
 

@@ -198,6 +198,7 @@ struct EngineGraph {
     Grid grid;
     cudaStream_t st;
     int device;
+    int *d_status;                   // the engine's device status word (EP_ERR_* bits)
 };
 int engine_graph(ep_engine *e, EngineGraph *g);
 // Movable-node centres from a device float2 array (clamped into the core).

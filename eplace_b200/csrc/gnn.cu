@@ -42,6 +42,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "tc_ptx.cuh"
 
 namespace ep {
 namespace {
@@ -73,6 +74,10 @@ struct Net {
     const int32_t *net_order;            // nets in device pin order (neighbouring nets of equal degree)
     int n_big;                           // nets above kWarpPins pins: the head of net_order
     const int32_t *pad_start, *pad_net;  // terminals' pins (training only; may be null)
+    // flattened indices, built once per bound netlist (k_graph_index):
+    const int4 *kinfo;        // [nnet] per net in device order: first pin, degree, 1/degree (bits), net
+    const int32_t *pin_node;  // [np] node (0..N-1) of each device pin
+    const int32_t *q_net;     // [pins of movable nodes] net of each pin, in object pin order
 };
 
 __device__ __forceinline__ int node_of(int o, int nn, int n_obj) { return o < nn ? o : nn + (o - n_obj); }
@@ -117,19 +122,35 @@ __global__ void k_inv_deg(int nnet, const int32_t *__restrict__ deg, float *__re
     if (n < nnet) inv[n] = deg[n] > 0 ? 1.f / deg[n] : 0.f;
 }
 
+// The aggregations' index arrays, one level of indirection shallower than
+// the engine's: kinfo[k] for the k-th net of the device order (its first
+// pin, degree, 1/degree as in k_inv_deg, id), the node of every pin, and the
+// net of every pin of a movable node in object pin order.  Launched with
+// max(nnet, np) threads.
+__global__ void k_graph_index(Net g, int np, int4 *__restrict__ kinfo, int32_t *__restrict__ pin_node,
+                              int32_t *__restrict__ q_net) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < g.nnet) {
+        const int n = g.net_order[t], d = g.net_deg[n];
+        kinfo[t] = make_int4(g.net_first[n], d, __float_as_int(d > 0 ? 1.f / d : 0.f), n);
+    }
+    if (t < np) pin_node[t] = node_of(g.owner[t], g.nn, g.n_obj);
+    if (t < g.obj_pin_start[g.nn]) q_net[t] = g.pin_net[g.obj_pin_dev[t]];
+}
+
 // The nets above kWarpPins pins (the head of the device order) take a warp
 // each: lane l sums pins l, l + 32, ... and a fixed xor tree adds the lanes.
 // Every other net takes a thread, in device order, so a warp's nets have the
 // same degree.  Launched with 32 n_big + (nnet - n_big) threads.
-__global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ v,
-                           float2 *__restrict__ a) {
+__global__ void k_diff_net(Net g, const float2 *__restrict__ v, float2 *__restrict__ a) {
     pdl_begin();
     const int t = blockIdx.x * blockDim.x + threadIdx.x, big = g.n_big * 32;
     if (t < big) {  // whole warps
-        const int n = g.net_order[t >> 5], lane = t & 31;
+        const int4 r = g.kinfo[t >> 5];
+        const int lane = t & 31;
         float sx = 0.f, sy = 0.f;
-        for (int p = g.net_first[n] + lane, e = g.net_first[n] + g.net_deg[n]; p < e; p += 32) {
-            const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
+        for (int p = r.x + lane, e = r.x + r.y; p < e; p += 32) {
+            const float2 q = v[g.pin_node[p]];
             sx += q.x;
             sy += q.y;
         }
@@ -138,20 +159,22 @@ __global__ void k_diff_net(Net g, const float *__restrict__ inv_deg, const float
             sx += __shfl_xor_sync(0xffffffffu, sx, o);
             sy += __shfl_xor_sync(0xffffffffu, sy, o);
         }
-        if (lane == 0) a[n] = make_float2(sx * inv_deg[n], sy * inv_deg[n]);
+        const float inv = __int_as_float(r.z);
+        if (lane == 0) a[r.w] = make_float2(sx * inv, sy * inv);
         return;
     }
     const int k = g.n_big + (t - big);
     if (k >= g.nnet) return;
-    const int n = g.net_order[k];
+    const int4 r = g.kinfo[k];
     float sx = 0.f, sy = 0.f;
 #pragma unroll 4
-    for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
-        const float2 q = v[node_of(g.owner[p], g.nn, g.n_obj)];
+    for (int p = r.x, e = r.x + r.y; p < e; p++) {
+        const float2 q = v[g.pin_node[p]];
         sx += q.x;
         sy += q.y;
     }
-    a[n] = make_float2(sx * inv_deg[n], sy * inv_deg[n]);
+    const float inv = __int_as_float(r.z);
+    a[r.w] = make_float2(sx * inv, sy * inv);
 }
 
 __global__ void k_diff_node(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ a,
@@ -162,8 +185,9 @@ __global__ void k_diff_node(Net g, const float *__restrict__ inv_pins, const flo
     const int q0 = g.obj_pin_start[c], q1 = g.obj_pin_start[c + 1];
     if (q1 == q0) return;
     float sx = 0.f, sy = 0.f;
+#pragma unroll 4
     for (int q = q0; q < q1; q++) {
-        const float2 t = a[g.pin_net[g.obj_pin_dev[q]]];
+        const float2 t = a[g.q_net[q]];
         sx += t.x;
         sy += t.y;
     }
@@ -189,10 +213,11 @@ __global__ void __launch_bounds__(kT) k_net_mean(Net g, const float *__restrict_
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if ((int)blockIdx.x < g.n_big) {
         __shared__ float2 part[kBigWarps][32];
-        const int n = g.net_order[blockIdx.x];
+        const int4 r = g.kinfo[blockIdx.x];
+        const int n = r.w;
         float2 s = make_float2(0.f, 0.f);
-        for (int p = g.net_first[n] + w, e = g.net_first[n] + g.net_deg[n]; p < e; p += kBigWarps) {
-            const float2 q = h[(size_t)node_of(g.owner[p], g.nn, g.n_obj) * 32 + lane];
+        for (int p = r.x + w, e = r.x + r.y; p < e; p += kBigWarps) {
+            const float2 q = h[(size_t)g.pin_node[p] * 32 + lane];
             s.x += q.x;
             s.y += q.y;
         }
@@ -204,21 +229,24 @@ __global__ void __launch_bounds__(kT) k_net_mean(Net g, const float *__restrict_
                 t.x += part[k][lane].x;
                 t.y += part[k][lane].y;
             }
-            a[(size_t)n * 32 + lane] = make_float2(t.x * inv_deg[n], t.y * inv_deg[n]);
+            const float inv = __int_as_float(r.z);
+            a[(size_t)n * 32 + lane] = make_float2(t.x * inv, t.y * inv);
         }
         return;
     }
     const int k = g.n_big + ((int)(blockIdx.x - g.n_big) * kBigWarps + w);
     if (k >= g.nnet) return;
-    const int n = g.net_order[k];
+    const int4 r = g.kinfo[k];
+    const int n = r.w;
     float2 s = make_float2(0.f, 0.f);
 #pragma unroll 4
-    for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
-        const float2 q = h[(size_t)node_of(g.owner[p], g.nn, g.n_obj) * 32 + lane];
+    for (int p = r.x, e = r.x + r.y; p < e; p++) {
+        const float2 q = h[(size_t)g.pin_node[p] * 32 + lane];
         s.x += q.x;
         s.y += q.y;
     }
-    a[(size_t)n * 32 + lane] = make_float2(s.x * inv_deg[n], s.y * inv_deg[n]);
+    const float inv = __int_as_float(r.z);
+    a[(size_t)n * 32 + lane] = make_float2(s.x * inv, s.y * inv);
 }
 
 __global__ void k_node_mean(Net g, const float *__restrict__ inv_pins, const float2 *__restrict__ a,
@@ -228,7 +256,7 @@ __global__ void k_node_mean(Net g, const float *__restrict__ inv_pins, const flo
     float2 s = make_float2(0.f, 0.f);
     if (c < g.nn) {
         for (int q = g.obj_pin_start[c]; q < g.obj_pin_start[c + 1]; q++) {
-            const float2 t = a[(size_t)g.pin_net[g.obj_pin_dev[q]] * 32 + lane];
+            const float2 t = a[(size_t)g.q_net[q] * 32 + lane];
             s.x += t.x;
             s.y += t.y;
         }
@@ -245,7 +273,7 @@ __global__ void k_node_mean_t(Net g, const float *__restrict__ inv_pins, const f
     if (n >= g.nnet) return;
     float2 s = make_float2(0.f, 0.f);
     for (int p = g.net_first[n], e = p + g.net_deg[n]; p < e; p++) {
-        const int c = node_of(g.owner[p], g.nn, g.n_obj);
+        const int c = g.pin_node[p];
         if (c >= g.nn) continue;
         const float2 t = dm[(size_t)c * 32 + lane];
         s.x += t.x * inv_pins[c];
@@ -262,7 +290,7 @@ __global__ void k_net_mean_t_add(Net g, const float *__restrict__ inv_deg, const
     float2 s = make_float2(0.f, 0.f);
     if (c < g.nn) {
         for (int q = g.obj_pin_start[c]; q < g.obj_pin_start[c + 1]; q++) {
-            const int n = g.pin_net[g.obj_pin_dev[q]];
+            const int n = g.q_net[q];
             const float2 t = da[(size_t)n * 32 + lane];
             s.x += t.x * inv_deg[n];
             s.y += t.y * inv_deg[n];
@@ -340,21 +368,208 @@ __global__ void __launch_bounds__(kT) k_dense(int N, const float *__restrict__ X
     }
 }
 
-// The dense layers' BF16 weights as FP32, transposed to [k][o] (layer 0,
-// then layers 1..3), for k_dense.
-constexpr int kWt0 = 0, kWtL = kF * kH, kWtSize = kF * kH + kLayers * 2 * kH * kH;
-inline int wt_off(int l) { return l == 0 ? kWt0 : kWtL + (l - 1) * 2 * kH * kH; }
+// The input layer's BF16 weights as FP32, transposed to [k][o], for k_dense.
+constexpr int kWtSize = kF * kH;
 __global__ void k_transpose_w(const __nv_bfloat16 *__restrict__ wb, float *__restrict__ wt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kWtSize) return;
-    if (i < kWtL) {
-        const int k = i / kH, o = i % kH;
-        wt[i] = bf(wb[kOffW0 + o * kF + k]);
-    } else {
-        const int l = (i - kWtL) / (2 * kH * kH) + 1, j = (i - kWtL) % (2 * kH * kH);
-        const int k = j / kH, o = j % kH;
-        wt[i] = bf(wb[kOffL + (l - 1) * kLayerParams + o * 2 * kH + k]);
+    const int k = i / kH, o = i % kH;
+    wt[i] = bf(wb[kOffW0 + o * kF + k]);
+}
+
+// ------------------------------------------------------ dense, tcgen05 ----
+// The hidden layers (K = 2 kH = 128 inputs [XA | XB], kH = 64 outputs) on
+// the tensor cores: Y = relu(b + [XA | XB] W^T).  Each FP32 input is split
+// into two BF16 planes, hi = bf16(x) and lo = bf16(x - hi) (hi + lo holds x
+// to 2^-17 relative), and both are multiplied by the BF16 weights (exact in
+// BF16) with tcgen05.mma.kind::f16, FP32 accumulators in tensor memory.  A
+// persistent CTA of 256 threads (two per SM) takes 128-row tiles in turn:
+//   all threads  load the tile's rows (coalesced float4), split them and
+//                store both planes in shared memory in the K-major,
+//                128-byte-swizzled layout of the MMA descriptors;
+//   thread 0     issues 16 MMAs (2 K blocks x 4 steps of 16 x 2 planes) and
+//                commits them to an mbarrier;
+//   all threads  wait (bounded), read the accumulators (warp w: TMEM lanes
+//                32 (w % 4) .. + 31 = tile rows, columns 32 (w / 4) .. + 31),
+//                add the bias, relu, stage the tile in shared memory (over the
+//                consumed planes) and store it row-major with coalesced float4
+//                stores.
+// The next tile's loads are in flight while the previous tile is stored.  The
+// weights (64 x 128 BF16) are staged once per CTA.  A wait that gives up sets
+// EP_ERR_TIMEOUT in *status (and in the engine's word, when given); the CTA
+// waits for its own MMAs (bounded) before it frees its tensor memory.
+constexpr int kTcRows = 128, kTcThreads = 256, kTcKB = 2;
+constexpr int kTcWBlock = kH * 128;                 // one K block of W: 64 rows x 128 B
+constexpr int kTcABlock = kTcRows * 128;            // one K block of one input plane
+constexpr int kTcW = kTcKB * kTcWBlock;             // 16 KB
+constexpr int kTcA = 2 * kTcKB * kTcABlock;         // hi and lo planes, 64 KB
+constexpr int kTcLd = kH + 4;                       // staging row stride, floats
+constexpr int kTcLoads = kTcRows * 32 / kTcThreads;  // float4 loads per thread and tile
+constexpr int kTcCols = 64;                         // TMEM columns
+static_assert(kTcRows * kTcLd * 4 <= kTcA, "the staged tile fits over the input planes");
+constexpr size_t kTcSmem = 1024 + kTcW + kTcA + 64;
+
+// Byte offset of element k (0..63) of row r in a K-major block with the
+// 128-byte swizzle: 8-row x 128-byte atoms 1024 bytes apart, the 16-byte
+// chunk index XOR-ed with the row inside the atom.
+__device__ __forceinline__ uint32_t sw128(int r, int k) {
+    return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + (((k >> 3) ^ (r & 7)) << 4) + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
+
+__global__ void __launch_bounds__(kTcThreads, 2)
+k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, const __nv_bfloat16 *__restrict__ W,
+           const float *__restrict__ b, float *__restrict__ Y, int *__restrict__ status, int *__restrict__ engine_status) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *Ws = smem, *As = smem + kTcW;
+    float *stage = (float *)As;
+    uint64_t *bar = (uint64_t *)(As + kTcA);
+    volatile uint32_t *tmem_slot = (volatile uint32_t *)(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(tc::smem_u32((const void *)tmem_slot)), "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // weights: row o, K block kb, 16-byte chunk j (8 BF16)
+    for (int i = tid; i < kH * kTcKB * 8; i += kTcThreads) {
+        const int o = i >> 4, kb = (i >> 3) & 1, j = i & 7;
+        const uint4 v = *reinterpret_cast<const uint4 *>(W + (size_t)o * 2 * kH + kb * 64 + j * 8);
+        *reinterpret_cast<uint4 *>(Ws + kb * kTcWBlock + sw128(o, j * 8)) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int ntiles = (N + kTcRows - 1) / kTcRows;
+    const int kb_l = lane >> 4, k_l = (lane & 15) * 4;  // this lane's K block and first K of its float4
+    const float *src = kb_l ? XB : XA;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int r0 = tile * kTcRows;
+        // warp w, load i: row 8 i + w (a warp reads one row: XA's 64 floats in
+        // lanes 0-15, XB's in lanes 16-31)
+        float4 v[kTcLoads];
+#pragma unroll
+        for (int i = 0; i < kTcLoads; i++) {
+            const int gr = r0 + i * 8 + warp;
+            v[i] = gr < N ? __ldg(reinterpret_cast<const float4 *>(src + (size_t)gr * kH + k_l))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();  // the previous tile's staged rows are stored
+#pragma unroll
+        for (int i = 0; i < kTcLoads; i++) {
+            const int row = i * 8 + warp;
+            uint16_t h[4], l[4];
+            tc::bf16_split(v[i].x, h[0], l[0]);
+            tc::bf16_split(v[i].y, h[1], l[1]);
+            tc::bf16_split(v[i].z, h[2], l[2]);
+            tc::bf16_split(v[i].w, h[3], l[3]);
+            const uint32_t off = kb_l * kTcABlock + sw128(row, k_l);
+            *reinterpret_cast<uint2 *>(As + off) = make_uint2(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]));
+            *reinterpret_cast<uint2 *>(As + kTcKB * kTcABlock + off) =
+                make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t idesc = tc::umma_idesc(kTcRows, kH);
+            const uint32_t a = tc::smem_u32(As), w = tc::smem_u32(Ws);
+#pragma unroll
+            for (int kb = 0; kb < kTcKB; kb++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t ao = kb * kTcABlock + k * 32, wo = kb * kTcWBlock + k * 32;
+                    tc::umma_bf16(tmem, tc::umma_desc(a + ao), tc::umma_desc(w + wo), idesc, (kb | k) != 0);
+                    tc::umma_bf16(tmem, tc::umma_desc(a + kTcKB * kTcABlock + ao), tc::umma_desc(w + wo), idesc, 1);
+                }
+            tc::umma_commit(bar);
+        }
+        // lane 0 of each warp waits; the CTA goes on only if every warp saw
+        // the commit (a uniform verdict, so no barrier is left half-reached)
+        int got = 1;
+        if (lane == 0) {
+            got = 0;
+            for (unsigned it = 0; it < tc::kWaitLimit; it++)
+                if (tc::mbar_try_wait(bar, phase)) {
+                    got = 1;
+                    break;
+                }
+        }
+        got = __shfl_sync(0xffffffffu, got, 0);
+        ok = __syncthreads_and(got) != 0;
+        if (!ok) break;
+        phase ^= 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        {
+            const int q = warp & 3, ch = warp >> 2, row = q * 32 + lane;
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ch * 32);
+#pragma unroll
+            for (int c0 = 0; c0 < 32; c0 += 16) {
+                uint32_t r[16];
+                tc::tmem_ld16(taddr + (uint32_t)c0, r);
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    const int col = ch * 32 + c0 + j;
+                    float4 o;
+                    o.x = fmaxf(__uint_as_float(r[j]) + __ldg(b + col), 0.f);
+                    o.y = fmaxf(__uint_as_float(r[j + 1]) + __ldg(b + col + 1), 0.f);
+                    o.z = fmaxf(__uint_as_float(r[j + 2]) + __ldg(b + col + 2), 0.f);
+                    o.w = fmaxf(__uint_as_float(r[j + 3]) + __ldg(b + col + 3), 0.f);
+                    *reinterpret_cast<float4 *>(stage + row * kTcLd + col) = o;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kTcRows * 16 / kTcThreads; i++) {
+            const int u = i * kTcThreads + tid, row = u >> 4, c4 = u & 15, gr = r0 + row;
+            if (gr < N)
+                *reinterpret_cast<float4 *>(Y + (size_t)gr * kH + c4 * 4) =
+                    *reinterpret_cast<const float4 *>(stage + row * kTcLd + c4 * 4);
+        }
+    }
+    if (!ok && tid == 0) {
+        // the MMAs of the tile in flight complete before the tensor memory is freed
+        for (unsigned it = 0; it < tc::kWaitLimit && !tc::mbar_try_wait(bar, phase); it++) {
+        }
+        atomicOr(status, 1 << EP_ERR_TIMEOUT);
+        if (engine_status) atomicOr(engine_status, 1 << EP_ERR_TIMEOUT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
+    }
+}
+
+// Launched as clusters of one CTA, like the tensor-core Poisson GEMMs.
+void launch_dense_tc(int grid, cudaStream_t st, int N, const float *XA, const float *XB, const __nv_bfloat16 *W,
+                     const float *b, float *Y, int *status, int *engine_status) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = kTcSmem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_dense_tc, N, XA, XB, W, b, Y, status, engine_status);
 }
 
 // dX = (dY .* (Y > 0)) W, split into dXA (KA cols) and dXB (KB cols).
@@ -476,12 +691,17 @@ __global__ void k_output(int N, const float *__restrict__ h, const __nv_bfloat16
     float r[kOut];
 #pragma unroll
     for (int j = 0; j < kOut; j++) r[j] = b4[j];
-    const float *hc = h + (size_t)c * kH;
-#pragma unroll 8
-    for (int k = 0; k < kH; k++) {
-        const float x = hc[k];
+    const float4 *hc = reinterpret_cast<const float4 *>(h + (size_t)c * kH);
+    float4 x4[kH / 4];
 #pragma unroll
-        for (int j = 0; j < kOut; j++) r[j] = fmaf(x, bf(W4[j * kH + k]), r[j]);
+    for (int k4 = 0; k4 < kH / 4; k4++) x4[k4] = __ldg(hc + k4);  // the whole row in flight
+#pragma unroll
+    for (int k4 = 0; k4 < kH / 4; k4++) {
+        const float x[4] = {x4[k4].x, x4[k4].y, x4[k4].z, x4[k4].w};
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < kOut; j++) r[j] = fmaf(x[i], bf(W4[j * kH + 4 * k4 + i]), r[j]);
     }
     raw[c] = make_float4(r[0], r[1], r[2], r[3]);
     const float2 b = base[c];
@@ -583,7 +803,9 @@ struct ep_gnn {
     std::string err;
     float *w = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *wb = nullptr;
-    float *wt = nullptr;  // the dense layers' weights as FP32 [k][o] (k_transpose_w)
+    float *wt = nullptr;  // the input layer's weights as FP32 [k][o] (k_transpose_w)
+    int *tc_flag_h = nullptr, *tc_flag_d = nullptr;  // mapped: EP_ERR_TIMEOUT bit of the tensor-core layers
+    int sms = 148;
     double *loss = nullptr;
     int64_t step = 0;
     // bound netlist
@@ -592,11 +814,13 @@ struct ep_gnn {
     Net net{};
     EngineGraph eg{};
     // capacities and buffers
-    size_t capN = 0, capNet = 0, capPad = 0, capT = 0;
+    size_t capN = 0, capNet = 0, capPad = 0, capT = 0, capP = 0;
     float *X = nullptr, *inv_pins = nullptr, *inv_deg = nullptr;
     float2 *v = nullptr, *netv = nullptr;
     int *padcnt = nullptr;
     int32_t *pad_start = nullptr, *pad_net = nullptr;
+    int4 *kinfo = nullptr;
+    int32_t *pin_node = nullptr, *q_net = nullptr;
     float *h[kLayers + 1] = {}, *m[kLayers + 1] = {};
     float *a = nullptr, *dh = nullptr, *dx = nullptr, *dm = nullptr, *da = nullptr, *partial = nullptr;
     float4 *raw = nullptr, *pred = nullptr, *dout = nullptr, *target = nullptr;
@@ -627,7 +851,7 @@ void set_smem_attrs() {
     if (std::find(done.begin(), done.end(), dev) != done.end()) return;
     done.push_back(dev);
     cudaFuncSetAttribute(k_dense<kF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dense(kF));
-    cudaFuncSetAttribute(k_dense<kH, kH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dense(2 * kH));
+    cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     cudaFuncSetAttribute(k_dense_dx<kH, kH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dx(2 * kH));
 }
 
@@ -641,9 +865,9 @@ bool walloc(ep_gnn *g, T *&p, size_t n) {
     return true;
 }
 
-// Grow the workspace to hold N nodes, nnet nets and nt terminals.
-ep_status reserve(ep_gnn *g, size_t N, size_t nnet, size_t nt) {
-    if (N <= g->capN && nnet <= g->capNet && nt <= g->capT) return EP_OK;
+// Grow the workspace to hold N nodes, nnet nets, nt terminals and np pins.
+ep_status reserve(ep_gnn *g, size_t N, size_t nnet, size_t nt, size_t np) {
+    if (N <= g->capN && nnet <= g->capNet && nt <= g->capT && np <= g->capP) return EP_OK;
     cudaDeviceSynchronize();
     for (void *p : g->ws) cudaFree(p);
     g->ws.clear();
@@ -654,22 +878,25 @@ ep_status reserve(ep_gnn *g, size_t N, size_t nnet, size_t nt) {
     N = std::max(N, g->capN);
     nnet = std::max(nnet, g->capNet);
     nt = std::max(nt, g->capT);
+    np = std::max(np, g->capP);
     bool ok = walloc(g, g->X, N * kF) && walloc(g, g->inv_pins, N) && walloc(g, g->inv_deg, nnet) &&
               walloc(g, g->v, N) && walloc(g, g->netv, nnet) && walloc(g, g->padcnt, nt) &&
               walloc(g, g->pad_start, nt + 1) && walloc(g, g->a, nnet * kH) && walloc(g, g->dh, N * kH) &&
               walloc(g, g->dx, N * kH) && walloc(g, g->dm, N * kH) && walloc(g, g->da, nnet * kH) &&
               walloc(g, g->partial, (size_t)nblk((long long)N, kRowsPerBlock) * (kH * 2 * kH + kH)) &&
               walloc(g, g->raw, N) && walloc(g, g->pred, N) && walloc(g, g->dout, N) && walloc(g, g->target, N) &&
-              walloc(g, g->xy, N) && walloc(g, g->loss_part, nblk((long long)N));
+              walloc(g, g->xy, N) && walloc(g, g->loss_part, nblk((long long)N)) && walloc(g, g->kinfo, nnet) &&
+              walloc(g, g->pin_node, np) && walloc(g, g->q_net, np);
     for (int l = 0; l <= kLayers && ok; l++) ok = walloc(g, g->h[l], N * kH) && walloc(g, g->m[l], N * kH);
     if (!ok) {
-        g->capN = g->capNet = g->capT = 0;
+        g->capN = g->capNet = g->capT = g->capP = 0;
         g->err = "cudaMalloc failed for the network's workspace";
         return EP_ERR_NOMEM;
     }
     g->capN = N;
     g->capNet = nnet;
     g->capT = nt;
+    g->capP = np;
     return EP_OK;
 }
 
@@ -692,7 +919,7 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     }
     set_smem_attrs();
     const int N = eg.nn + eg.nt;
-    ep_status s = reserve(g, N, eg.nnet, eg.nt);
+    ep_status s = reserve(g, N, eg.nnet, eg.nt, eg.np);
     if (s) return s;
     g->eg = eg;
     g->pads_ready = false;
@@ -711,6 +938,9 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
     n.n_big = eg.n_big_nets;
     n.pad_start = g->pad_start;
     n.pad_net = g->pad_net;
+    n.kinfo = g->kinfo;
+    n.pin_node = g->pin_node;
+    n.q_net = g->q_net;
     cudaStream_t st = eg.st;
     if (eg.fp64)
         k_init<double><<<nblk(N), kT, 0, st>>>(n, eg.d_area, eg.d_npins, (const double2 *)eg.d_pos, eg.grid, g->X,
@@ -724,11 +954,11 @@ ep_status bind(ep_gnn *g, ep_engine *e) {
         k_pad_feature<<<nblk(eg.nt), kT, 0, st>>>(eg.nt, eg.nn, g->padcnt, g->X);
     }
     k_inv_deg<<<nblk(eg.nnet), kT, 0, st>>>(eg.nnet, eg.d_net_deg, g->inv_deg);
+    k_graph_index<<<nblk(std::max(eg.nnet, eg.np)), kT, 0, st>>>(n, eg.np, g->kinfo, g->pin_node, g->q_net);
     int col = 3;
     for (int k = 1; k <= kDiffSteps[2]; k++) {
         // programmatic serialisation: the next pass's blocks wait resident
-        launch_k(k_diff_net, nblk(31LL * n.n_big + eg.nnet), kT, 0, st, n, (const float *)g->inv_deg,
-                 (const float2 *)g->v, g->netv);
+        launch_k(k_diff_net, nblk(31LL * n.n_big + eg.nnet), kT, 0, st, n, (const float2 *)g->v, g->netv);
         launch_k(k_diff_node, nblk(eg.nn), kT, 0, st, n, (const float *)g->inv_pins, (const float2 *)g->netv, g->v);
         if (k == kDiffSteps[0] || k == kDiffSteps[1] || k == kDiffSteps[2]) {
             launch_k(k_store_feature, nblk(N), kT, 0, st, N, (const float2 *)g->v, g->X, col);
@@ -785,14 +1015,20 @@ ep_status forward(ep_gnn *g) {
     cudaStream_t st = g->eg.st;
     const float *w = g->w;
     const __nv_bfloat16 *wb = g->wb;
-    k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, g->wt + wt_off(0), w + kOffB0,
+    if (*(volatile int *)g->tc_flag_h) {  // a give-up of an earlier forward pass, reported once
+        *(volatile int *)g->tc_flag_h = 0;
+        g->err = "a bounded wait of the tensor-core dense layers gave up";
+        return EP_ERR_TIMEOUT;
+    }
+    const int tc_grid = std::max(1, std::min((N + kTcRows - 1) / kTcRows, 2 * g->sms));
+    k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, g->wt, w + kOffB0,
                                                                     g->h[0]);
     for (int l = 1; l <= kLayers; l++) {
         k_net_mean<<<n.n_big + nblk(n.nnet - n.n_big, kBigWarps), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
                                                                 (float2 *)g->a);
         k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
-        k_dense<kH, kH><<<nblk(N, kDenseRows), kT, smem_dense(2 * kH), st>>>(N, g->h[l - 1], g->m[l], g->wt + wt_off(l),
-                                                                     w + off_b(l), g->h[l]);
+        launch_dense_tc(tc_grid, st, N, g->h[l - 1], g->m[l], wb + off_w(l), w + off_b(l), g->h[l], g->tc_flag_d,
+                        g->eg.d_status);
     }
     k_output<<<nblk(N), kT, 0, st>>>(N, g->h[kLayers], wb + kOffW4, w + kOffB4, g->v, g->raw, g->pred);
     GK(cudaGetLastError());
@@ -876,10 +1112,14 @@ ep_status ep_gnn_create(int32_t device, uint64_t seed, ep_gnn **out) try {
         cudaMalloc(&g->adam_v, sizeof(float) * kParams) != cudaSuccess ||
         cudaMalloc(&g->wb, sizeof(__nv_bfloat16) * kParams) != cudaSuccess ||
         cudaMalloc(&g->wt, sizeof(float) * kWtSize) != cudaSuccess ||
-        cudaMalloc(&g->loss, sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&g->loss, sizeof(double)) != cudaSuccess ||
+        cudaHostAlloc(&g->tc_flag_h, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&g->tc_flag_d, g->tc_flag_h, 0) != cudaSuccess) {
         g->err = "cudaMalloc failed for the network's weights";
         return EP_ERR_NOMEM;
     }
+    *g->tc_flag_h = 0;
+    cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, device);
     // Glorot-uniform weights, zero biases; the output layer starts small so
     // the first predictions stay near the diffusion coordinates
     std::vector<float> w(kParams, 0.f);
@@ -904,6 +1144,7 @@ void ep_gnn_destroy(ep_gnn *g) {
     for (void *p : {(void *)g->w, (void *)g->grad, (void *)g->adam_m, (void *)g->adam_v, (void *)g->wb,
                     (void *)g->wt, (void *)g->loss})
         if (p) cudaFree(p);
+    if (g->tc_flag_h) cudaFreeHost(g->tc_flag_h);
     delete g;
 }
 

@@ -198,3 +198,52 @@ def test_bad_arguments():
         g.set_weights(np.zeros(3, np.float32))
     g.close()
     e.close()
+
+
+def test_forward_at_many_tiles_per_cta():
+    """The forward pass on a design whose tensor-core dense layers take
+    several 128-row tiles per persistent CTA (60k nodes: 470 tiles over at
+    most two CTAs per SM), against a float64 forward pass with sparse
+    aggregations on the same features; 1e-5 of the core, as above."""
+    import scipy.sparse as sp
+    nl = small_design(60000, 12)
+    e = placer.Engine(nl, placer.default_params(target_density=1.0))
+    g = placer.Gnn(seed=6)
+    w = g.get_weights()
+    w[-(4 * H + 4):] = np.random.default_rng(2).uniform(-0.5, 0.5, 4 * H + 4).astype(np.float32)
+    g.set_weights(w)
+    x = g.features(e).astype(np.float64)
+    pred = g.forward(e)
+    nn, N, nnet = nl.num_nodes, nl.num_nodes + nl.num_terminals, nl.num_nets
+    deg = np.diff(nl.net_start)
+    inc = sp.csr_matrix((np.ones(len(nl.pin_owner)), (np.repeat(np.arange(nnet), deg),
+                                                        np.asarray(nl.pin_owner, np.int64))), shape=(nnet, N))
+    pins = np.asarray(inc.sum(0)).ravel()
+    A = sp.diags(1.0 / np.maximum(deg, 1)) @ inc
+    scale = np.where(np.arange(N) < nn, 1.0 / np.maximum(pins, 1), 0.0)
+    M = sp.diags(scale) @ inc.T.tocsr()
+    import torch
+    wb = torch.tensor(w).to(torch.bfloat16).to(torch.float64).numpy()
+    o = 0
+
+    def take(rows, cols, bf16):
+        nonlocal o
+        v = (wb if bf16 else w.astype(np.float64))[o:o + rows * cols].reshape(rows, cols)
+        o += rows * cols
+        return v
+
+    W0, b0 = take(H, F, True), take(1, H, False)
+    h = np.maximum(x @ W0.T + b0, 0)
+    for _ in range(3):
+        Wl, bl = take(H, 2 * H, True), take(1, H, False)
+        h = np.maximum(np.concatenate([h, M @ (A @ h)], 1) @ Wl.T + bl, 0)
+    W4, b4 = take(4, H, True), take(1, 4, False)
+    d = x[:, 7:9]
+    ref = np.concatenate([d, d], 1) + 0.25 * np.tanh(h @ W4.T + b4)
+    i = e.info
+    core_w, core_h = i.core_urx - i.core_llx, i.core_ury - i.core_lly
+    lo = np.array([i.core_llx, i.core_lly] * 2)
+    size = np.array([core_w, core_h] * 2)
+    assert np.abs(pred - (lo + ref[:nn] * size)).max() < 1e-5 * max(core_w, core_h)
+    g.close()
+    e.close()
