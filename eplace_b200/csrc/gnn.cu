@@ -394,7 +394,7 @@ __global__ void k_transpose_w(const __nv_bfloat16 *__restrict__ wb, float *__res
 //                add the bias, relu, stage the tile in shared memory (over the
 //                consumed planes) and store it row-major with coalesced float4
 //                stores.
-// The next tile's loads are in flight while the previous tile is stored.  The
+// The next tile's loads are in flight during a tile's MMAs and epilogue.  The
 // weights (64 x 128 BF16) are staged once per CTA.  A wait that gives up sets
 // EP_ERR_TIMEOUT in *status (and in the engine's word, when given); the CTA
 // waits for its own MMAs (bounded) before it frees its tensor memory.
@@ -453,18 +453,21 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
     const float *src = kb_l ? XB : XA;
     uint32_t phase = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int r0 = tile * kTcRows;
-        // warp w, load i: row 8 i + w (a warp reads one row: XA's 64 floats in
-        // lanes 0-15, XB's in lanes 16-31)
-        float4 v[kTcLoads];
+    // warp w, load i: row 8 i + w of a tile (a warp reads one row: XA's 64
+    // floats in lanes 0-15, XB's in lanes 16-31); rows past N (and tiles past
+    // the last) read as zeros
+    float4 v[kTcLoads];
+    auto load_tile = [&](int t) {
 #pragma unroll
         for (int i = 0; i < kTcLoads; i++) {
-            const int gr = r0 + i * 8 + warp;
+            const int gr = t * kTcRows + i * 8 + warp;
             v[i] = gr < N ? __ldg(reinterpret_cast<const float4 *>(src + (size_t)gr * kH + k_l))
                           : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        __syncthreads();  // the previous tile's staged rows are stored
+    };
+    load_tile(blockIdx.x);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int r0 = tile * kTcRows;
 #pragma unroll
         for (int i = 0; i < kTcLoads; i++) {
             const int row = i * 8 + warp;
@@ -494,6 +497,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
                 }
             tc::umma_commit(bar);
         }
+        load_tile(tile + gridDim.x);  // the next tile's rows in flight during the MMAs and the epilogue
         // lane 0 of each warp waits; the CTA goes on only if every warp saw
         // the commit (a uniform verdict, so no barrier is left half-reached)
         int got = 1;
@@ -538,6 +542,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
                 *reinterpret_cast<float4 *>(Y + (size_t)gr * kH + c4 * 4) =
                     *reinterpret_cast<const float4 *>(stage + row * kTcLd + c4 * 4);
         }
+        __syncthreads();  // the staged rows are read before the next tile's planes overwrite them
     }
     if (!ok && tid == 0) {
         // the MMAs of the tile in flight complete before the tensor memory is freed
