@@ -177,6 +177,14 @@ __device__ __forceinline__ int pair_terms(int i, int nn, int q2, int axis, const
     return -1;
 }
 
+// The count pass's test of a pair: the partner node when it gives an
+// off-diagonal entry (movable and not i itself), else -1 -- the entries
+// pair_terms reports, without the weights.
+__device__ __forceinline__ int pair_partner(int i, int nn, int q2, const int32_t *__restrict__ owner) {
+    const int j = owner[q2];
+    return j != i && j < nn ? j : -1;
+}
+
 // A pin's partner set as a range: pins [0, end) of its net but `skip`, then
 // `extra` (-1: none) -- the bound pins' sets of partners_x / partners_y.
 struct PartnerRange {
@@ -196,7 +204,9 @@ __device__ __forceinline__ bool range_y(int a, int d, int lo, int hi, PartnerRan
     r = PartnerRange{a, -1, hi > a ? hi : -1};
     return true;
 }
-// partner sets above kLongPartners pins are taken by the whole warp
+// partner sets above kLongPartners pins are taken by the whole warp (placed
+// after the row's short sets; the threshold fixes the order of a row's
+// entries, so the SpMV's sums)
 constexpr int kLongPartners = 32;
 __device__ __forceinline__ bool is_long(const PartnerRange &r) {
     return r.end - (r.skip >= 0) + (r.extra >= 0) > kLongPartners;
@@ -295,20 +305,23 @@ __global__ void __launch_bounds__(kQT) k_qp_offsets(const int32_t *__restrict__ 
     }
 }
 
-// One movable node's row of both systems: counts (fill = 0) or entries,
-// diagonal and right-hand side (fill = 1).  A thread per node takes its pins'
+// One movable node's row of both systems: counts (FILL = false: the
+// partners only, no weights) or entries, diagonal and right-hand side
+// (FILL = true).  A thread per node takes its pins'
 // short partner sets in pin order; then the warp takes the long ones (a bound
 // pin of a large net pairs with every other pin of it), in pin order, 32
 // partners at a time, entries placed by a ballot prefix so they keep the
 // partner order, the sums of the pairs' terms through a fixed xor tree.
+template <bool FILL>
 __global__ void __launch_bounds__(kQT)
-k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int32_t *__restrict__ obj_pin_dev,
+k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__restrict__ obj_pin_dev,
           const int32_t *__restrict__ pin_net, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
           const int4 *__restrict__ bound, const int32_t *__restrict__ owner, const float2 *__restrict__ off,
           const float2 *__restrict__ pos, int32_t *__restrict__ count, const int32_t *__restrict__ row_x,
           const int32_t *__restrict__ row_y, int32_t *__restrict__ col_x, float *__restrict__ val_x,
           int32_t *__restrict__ col_y, float *__restrict__ val_y, float2 *__restrict__ diag,
           float2 *__restrict__ rhs, const QpSolve *__restrict__ S) {
+    constexpr bool fill = FILL;
     if (fill && S->overflow) return;  // uniform: the offsets exceed the allocation, the solve reports it
     const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
     const bool valid = i < nn;  // every lane stays for the warp's long sets
@@ -334,15 +347,23 @@ k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int
         const bool ly = range_y(a, d, bd.z, bd.w, ry) && is_long(ry);
         if (!lx)
             partners_x(a, d, bd.x, bd.y, [&](int b) {
-                float w;
-                const int j = pair_terms(i, nn, f + b, 0, owner, pos, off, c, pa.x, oa.x, w, dsum[0], bsum[0]);
-                if (j >= 0) entry(0, j, w, cnt[0]++);
+                if constexpr (FILL) {
+                    float w;
+                    const int j = pair_terms(i, nn, f + b, 0, owner, pos, off, c, pa.x, oa.x, w, dsum[0], bsum[0]);
+                    if (j >= 0) entry(0, j, w, cnt[0]++);
+                } else if (pair_partner(i, nn, f + b, owner) >= 0) {
+                    cnt[0]++;
+                }
             });
         if (!ly)
             partners_y(a, d, bd.z, bd.w, [&](int b) {
-                float w;
-                const int j = pair_terms(i, nn, f + b, 1, owner, pos, off, c, pa.y, oa.y, w, dsum[1], bsum[1]);
-                if (j >= 0) entry(1, j, w, cnt[1]++);
+                if constexpr (FILL) {
+                    float w;
+                    const int j = pair_terms(i, nn, f + b, 1, owner, pos, off, c, pa.y, oa.y, w, dsum[1], bsum[1]);
+                    if (j >= 0) entry(1, j, w, cnt[1]++);
+                } else if (pair_partner(i, nn, f + b, owner) >= 0) {
+                    cnt[1]++;
+                }
             });
     }
     const int steps = __reduce_max_sync(0xffffffffu, np_i);
@@ -380,7 +401,9 @@ k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int
                     const int b = base + lane;
                     float w = 0.f;
                     int j = -1;
-                    if (b < end && b != skip) j = pair_terms(si, nn, sf + b, axis, owner, pos, off, c, pa, oa, w, ds, bs);
+                    if (b < end && b != skip)
+                        j = FILL ? pair_terms(si, nn, sf + b, axis, owner, pos, off, c, pa, oa, w, ds, bs)
+                                 : pair_partner(si, nn, sf + b, owner);
                     const unsigned m = __ballot_sync(0xffffffffu, j >= 0);
                     if (fill && j >= 0) {
                         const int at = row + at0 + added + __popc(m & ((1u << lane) - 1));
@@ -392,7 +415,9 @@ k_qp_rows(int nn, int fill, const int32_t *__restrict__ obj_pin_start, const int
                 if (extra >= 0) {
                     int j = -1;
                     float w = 0.f;
-                    if (lane == 0) j = pair_terms(si, nn, sf + extra, axis, owner, pos, off, c, pa, oa, w, ds, bs);
+                    if (lane == 0)
+                        j = FILL ? pair_terms(si, nn, sf + extra, axis, owner, pos, off, c, pa, oa, w, ds, bs)
+                                 : pair_partner(si, nn, sf + extra, owner);
                     if (fill && j >= 0) {
                         col[axis][row + at0 + added] = j;
                         val[axis][row + at0 + added] = -w;
@@ -786,7 +811,7 @@ void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st)
 }
 
 void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
-    k_qp_rows<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, fill, q.obj_pin_start, q.obj_pin_dev, q.pin_net, q.net_first,
+    (fill ? k_qp_rows<true> : k_qp_rows<false>)<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.obj_pin_start, q.obj_pin_dev, q.pin_net, q.net_first,
                                              q.net_deg, q.bound, q.owner, q.off, pos, q.count, q.row_x, q.row_y,
                                              q.col_x, q.val_x, q.col_y, q.val_y, q.diag, q.rhs, q.solve);
 }
