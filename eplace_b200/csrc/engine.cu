@@ -2148,7 +2148,7 @@ ep_status qp_setup(ep_engine *e) {
     const size_t cap = 4 * (size_t)np + 16;
     const int pb = qp_partial_blocks(nn, nnet);
     ep_status s;
-    if ((s = dalloc(e, q.bound, std::max(nnet, 1))) ||
+    if ((s = dalloc(e, q.bound, std::max(nnet, 1))) || (s = dalloc(e, q.abspin, std::max(np, 1))) ||
         (s = dalloc(e, q.count, 2 * (size_t)nn)) || (s = dalloc(e, q.row_x, (size_t)nn + 1)) ||
         (s = dalloc(e, q.row_y, (size_t)nn + 1)) || (s = dalloc(e, q.col_x, cap)) || (s = dalloc(e, q.col_y, cap)) ||
         (s = dalloc(e, q.val_x, cap)) || (s = dalloc(e, q.val_y, cap)) || (s = dalloc(e, q.diag, nn)) ||
@@ -2180,15 +2180,16 @@ ep_status qp_read(ep_engine *e, int n) {
     return EP_OK;
 }
 
-// Build both systems at the current centres: count, prefix sum, fill.
-ep_status qp_build(ep_engine *e, const float2 *qpos) {
+// Build both systems at the centres of the last bounds pass (its bound pins
+// and pin positions): count, prefix sum, fill.
+ep_status qp_build(ep_engine *e) {
     // counts, the CSR offsets by a scan on the device, then the entries: no
     // host round trip (an allocation overflow is flagged in the solver state
     // and reported by qp_solve)
     QpDev &q = e->qp;
-    qp_rows(q, 0, qpos, e->st);
+    qp_rows(q, 0, e->st);
     qp_offsets(q, e->st);
-    qp_rows(q, 1, qpos, e->st);
+    qp_rows(q, 1, e->st);
     e->qp_launches += 5;
     CK(cudaGetLastError());
     return EP_OK;
@@ -2265,7 +2266,7 @@ static ep_status quadratic_placement(ep_engine *e, int32_t max_iterations, bool 
     double hpwl = e->qp_out_h[0], err[2] = {0, 0};
     int outer = 0, solver_iters = 0;
     for (int i = 0;; i++) {
-        if ((s = qp_build(e, qpos))) return s;
+        if ((s = qp_build(e))) return s;
         int it = 0;
         if ((s = qp_solve(e, qpos, solver_its, jacobi, err, it))) return s;  // solver.setMaxIterations(100)
         solver_iters += it;

@@ -228,6 +228,7 @@ struct QpDev {
     const int32_t *owner;
     const float2 *off;
     int4 *bound;                                 // per net: x-min, x-max, y-min, y-max pin (in net)
+    float2 *abspin;                              // [np] pin positions (device order) at the last bounds pass
     int32_t *count;                              // [2 nn] entries per row (X then Y)
     int32_t *row_x, *row_y;                      // [nn + 1] CSR offsets
     int32_t *col_x, *col_y;
@@ -243,7 +244,8 @@ struct QpDev {
     int cap_x, cap_y; // entries allocated per system
 };
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st);
-void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st);
+// the rows read the pin positions the last qp_bounds stored
+void qp_rows(const QpDev &q, int fill, cudaStream_t st);
 // CSR row offsets of both systems from the counts, on the device
 void qp_offsets(const QpDev &q, cudaStream_t st);
 int qp_scan_blocks(int nn);

@@ -71,8 +71,8 @@ __device__ __forceinline__ void ext_max(Ext &a, double v, int k) {
 __global__ void __launch_bounds__(kQT)
 k_qp_bounds(int nnet, int n_big, const int32_t *__restrict__ order, const int32_t *__restrict__ first,
             const int32_t *__restrict__ deg, const int32_t *__restrict__ owner, const float2 *__restrict__ off,
-            const float2 *__restrict__ pos, int4 *__restrict__ bound, double *__restrict__ partials,
-            unsigned *__restrict__ cnt, double *__restrict__ hpwl) {
+            const float2 *__restrict__ pos, int4 *__restrict__ bound, float2 *__restrict__ abspin,
+            double *__restrict__ partials, unsigned *__restrict__ cnt, double *__restrict__ hpwl) {
     __shared__ double sh[32];
     double acc[1] = {0.0};
     const long long big = 32LL * n_big, slots = big + (nnet - n_big);
@@ -85,6 +85,7 @@ k_qp_bounds(int nnet, int n_big, const int32_t *__restrict__ order, const int32_
             Ext ly{1.79769e308, 0x7fffffff}, hy{-1.79769e308, 0x7fffffff};
             for (int k = lane; k < d; k += 32) {
                 const float2 a = abs_pin(pos, off, owner[f + k], f + k);
+                abspin[f + k] = a;
                 ext_min(lx, a.x, k);
                 ext_max(hx, a.x, k);
                 ext_min(ly, a.y, k);
@@ -108,6 +109,7 @@ k_qp_bounds(int nnet, int n_big, const int32_t *__restrict__ order, const int32_
         int4 b = make_int4(0, 0, 0, 0);
         for (int k = 0; k < d; k++) {
             const float2 a = abs_pin(pos, off, owner[f + k], f + k);
+            abspin[f + k] = a;
             if ((double)a.x < mnx) { mnx = a.x; b.x = k; }
             if ((double)a.x > mxx) { mxx = a.x; b.y = k; }
             if ((double)a.y < mny) { mny = a.y; b.z = k; }
@@ -161,11 +163,11 @@ __device__ __forceinline__ float pair_weight(float c, float dist) {
 // (an off-diagonal entry of weight -w), -1 when it is i itself (no pair) or
 // fixed (right-hand side only).
 __device__ __forceinline__ int pair_terms(int i, int nn, int q2, int axis, const int32_t *__restrict__ owner,
-                                          const float2 *__restrict__ pos, const float2 *__restrict__ off, float c,
+                                          const float2 *__restrict__ abspin, const float2 *__restrict__ off, float c,
                                           float pa, float oa, float &w, double &dsum, double &bsum) {
     const int j = owner[q2];
     if (j == i) return -1;
-    const float2 pb2 = abs_pin(pos, off, j, q2);
+    const float2 pb2 = abspin[q2];
     const float pb = axis ? pb2.y : pb2.x, ob = axis ? off[q2].y : off[q2].x;
     w = pair_weight(c, fabsf(__fsub_rn(pa, pb)));
     dsum += w;
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(kQT)
 k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__restrict__ obj_pin_dev,
           const int32_t *__restrict__ pin_net, const int32_t *__restrict__ first, const int32_t *__restrict__ deg,
           const int4 *__restrict__ bound, const int32_t *__restrict__ owner, const float2 *__restrict__ off,
-          const float2 *__restrict__ pos, int32_t *__restrict__ count, const int32_t *__restrict__ row_x,
+          const float2 *__restrict__ abspin, int32_t *__restrict__ count, const int32_t *__restrict__ row_x,
           const int32_t *__restrict__ row_y, int32_t *__restrict__ col_x, float *__restrict__ val_x,
           int32_t *__restrict__ col_y, float *__restrict__ val_y, float2 *__restrict__ diag,
           float2 *__restrict__ rhs, const QpSolve *__restrict__ S) {
@@ -341,7 +343,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
         const int q = obj_pin_dev[k], n = pin_net[q], f = first[n], d = deg[n], a = q - f;
         const int4 bd = bound[n];
         const float c = (float)(1.0 / ((double)d - 1.0));
-        const float2 pa = abs_pin(pos, off, i, q), oa = off[q];
+        const float2 pa = abspin[q], oa = off[q];
         PartnerRange rx, ry;
         const bool lx = range_x(a, d, bd.x, bd.y, rx) && is_long(rx);
         const bool ly = range_y(a, d, bd.z, bd.w, ry) && is_long(ry);
@@ -349,7 +351,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
             partners_x(a, d, bd.x, bd.y, [&](int b) {
                 if constexpr (FILL) {
                     float w;
-                    const int j = pair_terms(i, nn, f + b, 0, owner, pos, off, c, pa.x, oa.x, w, dsum[0], bsum[0]);
+                    const int j = pair_terms(i, nn, f + b, 0, owner, abspin, off, c, pa.x, oa.x, w, dsum[0], bsum[0]);
                     if (j >= 0) entry(0, j, w, cnt[0]++);
                 } else if (pair_partner(i, nn, f + b, owner) >= 0) {
                     cnt[0]++;
@@ -359,7 +361,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
             partners_y(a, d, bd.z, bd.w, [&](int b) {
                 if constexpr (FILL) {
                     float w;
-                    const int j = pair_terms(i, nn, f + b, 1, owner, pos, off, c, pa.y, oa.y, w, dsum[1], bsum[1]);
+                    const int j = pair_terms(i, nn, f + b, 1, owner, abspin, off, c, pa.y, oa.y, w, dsum[1], bsum[1]);
                     if (j >= 0) entry(1, j, w, cnt[1]++);
                 } else if (pair_partner(i, nn, f + b, owner) >= 0) {
                     cnt[1]++;
@@ -392,7 +394,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
                 const int extra = __shfl_sync(0xffffffffu, r[axis].extra, src);
                 const int at0 = __shfl_sync(0xffffffffu, cnt[axis], src);
                 const float c = (float)(1.0 / ((double)sd - 1.0));
-                const float2 pa2 = abs_pin(pos, off, si, sq), oa2 = off[sq];
+                const float2 pa2 = abspin[sq], oa2 = off[sq];
                 const float pa = axis ? pa2.y : pa2.x, oa = axis ? oa2.y : oa2.x;
                 const int row = fill ? (axis ? row_y[si] : row_x[si]) : 0;
                 double ds = 0.0, bs = 0.0;
@@ -402,7 +404,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
                     float w = 0.f;
                     int j = -1;
                     if (b < end && b != skip)
-                        j = FILL ? pair_terms(si, nn, sf + b, axis, owner, pos, off, c, pa, oa, w, ds, bs)
+                        j = FILL ? pair_terms(si, nn, sf + b, axis, owner, abspin, off, c, pa, oa, w, ds, bs)
                                  : pair_partner(si, nn, sf + b, owner);
                     const unsigned m = __ballot_sync(0xffffffffu, j >= 0);
                     if (fill && j >= 0) {
@@ -416,7 +418,7 @@ k_qp_rows(int nn, const int32_t *__restrict__ obj_pin_start, const int32_t *__re
                     int j = -1;
                     float w = 0.f;
                     if (lane == 0)
-                        j = FILL ? pair_terms(si, nn, sf + extra, axis, owner, pos, off, c, pa, oa, w, ds, bs)
+                        j = FILL ? pair_terms(si, nn, sf + extra, axis, owner, abspin, off, c, pa, oa, w, ds, bs)
                                  : pair_partner(si, nn, sf + extra, owner);
                     if (fill && j >= 0) {
                         col[axis][row + at0 + added] = j;
@@ -806,13 +808,13 @@ __global__ void k_qp_center(Grid g, int nn, const float2 *__restrict__ size, flo
 
 void qp_bounds(const QpDev &q, const float2 *pos, double *hpwl, cudaStream_t st) {
     k_qp_bounds<<<qgrid(31 * q.n_big + q.nnet), kQT, 0, st>>>(q.nnet, q.n_big, q.net_order, q.net_first, q.net_deg,
-                                                               q.owner, q.off, pos, q.bound, q.partials, q.cnt,
-                                                               hpwl);
+                                                               q.owner, q.off, pos, q.bound, q.abspin, q.partials,
+                                                               q.cnt, hpwl);
 }
 
-void qp_rows(const QpDev &q, int fill, const float2 *pos, cudaStream_t st) {
+void qp_rows(const QpDev &q, int fill, cudaStream_t st) {
     (fill ? k_qp_rows<true> : k_qp_rows<false>)<<<qblocks(q.nn), kQT, 0, st>>>(q.nn, q.obj_pin_start, q.obj_pin_dev, q.pin_net, q.net_first,
-                                             q.net_deg, q.bound, q.owner, q.off, pos, q.count, q.row_x, q.row_y,
+                                             q.net_deg, q.bound, q.owner, q.off, q.abspin, q.count, q.row_x, q.row_y,
                                              q.col_x, q.val_x, q.col_y, q.val_y, q.diag, q.rhs, q.solve);
 }
 
