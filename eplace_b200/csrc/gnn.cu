@@ -396,7 +396,7 @@ __global__ void k_transpose_w(const __nv_bfloat16 *__restrict__ wb, float *__res
 //                stores.
 // The next tile's loads are in flight during a tile's MMAs and epilogue.  The
 // weights (64 x 128 BF16) are staged once per CTA.  A wait that gives up sets
-// EP_ERR_TIMEOUT in *status (and in the engine's word, when given); the CTA
+// its flag in *status (and EP_ERR_TIMEOUT in the engine's word); the CTA
 // waits for its own MMAs (bounded) before it frees its tensor memory.
 constexpr int kTcRows = 128, kTcThreads = 256, kTcKB = 2;
 constexpr int kTcWBlock = kH * 128;                 // one K block of W: 64 rows x 128 B
@@ -420,7 +420,8 @@ __device__ __forceinline__ uint32_t pack_bf16(uint16_t a, uint16_t b) { return (
 
 __global__ void __launch_bounds__(kTcThreads, 2)
 k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, const __nv_bfloat16 *__restrict__ W,
-           const float *__restrict__ b, float *__restrict__ Y, int *__restrict__ status, int *__restrict__ engine_status) {
+           const float *__restrict__ b, float *__restrict__ Y, int *__restrict__ status, int *__restrict__ engine_status,
+           unsigned wait_limit) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *Ws = smem, *As = smem + kTcW;
@@ -503,7 +504,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
         int got = 1;
         if (lane == 0) {
             got = 0;
-            for (unsigned it = 0; it < tc::kWaitLimit; it++)
+            for (unsigned it = 0; it < wait_limit; it++)
                 if (tc::mbar_try_wait(bar, phase)) {
                     got = 1;
                     break;
@@ -548,7 +549,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
         // the MMAs of the tile in flight complete before the tensor memory is freed
         for (unsigned it = 0; it < tc::kWaitLimit && !tc::mbar_try_wait(bar, phase); it++) {
         }
-        atomicOr(status, 1 << EP_ERR_TIMEOUT);
+        *(volatile int *)status = 1;  // mapped host memory: a plain store
         if (engine_status) atomicOr(engine_status, 1 << EP_ERR_TIMEOUT);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -561,7 +562,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
 
 // Launched as clusters of one CTA, like the tensor-core Poisson GEMMs.
 void launch_dense_tc(int grid, cudaStream_t st, int N, const float *XA, const float *XB, const __nv_bfloat16 *W,
-                     const float *b, float *Y, int *status, int *engine_status) {
+                     const float *b, float *Y, int *status, int *engine_status, unsigned wait_limit) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kTcThreads);
@@ -574,7 +575,7 @@ void launch_dense_tc(int grid, cudaStream_t st, int N, const float *XA, const fl
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_dense_tc, N, XA, XB, W, b, Y, status, engine_status);
+    cudaLaunchKernelEx(&cfg, k_dense_tc, N, XA, XB, W, b, Y, status, engine_status, wait_limit);
 }
 
 // dX = (dY .* (Y > 0)) W, split into dXA (KA cols) and dXB (KB cols).
@@ -810,6 +811,7 @@ struct ep_gnn {
     __nv_bfloat16 *wb = nullptr;
     float *wt = nullptr;  // the input layer's weights as FP32 [k][o] (k_transpose_w)
     int *tc_flag_h = nullptr, *tc_flag_d = nullptr;  // mapped: EP_ERR_TIMEOUT bit of the tensor-core layers
+    unsigned tc_wait_limit = tc::kWaitLimit;          // polls of their mbarrier wait (ep_gnn_set_wait_limit)
     int sms = 148;
     double *loss = nullptr;
     int64_t step = 0;
@@ -1013,6 +1015,15 @@ ep_status bind_pads(ep_gnn *g) {
     return EP_OK;
 }
 
+// A give-up of the tensor-core layers' wait since the last check, reported
+// once (the flag is mapped host memory the kernel writes).
+ep_status tc_give_up(ep_gnn *g) {
+    if (!*(volatile int *)g->tc_flag_h) return EP_OK;
+    *(volatile int *)g->tc_flag_h = 0;
+    g->err = "a bounded wait of the tensor-core dense layers gave up";
+    return EP_ERR_TIMEOUT;
+}
+
 // Forward pass on the bound netlist (activations kept for the backward pass).
 ep_status forward(ep_gnn *g) {
     const Net &n = g->net;
@@ -1020,11 +1031,7 @@ ep_status forward(ep_gnn *g) {
     cudaStream_t st = g->eg.st;
     const float *w = g->w;
     const __nv_bfloat16 *wb = g->wb;
-    if (*(volatile int *)g->tc_flag_h) {  // a give-up of an earlier forward pass, reported once
-        *(volatile int *)g->tc_flag_h = 0;
-        g->err = "a bounded wait of the tensor-core dense layers gave up";
-        return EP_ERR_TIMEOUT;
-    }
+    if (ep_status s = tc_give_up(g)) return s;  // of an earlier (asynchronous) pass
     const int tc_grid = std::max(1, std::min((N + kTcRows - 1) / kTcRows, 2 * g->sms));
     k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, g->wt, w + kOffB0,
                                                                     g->h[0]);
@@ -1033,7 +1040,7 @@ ep_status forward(ep_gnn *g) {
                                                                 (float2 *)g->a);
         k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
         launch_dense_tc(tc_grid, st, N, g->h[l - 1], g->m[l], wb + off_w(l), w + off_b(l), g->h[l], g->tc_flag_d,
-                        g->eg.d_status);
+                        g->eg.d_status, g->tc_wait_limit);
     }
     k_output<<<nblk(N), kT, 0, st>>>(N, g->h[kLayers], wb + kOffW4, w + kOffB4, g->v, g->raw, g->pred);
     GK(cudaGetLastError());
@@ -1197,6 +1204,7 @@ ep_status ep_gnn_forward(ep_gnn *g, ep_engine *e, float *xy4) try {
     std::vector<float4> p(nn);
     GK(cudaMemcpyAsync(p.data(), g->pred, sizeof(float4) * nn, cudaMemcpyDeviceToHost, g->eg.st));
     GK(cudaStreamSynchronize(g->eg.st));
+    if ((s = tc_give_up(g))) return s;
     const Grid &gr = g->eg.grid;
     const float W = gr.urx - gr.llx, H = gr.ury - gr.lly;
     for (int c = 0; c < nn; c++) {
@@ -1218,7 +1226,7 @@ ep_status ep_gnn_loss_grad(ep_gnn *g, ep_engine *e, const float *target4, double
     if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, g->eg.st));
     if (grad) GK(cudaMemcpyAsync(grad, g->grad, sizeof(float) * kParams, cudaMemcpyDeviceToHost, g->eg.st));
     GK(cudaStreamSynchronize(g->eg.st));
-    return EP_OK;
+    return tc_give_up(g);
 } catch (const std::bad_alloc &) {
     return oom(g);
 }
@@ -1235,9 +1243,15 @@ ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target4, float
     GK(cudaGetLastError());
     if (loss) GK(cudaMemcpyAsync(loss, g->loss, sizeof(double), cudaMemcpyDeviceToHost, g->eg.st));
     GK(cudaStreamSynchronize(g->eg.st));
-    return EP_OK;
+    return tc_give_up(g);
 } catch (const std::bad_alloc &) {
     return oom(g);
+}
+
+ep_status ep_gnn_set_wait_limit(ep_gnn *g, int32_t polls) {
+    if (!g) return EP_ERR_ARG;
+    g->tc_wait_limit = polls < 0 ? tc::kWaitLimit : (unsigned)polls;
+    return EP_OK;
 }
 
 ep_status ep_gnn_propose(ep_gnn *g, ep_engine *e, float alpha) {

@@ -119,7 +119,7 @@ EXPORTS = (
     "ep_get_limits", "ep_set_limits", "ep_quadratic_refine", "ep_state_size", "ep_save_state", "ep_load_state",
     "ep_gnn_num_weights", "ep_gnn_create", "ep_gnn_destroy", "ep_gnn_last_error", "ep_gnn_get_weights",
     "ep_gnn_set_weights", "ep_gnn_release", "ep_gnn_features", "ep_gnn_forward", "ep_gnn_loss_grad",
-    "ep_gnn_train_step", "ep_gnn_propose",
+    "ep_gnn_train_step", "ep_gnn_propose", "ep_gnn_set_wait_limit",
     "ep_get_density_fixed", "ep_query", "ep_set_lambda", "ep_penalty_init", "ep_penalty_update",
     "ep_hpwl", "ep_switch_stage", "ep_nesterov_run", "ep_nesterov_begin", "ep_nesterov_step",
     "ep_nesterov_end", "ep_save_positions", "ep_load_positions", "ep_time_kernels", "ep_quadratic_placement", "ep_run_batch",
@@ -215,6 +215,7 @@ def load():
     L.ep_gnn_loss_grad.argtypes = [vp, vp, _f32p, ctypes.POINTER(ctypes.c_double), _f32p]
     L.ep_gnn_train_step.argtypes = [vp, vp, _f32p, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
     L.ep_gnn_propose.argtypes = [vp, vp, ctypes.c_float]
+    L.ep_gnn_set_wait_limit.argtypes = [vp, ctypes.c_int32]
     L.ep_set_limits.argtypes = [vp, ctypes.POINTER(Limits)]
     L.ep_get_positions_f64.argtypes = [vp, ctypes.c_int32, _f64p, ctypes.c_int32]
     L.ep_get_field_f64.argtypes = [vp, _f64p, _f64p, _f64p]
@@ -788,6 +789,11 @@ class Gnn:
 
     def propose(self, engine, alpha=1.0):
         self._check(self._L.ep_gnn_propose(self.h, engine.h, float(alpha)))
+
+    def set_wait_limit(self, polls=None):
+        """ep_gnn_set_wait_limit: polls of the tensor-core layers' bounded
+        wait before it gives up (None: the default)."""
+        self._check(self._L.ep_gnn_set_wait_limit(self.h, -1 if polls is None else int(polls)))
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -466,6 +466,13 @@ ep_status ep_gnn_train_step(ep_gnn *g, ep_engine *e, const float *target4, float
  * clamped into the core; fillers stay.  Enqueued on the engine's stream;
  * ep_initialize must run again afterwards. */
 ep_status ep_gnn_propose(ep_gnn *g, ep_engine *e, float alpha);
+/* Polls of the tensor-core dense layers' mbarrier wait before it gives up
+ * (polls < 0: the default, 2^22).  A wait that gives up leaves that forward
+ * pass's outputs undefined and raises EP_ERR_TIMEOUT in the engine's status
+ * word and in the network's own flag, which the network's next call reports
+ * (the synchronous calls report their own pass's give-up before they
+ * return).  No counterpart in the reference. */
+ep_status ep_gnn_set_wait_limit(ep_gnn *g, int32_t polls);
 
 #ifdef __cplusplus
 }

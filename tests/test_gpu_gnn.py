@@ -247,3 +247,23 @@ def test_forward_at_many_tiles_per_cta():
     assert np.abs(pred - (lo + ref[:nn] * size)).max() < 1e-5 * max(core_w, core_h)
     g.close()
     e.close()
+
+
+def test_dense_layer_wait_gives_up_and_recovers():
+    """The tensor-core layers' mbarrier wait, bounded: with no polls allowed
+    every wait gives up, the forward pass reports EP_ERR_TIMEOUT (the CTA
+    still waits for its own MMAs before it frees its tensor memory), and with
+    the default limit restored the next pass gives the same predictions as
+    before, bit for bit."""
+    nl = small_design(3000, 5)
+    e = placer.Engine(nl, placer.default_params(target_density=1.0))
+    g = placer.Gnn(seed=2)
+    ref = g.forward(e)
+    g.set_wait_limit(0)
+    with pytest.raises(placer.EPError) as err:
+        g.forward(e)
+    assert err.value.status == placer.EP_ERR_TIMEOUT
+    g.set_wait_limit()
+    assert np.array_equal(g.forward(e), ref)
+    g.close()
+    e.close()
