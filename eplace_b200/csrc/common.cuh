@@ -53,8 +53,6 @@ struct DevScalars {
     int step_cap;      // > 0: also stop after this many steps (bounded runs)
     int bk_accept;     // backtracking: the last trial was accepted
     double bk_ratio;   // backtracking: a trial is accepted when 1/L >= bk_ratio * step
-    int loop_bodies;     // device-side loop: bodies of K steps run in this run
-    int loop_body_cap;   // device-side loop: bodies allowed in this run (set by the host)
 };
 
 // ----- working precision ------------------------------------------------------

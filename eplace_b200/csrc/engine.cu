@@ -92,7 +92,6 @@ struct ep_engine {
 
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
-    bool device_loop = false;  // graph = a WHILE node over graph_iters steps (else the steps, replayed)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_poll = nullptr;  // the run's read-back of `done` has landed
     std::mt19937_64 rng;
@@ -437,61 +436,11 @@ ep_status bktrk_step(ep_engine *e) {
     return fetch_scalars(e);
 }
 
-// The run's loop on the device: one graph holding a conditional WHILE node
-// whose body is `iters` captured steps and the condition kernel, so no host
-// round trip separates the bodies.  false (and nothing built) where the
-// driver refuses such a graph.
-bool build_device_loop(ep_engine *e, int iters) {
-    const int64_t before = e->launches;
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t x = nullptr;
-    cudaGraphConditionalHandle h{};
-    cudaGraphNodeParams p{};
-    cudaGraphNode_t node{};
-    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
-              cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
-    if (ok) {
-        p.type = cudaGraphNodeTypeConditional;
-        p.conditional.handle = h;
-        p.conditional.type = cudaGraphCondTypeWhile;
-        p.conditional.size = 1;
-        ok = cudaGraphAddNode(&node, g, nullptr, 0, &p) == cudaSuccess;
-    }
-    if (ok) {
-        cudaGraph_t body = p.conditional.phGraph_out[0];
-        ok = cudaStreamBeginCaptureToGraph(e->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
-             cudaSuccess;
-        if (ok) {
-            for (int i = 0; i < iters; i++) enqueue_loop_step(e);
-            launch_loop_cond(h, e->S, e->st);
-            e->launches += 1;
-            cudaGraph_t out = nullptr;
-            ok = cudaStreamEndCapture(e->st, &out) == cudaSuccess;
-        }
-    }
-    ok = ok && cudaGraphInstantiate(&x, g, 0) == cudaSuccess;
-    if (g) cudaGraphDestroy(g);
-    if (!ok) {
-        if (x) cudaGraphExecDestroy(x);
-        e->launches = before;
-        cudaGetLastError();  // a refused call leaves its error behind
-        return false;
-    }
-    e->graph = x;
-    e->graph_kernels = e->launches - before;  // counted per body run, not at capture
-    e->launches = before;
-    e->graph_iters = iters;
-    e->device_loop = true;
-    return true;
-}
-
 ep_status build_graph(ep_engine *e, int iters) {
     if (e->graph) {
         cudaGraphExecDestroy(e->graph);
         e->graph = nullptr;
     }
-    e->device_loop = false;
-    if (build_device_loop(e, iters)) return EP_OK;
     cudaGraph_t g = nullptr;
     int64_t before = e->launches;
     CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
@@ -1728,7 +1677,6 @@ namespace {
 struct RunState {
     int K = 8;
     bool bktrk = false;
-    bool device = false;  // the loop runs as the graph's WHILE node
     int64_t launches0 = 0;
     int cap = 0, launched = 0;
 };
@@ -1736,22 +1684,13 @@ struct RunState {
 ep_status run_start(ep_engine *e, int32_t max_steps, RunState &r) {
     ep_status s = ep_nesterov_begin(e);
     if (s) return s;
-    const int K = r.K;
-    s = update_scalars(e, [max_steps, K](DevScalars &h) {
-        h.step_cap = max_steps > 0 ? max_steps : 0;
-        // the device-side loop's bound on bodies: past the host loop's cap
-        // (run_check), never reached before the stop flag
-        const int cap = (max_steps > 0 ? max_steps : h.max_iter + 1) + K;
-        h.loop_bodies = 0;
-        h.loop_body_cap = (cap + 2 * K) / K + 1;
-    });
+    s = update_scalars(e, [max_steps](DevScalars &h) { h.step_cap = max_steps > 0 ? max_steps : 0; });
     if (s) return s;
     r.bktrk = e->prm.step_rule == EP_STEP_BKTRK;
     if (!r.bktrk && (!e->graph || e->graph_iters != r.K)) {
         s = build_graph(e, r.K);
         if (s) return s;
     }
-    r.device = !r.bktrk && e->device_loop;
     r.launches0 = e->launches - 1;  // include the stage-begin kernel
     CK(cudaEventRecord(e->ev0, e->st));
     r.cap = (max_steps > 0 ? max_steps : e->hS->max_iter + 1) + r.K;
@@ -1774,10 +1713,6 @@ ep_status run_launch(ep_engine *e, RunState &r) {
         return bktrk_step(e);
     }
     CK(cudaGraphLaunch(e->graph, e->st));
-    if (r.device) {  // the whole run; its bodies are counted by run_finish
-        CK(cudaEventRecord(e->ev_poll, e->st));
-        return EP_OK;
-    }
     e->launches += e->graph_kernels;
     r.launched += r.K;
     CK(cudaMemcpyAsync(&e->hS->done, &e->S->done, sizeof(int), cudaMemcpyDeviceToHost, e->st));
@@ -1791,7 +1726,7 @@ ep_status run_check(ep_engine *e, RunState &r, bool &more) {
         return EP_OK;
     }
     CK(cudaEventSynchronize(e->ev_poll));
-    more = !r.device && !(e->hS->done || r.launched > r.cap + r.K);
+    more = !(e->hS->done || r.launched > r.cap + r.K);
     return EP_OK;
 }
 
@@ -1813,7 +1748,6 @@ ep_status run_finish(ep_engine *e, RunState &r, ep_run_stats *stats) {
     ep_status s = fetch_scalars(e);
     e->in_run = false;
     if (s) return s;
-    if (r.device) e->launches += (int64_t)e->hS->loop_bodies * e->graph_kernels;
     if (stats) {
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev0, e->ev1);

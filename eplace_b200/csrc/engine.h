@@ -173,8 +173,6 @@ void launch_bktrk_commit(DevScalars *S, cudaStream_t st);
 void launch_stage_begin(const KernelCtx &c, const DeviceNetlist &d, const void *pos, void *x, DevScalars *S,
                         cudaStream_t st);
 void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, void *pos, const void *x, cudaStream_t st);
-// The condition kernel of the device-side loop's WHILE node.
-void launch_loop_cond(cudaGraphConditionalHandle h, DevScalars *S, cudaStream_t st);
 // HPWL at the current positions; mode 0 stores it, mode 1 also applies the
 // updatePenaltyFactor rule, mode 2 applies it only if a lambda update is pending.
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S, cudaStream_t st);

@@ -882,10 +882,14 @@ ep_status reserve(ep_gnn *g, size_t N, size_t nnet, size_t nt, size_t np) {
     g->pads_ready = false;
     g->capPad = 0;
     g->pad_net = nullptr;
-    N = std::max(N, g->capN);
-    nnet = std::max(nnet, g->capNet);
-    nt = std::max(nt, g->capT);
-    np = std::max(np, g->capP);
+    // a quarter of headroom on every dimension, so designs of about the same
+    // size do not each grow the workspace again (a growth frees and
+    // reallocates all of it)
+    auto grow = [](size_t want, size_t cap) { return std::max(want + want / 4, cap); };
+    N = grow(N, g->capN);
+    nnet = grow(nnet, g->capNet);
+    nt = grow(nt, g->capT);
+    np = grow(np, g->capP);
     bool ok = walloc(g, g->X, N * kF) && walloc(g, g->inv_pins, N) && walloc(g, g->inv_deg, nnet) &&
               walloc(g, g->v, N) && walloc(g, g->netv, nnet) && walloc(g, g->padcnt, nt) &&
               walloc(g, g->pad_start, nt + 1) && walloc(g, g->a, nnet * kH) && walloc(g, g->dh, N * kH) &&

@@ -1089,19 +1089,6 @@ void launch_wrap_up(const KernelCtx &c, const DeviceNetlist &d, void *pos, const
                  V<float>(pos), V<float>(x));
 }
 
-// Condition of the device-side loop (a conditional WHILE node whose body is
-// K captured steps): run another body while the stop flag is clear and the
-// run's bound on bodies is not reached.  Launched after the body's last step
-// without programmatic serialisation, so it reads the flag that step left.
-__global__ void k_loop_cond(cudaGraphConditionalHandle h, DevScalars *__restrict__ S) {
-    const int n = ++S->loop_bodies;
-    cudaGraphSetConditional(h, (!S->done && n < S->loop_body_cap) ? 1u : 0u);
-}
-
-void launch_loop_cond(cudaGraphConditionalHandle h, DevScalars *S, cudaStream_t st) {
-    k_loop_cond<<<1, 1, 0, st>>>(h, S);
-}
-
 void launch_hpwl(const KernelCtx &c, const DeviceNetlist &d, int mode, DevScalars *S, cudaStream_t st) {
     c.fp64 ? launch_nets<false, false, false, double>(c, d, nullptr, c.part_hp, mode, S, st)
            : launch_nets<false, false, false, float>(c, d, nullptr, c.part_hp, mode, S, st);
