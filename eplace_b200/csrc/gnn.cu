@@ -208,7 +208,7 @@ __global__ void k_store_feature(int N, const float2 *__restrict__ v, float *__re
 // pins w, w + 8, ..., the 8 warp sums are added in warp order); the other
 // nets take a warp each.
 constexpr int kBigWarps = kT / 32;
-__global__ void __launch_bounds__(kT) k_net_mean(Net g, const float *__restrict__ inv_deg, const float2 *__restrict__ h,
+__global__ void __launch_bounds__(kT) k_net_mean(Net g, const float2 *__restrict__ h,
                                                  float2 *__restrict__ a) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if ((int)blockIdx.x < g.n_big) {
@@ -1040,7 +1040,7 @@ ep_status forward(ep_gnn *g) {
     k_dense<kF, 0><<<nblk(N, kDenseRows), kT, smem_dense(kF), st>>>(N, g->X, nullptr, g->wt, w + kOffB0,
                                                                     g->h[0]);
     for (int l = 1; l <= kLayers; l++) {
-        k_net_mean<<<n.n_big + nblk(n.nnet - n.n_big, kBigWarps), kT, 0, st>>>(n, g->inv_deg, (const float2 *)g->h[l - 1],
+        k_net_mean<<<n.n_big + nblk(n.nnet - n.n_big, kBigWarps), kT, 0, st>>>(n, (const float2 *)g->h[l - 1],
                                                                 (float2 *)g->a);
         k_node_mean<<<nblk((long long)N * 32), kT, 0, st>>>(n, g->inv_pins, (const float2 *)g->a, (float2 *)g->m[l]);
         launch_dense_tc(tc_grid, st, N, g->h[l - 1], g->m[l], wb + off_w(l), w + off_b(l), g->h[l], g->tc_flag_d,
