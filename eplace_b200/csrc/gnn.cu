@@ -500,7 +500,7 @@ k_dense_tc(int N, const float *__restrict__ XA, const float *__restrict__ XB, co
         }
         load_tile(tile + gridDim.x);  // the next tile's rows in flight during the MMAs and the epilogue
         // lane 0 of each warp waits; the CTA goes on only if every warp saw
-        // the commit (a uniform verdict, so no barrier is left half-reached)
+        // the commit (a uniform decision, so no barrier is left half-reached)
         int got = 1;
         if (lane == 0) {
             got = 0;
