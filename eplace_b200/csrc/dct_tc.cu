@@ -196,7 +196,7 @@ k_umma_nt(const __grid_constant__ TcGemmParams p, DevScalars *__restrict__ S) {
     __syncwarp();
 
     // ---- epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows ----
-    // lane 0 waits, the warp follows its verdict (tcgen05.ld is warp-aligned).
+    // lane 0 waits, the warp follows its result (tcgen05.ld is warp-aligned).
     // Every GEMM stores its tile transposed, C[m][n] -> out[n * ldo + m], so
     // the 32 lanes of a warp (consecutive m) write consecutive addresses.
     // On an abort, `done` still completes: the issuer commits it after its
