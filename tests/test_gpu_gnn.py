@@ -7,8 +7,9 @@ Tolerances:
     the same 8/32/128 mean-aggregation steps in float64;
   * both heads' predictions and the loss: 1e-5 relative; every weight
     gradient: 1e-4 of the largest gradient entry, against autograd on the
-    BF16-rounded weights (the forward pass uses BF16 weights, FP32
-    accumulation);
+    BF16-rounded weights (the forward pass uses BF16 weights and FP32
+    accumulation; its hidden layers run on the tensor cores with each FP32
+    input split into two BF16 planes, 2^-17 relative);
   * a training step is bitwise repeatable, and 60 Adam steps on one design
     lower its loss by at least a fifth;
   * a proposal puts the movable nodes at q + alpha (f - q) of the forward
